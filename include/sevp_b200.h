@@ -1,0 +1,206 @@
+/*
+ * sevp_b200.h -- C ABI of the B200 (sm_100a) SEVP barotropic elliptic solver.
+ *
+ * Two layers:
+ *
+ *  1. Fortran-compatible entry points.  Same names (gfortran mangling: lower
+ *     case plus a trailing underscore), same argument lists and same array
+ *     layouts as the reference routines; every argument is passed by
+ *     reference and every array is a column-major HOST array.  A gfortran
+ *     caller links them in place of the reference objects.  They copy their
+ *     inputs to the GPU, run the computation there and copy the outputs
+ *     back.  The reference stops the program on failure; these return
+ *     normally and record a status that sevp_last_status() reports.
+ *
+ *  2. A native API on DEVICE pointers: an operator context holding the
+ *     coefficients and the tile influence data, and status-returning solves
+ *     (FP64 PCG, or FP32 PCG inside FP64 iterative refinement).
+ *
+ * Reference paths are relative to the reference project; M/ is
+ * MAIN/template/GLOBAL/src/ and P/ is PREP/template/GLOBAL/src/.
+ *
+ * Array conventions (as in the reference):
+ *   coefficients AX,AY,BB,CX,CY = west, south, centre, east, north
+ *   (called as AL,AB,AC,AR,AT), REAL*4 (I2, J2);
+ *   X, H REAL*8 (I0, J0) with one ghost cell on each side (I0 = I2 + 2);
+ *   F, S REAL*4 (I2, J2); RINV REAL*8 (I2, I2, NB0); RINV1 (I2, I2, NB0-1);
+ *   IE INTEGER (NB0) block boundaries.
+ */
+#ifndef SEVP_B200_H
+#define SEVP_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+#define SEVP_OK 0
+#define SEVP_MAXITER 1     /* iteration cap reached before the tolerance */
+#define SEVP_BREAKDOWN 2   /* a Krylov scalar became zero */
+#define SEVP_NONFINITE 3   /* NaN or Inf in a residual or an input */
+#define SEVP_TIMEOUT 4     /* a bounded device wait gave up */
+#define SEVP_BAD_ARG 5     /* invalid size, pointer or option */
+#define SEVP_CUDA_ERROR 6  /* a CUDA runtime call failed (see sevp_last_error) */
+#define SEVP_SINGULAR 7    /* an influence matrix had a zero pivot */
+
+const char *sevp_status_string(int status);
+/* Text of the last CUDA error seen by the library (empty if none). */
+const char *sevp_last_error(void);
+/* Status of the most recent Fortran-compatible call in this thread. */
+int sevp_last_status(void);
+/* Periodic east-west ghost refresh used by the Krylov drop-ins; the reference
+ * compiles it in with FLAG_PERIODIC_WE (M/sevp.f90:780-786).  Default 1. */
+void sevp_set_periodic_we(int periodic);
+int sevp_get_periodic_we(void);
+
+/* ------------------------------------------- Fortran-compatible drop-ins */
+
+/* Replaces SUBROUTINE REP1, M/sevp.f90:11-107 (periodic, full width). */
+void rep1_(const float *ax, const float *ay, const float *bb, const float *cx, const float *cy,
+           const double *rinv, const double *rinv1, double *dum0, double *dum1, double *dum2,
+           const float *f, double *h, double *x, const int *ie, const int *i0, const int *i2,
+           const int *nblk);
+
+/* Replaces SUBROUTINE REP, M/sevp.f90:335-438 (non-periodic, full width). */
+void rep_(const float *ax, const float *ay, const float *bb, const float *cx, const float *cy,
+          const double *rinv, const double *rinv1, double *dum0, double *dum1, double *dum2,
+          const float *f, double *h, double *x, const int *ie, const int *i0, const int *i2,
+          const int *nblk);
+
+/* Replaces SUBROUTINE REPBIR, M/sevp.f90:218-328 (one strip of M2 columns;
+ * coefficients with leading dimension I2, X with I0, F and RINV with M2). */
+void repbir_(const float *ax, const float *ay, const float *bb, const float *cx, const float *cy,
+             const double *rinv, const double *rinv1, double *dum0, double *dum1, double *dum2,
+             const float *f, double *h, double *x, const int *ie, const int *i0, const int *i2,
+             const int *m0, const int *m2, const int *nblk);
+
+/* Replaces SUBROUTINE REPBIR_PERIOD, M/sevp.f90:109-217 (defined for M0 == I0). */
+void repbir_period_(const float *ax, const float *ay, const float *bb, const float *cx,
+                    const float *cy, const double *rinv, const double *rinv1, double *dum0,
+                    double *dum1, double *dum2, const float *f, double *h, double *x,
+                    const int *ie, const int *i0, const int *i2, const int *m0, const int *m2,
+                    const int *nblk);
+
+/* Replaces the internal PRE1 of P/prep_GLOBAL.f90:327-386 (called at :271). */
+void pre1_(const float *ax, const float *ay, const float *bb, const float *cx, const float *cy,
+           double *rinv, double *rinv1, double *h, const int *ie, const int *i0, const int *i2,
+           const int *nblk);
+
+/* Replaces the internal PRE of P/prep_GLOBAL.f90:457-513 (called at :292, :315). */
+void pre_(const float *ax, const float *ay, const float *bb, const float *cx, const float *cy,
+          double *rinv, double *rinv1, double *h, const int *ie, const int *i2, const int *m0,
+          const int *m2, const int *nblk);
+
+/* Replaces the internal MATINV of P/prep_GLOBAL.f90:516-568 (no pivoting). */
+void matinv_(double *b, const int *n);
+
+/* Replaces subroutine p_sqprod, M/sevp.f90:696-713: r(interior) = A x. */
+void p_sqprod_(const float *al, const float *ab, const float *ac, const float *ar, const float *at,
+               const double *x, double *r, const int *i2, const int *j2);
+
+/* Replaces subroutine p_sqprod_T, M/sevp.f90:714-742. */
+void p_sqprod_t_(const float *al, const float *ab, const float *ac, const float *ar,
+                 const float *at, const double *x, double *r, const int *i2, const int *j2);
+
+/* Replaces subroutine p_inprod, M/sevp.f90:743-757. */
+void p_inprod_(const double *r, const double *p, double *tp, const int *i2, const int *j2);
+
+/* Replaces subroutine solver_boundary_update, M/sevp.f90:773-787. */
+void solver_boundary_update_(double *x, const int *i2, const int *j2);
+
+/* Replaces subroutine p_bicgstab_le, M/sevp.f90:443-552. */
+void p_bicgstab_le_(const float *al, const float *ab, const float *ac, const float *ar,
+                    const float *at, const float *b, double *x, const float *cl, const float *cb,
+                    const float *cc, const float *cr, const float *ct, const int *i2,
+                    const int *j2);
+
+/* Replaces subroutine p_csi, M/sevp.f90:553-616. */
+void p_csi_(const float *al, const float *ab, const float *ac, const float *ar, const float *at,
+            const double *mineig, const double *maxeig, const float *b, double *x,
+            const float *cl, const float *cb, const float *cc, const float *cr, const float *ct,
+            const int *i2, const int *j2);
+
+/* Replaces subroutine lanczos, M/sevp.f90:618-694 (figi :838-904 and ratqr
+ * :906-1006 run on the host: they act on a 10x10 tridiagonal matrix). */
+void lanczos_(const float *al, const float *ab, const float *ac, const float *ar, const float *at,
+              double *mineig, double *maxeig, const int *i2, const int *j2);
+
+/* Overlapping-strip Schwarz sweeps of FS_SOLVER, M/fs_GLOBAL.f90:1904-1966
+ * (FL_EVP_STP == 1): niter sweeps over nbir strips of REPBIR.  RINV is
+ * (IBIR*IBIR, NB0, NBIR) and RINV1 (IBIR*IBIR, NB0-1, NBIR) as written by
+ * PREP; xx ((IBIR+2), J0) is the caller's persistent wrap-strip scratch. */
+void sevp_bir_sweeps_(const float *al, const float *ab, const float *ac, const float *ar,
+                      const float *at, const float *s, const double *rinv, const double *rinv1,
+                      double *x, double *xx, const int *ie, const int *i2, const int *j2,
+                      const int *nb0, const int *nbir, const int *niter);
+
+/* Influence precompute for all BIR strips, P/prep_GLOBAL.f90:272-318. */
+void sevp_pre_strips_(const float *al, const float *ab, const float *ac, const float *ar,
+                      const float *at, double *rinv, double *rinv1, const int *ie, const int *i2,
+                      const int *j2, const int *nb0, const int *nbir);
+
+/* ---------------------------------------------------- native device API */
+
+typedef struct sevp_ctx sevp_ctx;
+
+/* Tile decomposition of the block-Jacobi SEVP preconditioner. */
+typedef struct {
+  int tile_m;   /* tile width in columns: 1..32 */
+  int tile_h;   /* tile height in rows: 1..32 */
+  int sub_rows; /* marching sub-block height in rows (>= 1) */
+  /* optional host array of ceil(ny / tile_h) sub-block heights, one per tile
+   * row (latitude band); NULL uses sub_rows everywhere */
+  const int *sub_rows_by_tile_row;
+} sevp_tiling;
+
+typedef struct {
+  int precision;     /* 0: FP64 PCG; 1: FP32 PCG inside FP64 iterative refinement */
+  double tol;        /* target ||b - A x||_2 / ||b||_2 evaluated in FP64 */
+  int max_iter;      /* cap on the total number of PCG iterations */
+  double inner_tol;  /* precision 1: relative reduction asked of each FP32 solve */
+  int use_guess;     /* 1: x holds the initial guess on entry; 0: start from zero */
+  int check_every;   /* PCG iterations between convergence reads by the host */
+} sevp_solve_opts;
+
+typedef struct {
+  int status;          /* SEVP_* */
+  int iterations;      /* total PCG iterations */
+  int refinements;     /* FP64 residual evaluations (precision 1) */
+  double rel_residual; /* final ||b - A x|| / ||b||, FP64 */
+  double bnorm;        /* ||b||_2 */
+  double ms;           /* device time of the solve */
+} sevp_report;
+
+/* Creates a context for an nx x ny interior grid (periodic in x if
+ * periodic != 0) bound to a CUDA stream (NULL = default stream).  The
+ * context is tied to the current device. */
+int sevp_create(sevp_ctx **ctx, int nx, int ny, int periodic, void *stream);
+int sevp_destroy(sevp_ctx *ctx);
+/* Binds the five FP32 coefficient planes (device pointers, (nx, ny)
+ * column-major, not copied: they must outlive the context's use) and
+ * computes the tile influence data on the GPU. */
+int sevp_set_operator(sevp_ctx *ctx, const float *al, const float *ab, const float *ac,
+                      const float *ar, const float *at, const sevp_tiling *tiling);
+/* Device bytes held by the tile influence data. */
+long long sevp_influence_bytes(const sevp_ctx *ctx);
+/* Solves A x = b (device pointers, (nx, ny) column-major FP64). */
+int sevp_solve(sevp_ctx *ctx, const double *b, double *x, const sevp_solve_opts *opts,
+               sevp_report *report);
+/* Same with host buffers: copies b (and the guess) in and x out. */
+int sevp_solve_host(sevp_ctx *ctx, const double *b_host, double *x_host,
+                    const sevp_solve_opts *opts, sevp_report *report);
+/* y = A x on the unpadded grid (device pointers). */
+int sevp_apply(sevp_ctx *ctx, const double *x, double *y);
+/* z = M^{-1} r: block-Jacobi tiles solved by SEVP marching (device). */
+int sevp_precondition(sevp_ctx *ctx, const double *r, double *z);
+/* Same in the FP32 vector format of the mixed-precision inner solve. */
+int sevp_precondition_f32(sevp_ctx *ctx, const float *r, float *z);
+/* Writes ||b - A x||_2 / ||b||_2 (FP64). */
+int sevp_relative_residual(sevp_ctx *ctx, const double *b, const double *x, double *relres);
+/* Number of kernel launches issued by this context since creation. */
+long long sevp_kernel_launches(const sevp_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SEVP_B200_H */

@@ -1,0 +1,1063 @@
+// Native SEVP-PCG solver for sm_100a: operator apply, block-Jacobi tile SEVP
+// preconditioner (precompute and apply), and the FP64 / mixed-precision
+// preconditioned conjugate-gradient drivers.
+//
+// The reference solves the barotropic pressure equation with SEVP marching
+// alone (M/sevp.f90:11-438) or with an unpreconditioned BiCGSTAB / Chebyshev
+// iteration (M/sevp.f90:443-616).  This file implements the method the
+// library adds: SEVP as the preconditioner of an outer CG iteration, with the
+// domain cut into tiles that are solved by SEVP independently.
+//
+// Per PCG iteration two grid passes are made (the two global reductions of CG
+// force two synchronisation points):
+//   pass A (stencil kernel):  p = z + beta p_old ; q = A p ; partial p.q
+//   pass B (tile kernel):     x += alpha p ; r -= alpha q ; z = M^{-1} r ;
+//                             partial r.z and r.r
+// Scalars (alpha, beta, convergence) are formed on the device by the last CTA
+// of each pass from the per-CTA partial sums, in a fixed order, so results
+// are deterministic and the host only polls a "done" flag between chunks of
+// iterations.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "tile_sevp.cuh"
+
+namespace sevp {
+
+// ------------------------------------------------------------------ state
+struct SolveState {
+  double rz;      // current r.z
+  double pq;      // current p.(A p)
+  double rr;      // current ||r||^2 (recursive residual)
+  double bb;      // reference norm^2 for the stopping test
+  double alpha, beta;
+  double tol2;    // stop when rr <= tol2 * bb
+  double rr64;    // FP64 true residual ||b - A x||^2 (residual kernel)
+  double bb64;    // ||b||^2 (residual kernel)
+  int iter, max_iter, done, status;
+  unsigned ticket[4];
+};
+
+struct Coeffs {
+  const float *al, *ab, *ac, *ar, *at;
+};
+
+struct GridDims {
+  int nx, ny, periodic;
+};
+
+// ------------------------------------------------- reductions / finisher
+// Writes this CTA's NV partial sums, and lets the last CTA to arrive sum all
+// partials in block order and call fin(sums) once.
+template <int NV, class Fin>
+__device__ __forceinline__ void reduce_and_finish(double (&v)[NV], double *partials,
+                                                  unsigned *ticket, Fin &fin) {
+  __shared__ double red[NV * 32];
+  __shared__ int s_last;
+  const int nblk = gridDim.x * gridDim.y;
+  const int bid = blockIdx.y * gridDim.x + blockIdx.x;
+  block_sum<NV>(v, red);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) partials[(size_t)bid * NV + k] = v[k];
+    __threadfence();
+    unsigned t = atomicAdd(ticket, 1u);
+    s_last = (t == (unsigned)nblk - 1u);
+  }
+  __syncthreads();
+  if (s_last) {
+    __threadfence();
+    double acc[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) acc[k] = 0.0;
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x)
+#pragma unroll
+      for (int k = 0; k < NV; ++k) acc[k] += __ldcg(&partials[(size_t)b * NV + k]);
+    __syncthreads();
+    block_sum<NV>(acc, red);
+    if (threadIdx.x == 0) {
+      fin(acc);
+      *ticket = 0u;
+      __threadfence();
+    }
+  }
+}
+
+// ------------------------------------------------------ stencil kernels
+// Column-walking 5-point stencil.  A CTA of 256 threads covers 32 columns;
+// its 8 warps are stacked in y, each walking `rpw` rows.  The field value at
+// a point is produced by op.value(idx) (fused producers: z + beta p, x + d);
+// east/west neighbours come from warp shuffles, except at the warp's edge
+// lanes, which evaluate the neighbour column directly (periodic wrap in x).
+constexpr int kStencilThreads = 256;
+
+template <class Op>
+__global__ void __launch_bounds__(kStencilThreads)
+    k_stencil(GridDims g, Coeffs c, Op op, int rpw, double *partials, unsigned *ticket,
+              SolveState *st) {
+  using T = typename Op::T;
+  if (Op::kUsesState && st->done) return;
+  op.prepare(st);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int nx = g.nx, ny = g.ny;
+  const int i = blockIdx.x * 32 + lane;
+  const int j0 = (blockIdx.y * (kStencilThreads / 32) + w) * rpw;
+  const int j1 = min(j0 + rpw, ny);
+  const bool col_ok = i < nx;
+  double acc[Op::NV];
+#pragma unroll
+  for (int k = 0; k < Op::NV; ++k) acc[k] = 0.0;
+  if (j0 < ny) {
+    int iw = i - 1;
+    if (iw < 0) iw = g.periodic ? nx - 1 : -1;
+    int ie = i + 1;
+    if (ie >= nx) ie = g.periodic ? ie - nx : -1;
+    const bool own_w = (lane == 0);
+    const bool own_e = (lane == 31) || (i + 1 >= nx);
+    T vb = (j0 > 0 && col_ok) ? op.value((size_t)(j0 - 1) * nx + i) : T(0);
+    T vc = col_ok ? op.value((size_t)j0 * nx + i) : T(0);
+    for (int j = j0; j < j1; ++j) {
+      const size_t row = (size_t)j * nx;
+      T va = (j + 1 < ny && col_ok) ? op.value(row + nx + i) : T(0);
+      T vw = __shfl_up_sync(0xffffffffu, vc, 1);
+      T ve = __shfl_down_sync(0xffffffffu, vc, 1);
+      if (own_w) vw = (iw >= 0 && col_ok) ? op.value(row + iw) : T(0);
+      if (own_e) ve = (ie >= 0 && col_ok) ? op.value(row + ie) : T(0);
+      if (col_ok) {
+        const size_t idx = row + i;
+        T av = T(__ldg(c.ab + idx)) * vb;
+        av += T(__ldg(c.al + idx)) * vw;
+        av += T(__ldg(c.ac + idx)) * vc;
+        av += T(__ldg(c.ar + idx)) * ve;
+        av += T(__ldg(c.at + idx)) * va;
+        op.emit(idx, vc, av, acc);
+      }
+      vb = vc;
+      vc = va;
+    }
+  }
+  if (Op::NV > 0) reduce_and_finish<Op::NV>(acc, partials, ticket, op);
+}
+
+// y = A x
+template <typename TT>
+struct OpApply {
+  using T = TT;
+  static constexpr int NV = 1;
+  static constexpr bool kUsesState = false;
+  const T *x;
+  T *y;
+  __device__ void prepare(SolveState *) {}
+  __device__ T value(size_t idx) const { return x[idx]; }
+  __device__ void emit(size_t idx, T, T av, double (&acc)[NV]) const { y[idx] = av; }
+  __device__ void operator()(double (&)[NV]) {}
+};
+
+// PCG pass A: p = z + beta p_old ; q = A p ; p.q  -> alpha = r.z / p.q
+template <typename V>
+struct OpPassA {
+  using T = V;
+  static constexpr int NV = 1;
+  static constexpr bool kUsesState = true;
+  const V *z, *pold;
+  V *pnew, *q;
+  SolveState *st;
+  V beta;
+  bool first;
+  __device__ void prepare(SolveState *s) {
+    beta = (V)s->beta;
+    first = (s->beta == 0.0);
+  }
+  __device__ V value(size_t idx) const {
+    V zv = z[idx];
+    return first ? zv : zv + beta * pold[idx];
+  }
+  __device__ void emit(size_t idx, V vc, V av, double (&acc)[NV]) const {
+    pnew[idx] = vc;
+    q[idx] = av;
+    acc[0] += (double)vc * (double)av;
+  }
+  __device__ void operator()(double (&s)[NV]) {
+    st->pq = s[0];
+    st->iter += 1;
+    if (!isfinite(s[0])) {
+      st->status = SEVP_NONFINITE;
+      st->done = 1;
+    } else if (s[0] == 0.0) {
+      st->status = SEVP_BREAKDOWN;
+      st->done = 1;
+    } else {
+      st->alpha = st->rz / s[0];
+    }
+  }
+};
+
+// FP64 residual: x_out = x + d (d optional, FP32 correction); r = b - A x_out
+// written as R (double or float, optional); sums ||r||^2 and ||b||^2.
+template <typename R>
+struct OpResidual {
+  using T = double;
+  static constexpr int NV = 2;
+  static constexpr bool kUsesState = false;
+  const double *x;
+  const float *d;
+  double *xout;
+  const double *b;
+  R *r;
+  SolveState *st;
+  double tol2;
+  int set_inner;  // 1: also initialise the inner FP32 solve state
+  __device__ void prepare(SolveState *) {}
+  __device__ double value(size_t idx) const {
+    double v = x[idx];
+    if (d) v += (double)d[idx];
+    return v;
+  }
+  __device__ void emit(size_t idx, double vc, double av, double (&acc)[NV]) const {
+    if (xout) xout[idx] = vc;
+    double bv = b[idx];
+    double rv = bv - av;
+    if (r) r[idx] = (R)rv;
+    acc[0] += rv * rv;
+    acc[1] += bv * bv;
+  }
+  __device__ void operator()(double (&s)[NV]) {
+    st->rr64 = s[0];
+    st->bb64 = s[1];
+    if (set_inner) {
+      // inner solve starts from zero: its reference norm is ||r||^2
+      st->bb = s[0];
+      st->rr = s[0];
+      st->tol2 = tol2;
+      st->iter = 0;
+      st->done = 0;
+      st->beta = 0.0;
+      st->status = SEVP_OK;
+    }
+    if (!isfinite(s[0]) || !isfinite(s[1])) st->status = SEVP_NONFINITE;
+  }
+};
+
+// --------------------------------------------------- tile apply kernel
+constexpr int kTileWarps = 4;
+
+struct TileSmem {
+  double *zs;   // [hmax][32]
+  void *rs;     // [hmax][32] of V
+  double *rho;  // [nbmax][32]
+  double *u0;   // [nbmax][32]
+  double *dv;   // [32]
+};
+
+__host__ __device__ inline size_t tile_smem_per_warp(int hmax, int nbmax, int vbytes) {
+  return (size_t)hmax * 32 * 8 + (size_t)hmax * 32 * vbytes + (size_t)nbmax * 32 * 16 + 32 * 8;
+}
+
+// out(n) = sum_k dv[seg + k] * M[k * mw + n]
+__device__ __forceinline__ double seg_matvec(const double *dv, int segbase, const double *M, int mw,
+                                             int n) {
+  double s = 0.0;
+  int k = 0;
+  for (; k + 4 <= mw; k += 4) {
+    double m0 = __ldg(M + (size_t)k * mw + n), m1 = __ldg(M + (size_t)(k + 1) * mw + n);
+    double m2 = __ldg(M + (size_t)(k + 2) * mw + n), m3 = __ldg(M + (size_t)(k + 3) * mw + n);
+    s += dv[segbase + k] * m0;
+    s += dv[segbase + k + 1] * m1;
+    s += dv[segbase + k + 2] * m2;
+    s += dv[segbase + k + 3] * m3;
+  }
+  for (; k < mw; ++k) s += dv[segbase + k] * __ldg(M + (size_t)k * mw + n);
+  return s;
+}
+
+// UPDATE: fused x += alpha p, r -= alpha q before preconditioning (pass B).
+// DOTS:   accumulate r.z and r.r and finish the iteration on the device.
+template <typename V, bool UPDATE, bool DOTS>
+__global__ void __launch_bounds__(kTileWarps * 32)
+    k_tile_apply(TileGeom tg, Coeffs c, const double *__restrict__ mats, V *x, const V *p, V *r,
+                 const V *q, V *z, SolveState *st, double *partials, unsigned *ticket) {
+  if (DOTS && st->done) return;
+  extern __shared__ __align__(16) unsigned char tsm[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const size_t per_warp = tile_smem_per_warp(tg.hmax, tg.nbmax, sizeof(V));
+  unsigned char *base = tsm + per_warp * wib;
+  double *zs = (double *)base;
+  V *rs = (V *)(base + (size_t)tg.hmax * 32 * 8);
+  double *rho_s = (double *)(base + (size_t)tg.hmax * 32 * (8 + sizeof(V)));
+  double *u0_s = rho_s + (size_t)tg.nbmax * 32;
+  double *dv = u0_s + (size_t)tg.nbmax * 32;
+
+  double acc_rz = 0.0, acc_rr = 0.0;
+  const int gw = blockIdx.x * kTileWarps + wib;
+  const int b = gw / tg.txg;
+  if (b < tg.ty) {
+    const int grp = gw - b * tg.txg;
+    const int seg = lane / tg.wseg, n = lane - seg * tg.wseg, segbase = seg * tg.wseg;
+    const int a = grp * tg.tpw + seg;
+    const int mw = (a < tg.tx) ? tile_width(tg, a) : 0;
+    const bool active = n < mw;
+    const int nx = tg.nx;
+    const int j0 = b * tg.th, hh = tile_height(tg, b), nb = tg.row_nb[b];
+    const int i = a * tg.tm + n;
+    const double *mt = mats + (mw > 0 ? tg.moff[(size_t)b * tg.tx + a] : 0);
+    const size_t msz = (size_t)mw * mw;
+    double alpha = 0.0;
+    if (UPDATE) alpha = st->alpha;
+
+    // ---- forward sweep: particular solution with zero guess rows and
+    //      block-top corrections (the elimination of the SEVP system)
+    double zb = 0.0, zc = 0.0;
+    int t = 0, kb = 0, ke = sub_start(1, hh, nb) - 1;
+    for (int k = 0; k < hh; ++k) {
+      const size_t idx = (size_t)(j0 + k) * nx + i;
+      double rv = 0.0, cw = 0.0, cs = 0.0, cc = 0.0, ce = 0.0, cn = 1.0;
+      if (active) {
+        if (UPDATE) {
+          V xv = x[idx], pv = p[idx], rov = r[idx], qv = q[idx];
+          V xn = xv + (V)alpha * pv;
+          V rn = rov - (V)alpha * qv;
+          x[idx] = xn;
+          r[idx] = rn;
+          rv = (double)rn;
+        } else {
+          rv = (double)r[idx];
+        }
+        cw = __ldg(c.al + idx);
+        cs = __ldg(c.ab + idx);
+        cc = __ldg(c.ac + idx);
+        ce = __ldg(c.ar + idx);
+        cn = __ldg(c.at + idx);
+        acc_rr += rv * rv;
+      }
+      rs[k * 32 + lane] = (V)rv;
+      if (k == kb) zc = 0.0;
+      zs[k * 32 + lane] = zc;
+      double zw = __shfl_up_sync(0xffffffffu, zc, 1);
+      double ze = __shfl_down_sync(0xffffffffu, zc, 1);
+      if (n == 0) zw = 0.0;
+      if (n >= mw - 1) ze = 0.0;
+      if (k < ke) {
+        double zn = active ? ((((rv - cw * zw) - cs * zb) - cc * zc) - ce * ze) / cn : 0.0;
+        zb = zc;
+        zc = zn;
+      } else {
+        double rho = active ? (((rv - cw * zw) - cs * zb) - cc * zc) - ce * ze : 0.0;
+        rho_s[t * 32 + lane] = rho;
+        u0_s[t * 32 + lane] = zc;
+        if (t < nb - 1) {
+          dv[lane] = rho;
+          __syncwarp();
+          double s = active ? seg_matvec(dv, segbase, mt + (size_t)(nb + t) * msz, mw, n) : 0.0;
+          __syncwarp();
+          zc = zc - s;
+          zs[k * 32 + lane] = zc;
+        }
+        zb = zc;
+        ++t;
+        kb = k + 1;
+        ke = sub_start(t + 1, hh, nb) - 1;
+      }
+    }
+    // ---- backward sweep: guess-row values and homogeneous corrections
+    double vnext = 0.0;
+    for (t = nb - 1; t >= 0; --t) {
+      kb = sub_start(t, hh, nb);
+      ke = sub_start(t + 1, hh, nb) - 1;
+      if (t < nb - 1) zs[ke * 32 + lane] = u0_s[t * 32 + lane];
+      double cnk = active ? (double)__ldg(c.at + (size_t)(j0 + ke) * nx + i) : 0.0;
+      dv[lane] = rho_s[t * 32 + lane] - cnk * vnext;
+      __syncwarp();
+      double v = active ? seg_matvec(dv, segbase, mt + (size_t)t * msz, mw, n) : 0.0;
+      __syncwarp();
+      zs[kb * 32 + lane] += v;
+      double hb = 0.0, hc = v;
+      if (t > 0) {
+        double cnb = active ? (double)__ldg(c.at + (size_t)(j0 + kb - 1) * nx + i) : 0.0;
+        dv[lane] = v * cnb;
+        __syncwarp();
+        hb = active ? seg_matvec(dv, segbase, mt + (size_t)(nb + t - 1) * msz, mw, n) : 0.0;
+        __syncwarp();
+      }
+      for (int k = kb; k < ke; ++k) {
+        const size_t idx = (size_t)(j0 + k) * nx + i;
+        double hw = __shfl_up_sync(0xffffffffu, hc, 1);
+        double he = __shfl_down_sync(0xffffffffu, hc, 1);
+        if (n == 0) hw = 0.0;
+        if (n >= mw - 1) he = 0.0;
+        double hn = 0.0;
+        if (active) {
+          double cw = __ldg(c.al + idx), cs = __ldg(c.ab + idx), cc = __ldg(c.ac + idx);
+          double ce = __ldg(c.ar + idx), cn = __ldg(c.at + idx);
+          hn = ((((-(cw * hw)) - cs * hb) - cc * hc) - ce * he) / cn;
+        }
+        zs[(k + 1) * 32 + lane] += hn;
+        hb = hc;
+        hc = hn;
+      }
+      if (active)
+        for (int k = kb; k <= ke; ++k) {
+          V zv = (V)zs[k * 32 + lane];
+          z[(size_t)(j0 + k) * nx + i] = zv;
+          if (DOTS) acc_rz += (double)rs[k * 32 + lane] * (double)zv;
+        }
+      vnext = v;
+    }
+  }
+  if (DOTS) {
+    double v2[2] = {acc_rz, acc_rr};
+    struct Fin {
+      SolveState *st;
+      __device__ void operator()(double (&s)[2]) {
+        double rz = s[0], rr = s[1];
+        int first = (st->beta == 0.0 && st->iter == 0);
+        st->rr = rr;
+        if (!isfinite(rz) || !isfinite(rr)) {
+          st->status = SEVP_NONFINITE;
+          st->done = 1;
+          return;
+        }
+        if (rr <= st->tol2 * st->bb) {
+          st->done = 1;
+          st->status = SEVP_OK;
+          st->rz = rz;
+          return;
+        }
+        if (st->iter >= st->max_iter) {
+          st->done = 1;
+          st->status = SEVP_MAXITER;
+          st->rz = rz;
+          return;
+        }
+        if (rz == 0.0) {
+          st->status = SEVP_BREAKDOWN;
+          st->done = 1;
+          return;
+        }
+        st->beta = first ? 0.0 : rz / st->rz;
+        st->rz = rz;
+      }
+    } fin{st};
+    reduce_and_finish<2>(v2, partials, ticket, fin);
+  }
+}
+
+// -------------------------------------------------- tile precompute
+// One CTA per tile, 32 warps; warp g marches the response to a unit guess
+// value in column g.  Coefficients are staged in shared memory.  The
+// guess-row -> last-equation map of each sub-block is inverted by
+// Gauss-Jordan elimination with partial pivoting.
+__global__ void __launch_bounds__(1024)
+    k_tile_precompute(TileGeom tg, Coeffs c, double *mats, int *status) {
+  extern __shared__ __align__(16) unsigned char psm[];
+  const int tile = blockIdx.x;
+  const int a = tile % tg.tx, b = tile / tg.tx;
+  const int mw = tile_width(tg, a), hh = tile_height(tg, b), nb = tg.row_nb[b];
+  const int i0 = a * tg.tm, j0 = b * tg.th;
+  const int lane = threadIdx.x & 31, g = threadIdx.x >> 5;
+  const int TM = 32;
+  float *cf = (float *)psm;  // [5][hmax][32]
+  const int hm = tg.hmax;
+  double *S = (double *)(psm + (size_t)5 * hm * TM * sizeof(float));  // [32][32]
+  double *P = S + TM * TM;
+  double *Aug = P + TM * TM;   // [32][64]
+  double *R1p = Aug + TM * 2 * TM;
+  double *fac = R1p + TM * TM;  // [32]
+  __shared__ int s_piv;
+  __shared__ double s_pval;
+  __shared__ int s_bad;
+  if (threadIdx.x == 0) s_bad = 0;
+  for (int e = threadIdx.x; e < hh * TM; e += blockDim.x) {
+    int k = e / TM, n = e % TM;
+    float w = 0.f, s = 0.f, cc = 0.f, ee = 0.f, nn = 0.f;
+    if (n < mw) {
+      size_t idx = (size_t)(j0 + k) * tg.nx + i0 + n;
+      w = c.al[idx], s = c.ab[idx], cc = c.ac[idx], ee = c.ar[idx], nn = c.at[idx];
+    }
+    cf[(0 * hm + k) * TM + n] = w;
+    cf[(1 * hm + k) * TM + n] = s;
+    cf[(2 * hm + k) * TM + n] = cc;
+    cf[(3 * hm + k) * TM + n] = ee;
+    cf[(4 * hm + k) * TM + n] = nn;
+  }
+  __syncthreads();
+  const size_t msz = (size_t)mw * mw;
+  double *mt = mats + tg.moff[(size_t)b * tg.tx + a];
+#define CF(q, k, n) ((double)cf[((q) * hm + (k)) * TM + (n)])
+  for (int t = 0; t < nb; ++t) {
+    const int kb = sub_start(t, hh, nb), ke = sub_start(t + 1, hh, nb) - 1;
+    if (g < mw) {
+      const int n = lane;
+      double hb = (t > 0 && n < mw) ? R1p[g * TM + n] * CF(4, kb - 1, g) : 0.0;
+      double hc = (n == g) ? 1.0 : 0.0;
+      for (int k = kb; k < ke; ++k) {
+        double hw = __shfl_up_sync(0xffffffffu, hc, 1);
+        double he = __shfl_down_sync(0xffffffffu, hc, 1);
+        if (n == 0) hw = 0.0;
+        if (n >= mw - 1) he = 0.0;
+        double hn = 0.0;
+        if (n < mw)
+          hn = -((((CF(0, k, n) * hw) + CF(1, k, n) * hb) + CF(2, k, n) * hc) + CF(3, k, n) * he) /
+               CF(4, k, n);
+        hb = hc;
+        hc = hn;
+      }
+      double hw = __shfl_up_sync(0xffffffffu, hc, 1);
+      double he = __shfl_down_sync(0xffffffffu, hc, 1);
+      if (n == 0) hw = 0.0;
+      if (n >= mw - 1) he = 0.0;
+      if (n < mw) {
+        S[g * TM + n] =
+            (((CF(0, ke, n) * hw) + CF(1, ke, n) * hb) + CF(2, ke, n) * hc) + CF(3, ke, n) * he;
+        P[g * TM + n] = hc;
+      }
+    }
+    __syncthreads();
+    // Gauss-Jordan on [S | I]
+    for (int e = threadIdx.x; e < TM * 2 * TM; e += blockDim.x) {
+      int r = e / (2 * TM), cix = e % (2 * TM);
+      double v = 0.0;
+      if (r < mw) {
+        if (cix < mw) v = S[r * TM + cix];
+        else if (cix >= TM && cix - TM < mw) v = (cix - TM == r) ? 1.0 : 0.0;
+      }
+      Aug[r * 2 * TM + cix] = v;
+    }
+    __syncthreads();
+    for (int k = 0; k < mw; ++k) {
+      if (g == 0) {
+        double av = (lane >= k && lane < mw) ? fabs(Aug[lane * 2 * TM + k]) : -1.0;
+        int ai = lane;
+        for (int o = 16; o > 0; o >>= 1) {
+          double ov = __shfl_down_sync(0xffffffffu, av, o);
+          int oi = __shfl_down_sync(0xffffffffu, ai, o);
+          if (ov > av || (ov == av && oi < ai)) av = ov, ai = oi;
+        }
+        if (lane == 0) {
+          s_piv = ai;
+          s_pval = av;
+        }
+      }
+      __syncthreads();
+      const int piv = s_piv;
+      if (!(s_pval > 0.0) || !isfinite(s_pval)) {
+        if (threadIdx.x == 0) s_bad = 1;
+      }
+      if (piv != k) {
+        for (int cix = threadIdx.x; cix < 2 * TM; cix += blockDim.x) {
+          double t0 = Aug[k * 2 * TM + cix];
+          Aug[k * 2 * TM + cix] = Aug[piv * 2 * TM + cix];
+          Aug[piv * 2 * TM + cix] = t0;
+        }
+      }
+      __syncthreads();
+      double pv = Aug[k * 2 * TM + k];
+      double inv = (pv != 0.0) ? 1.0 / pv : 0.0;
+      if (threadIdx.x < TM) fac[threadIdx.x] = Aug[threadIdx.x * 2 * TM + k];
+      __syncthreads();
+      for (int cix = threadIdx.x; cix < 2 * TM; cix += blockDim.x) Aug[k * 2 * TM + cix] *= inv;
+      __syncthreads();
+      for (int e = threadIdx.x; e < mw * 2 * TM; e += blockDim.x) {
+        int r = e / (2 * TM), cix = e % (2 * TM);
+        if (r != k) {
+          double f = fac[r];
+          if (f != 0.0) Aug[r * 2 * TM + cix] -= f * Aug[k * 2 * TM + cix];
+        }
+      }
+      __syncthreads();
+    }
+    // Sinv_t -> global; R1_t = -Sinv_t P -> global and shared (next sub-block)
+    for (int e = threadIdx.x; e < mw * mw; e += blockDim.x) {
+      int r = e / mw, cix = e % mw;
+      mt[(size_t)t * msz + e] = Aug[r * 2 * TM + TM + cix];
+    }
+    if (t < nb - 1) {
+      for (int e = threadIdx.x; e < mw * mw; e += blockDim.x) {
+        int r = e / mw, cix = e % mw;
+        double s = 0.0;
+        for (int k = 0; k < mw; ++k) s = s - Aug[r * 2 * TM + TM + k] * P[k * TM + cix];
+        mt[(size_t)(nb + t) * msz + e] = s;
+        R1p[r * TM + cix] = s;
+      }
+    }
+    __syncthreads();
+  }
+#undef CF
+  if (threadIdx.x == 0 && s_bad) atomicOr(status, 1);
+}
+
+}  // namespace sevp
+
+// ======================================================================
+// context
+// ======================================================================
+using namespace sevp;
+
+struct sevp_ctx {
+  int nx = 0, ny = 0, periodic = 0;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  Coeffs c{};
+  bool have_op = false;
+  // tiles
+  TileGeom tg{};
+  int *d_row_nb = nullptr;
+  long long *d_moff = nullptr;
+  double *d_mats = nullptr;
+  long long mats_elems = 0;
+  std::vector<int> row_nb;
+  // work vectors
+  size_t n = 0;
+  double *r64 = nullptr, *z64 = nullptr, *p64[2] = {nullptr, nullptr}, *q64 = nullptr;
+  double *x64s = nullptr;  // ping-pong partner for the refinement update
+  float *r32 = nullptr, *z32 = nullptr, *p32[2] = {nullptr, nullptr}, *q32 = nullptr,
+        *d32 = nullptr;
+  double *bh = nullptr;  // device staging for host solves
+  double *xh = nullptr;
+  // device scalars
+  SolveState *st = nullptr;
+  SolveState *h_st = nullptr;  // pinned mirror
+  double *partials = nullptr;
+  size_t partials_n = 0;
+  unsigned *tickets = nullptr;
+  long long launches = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace {
+thread_local char g_err[512] = {0};
+}
+void sevp_internal_set_error(cudaError_t e, const char *what, const char *file, int line) {
+  snprintf(g_err, sizeof g_err, "%s: %s (%s:%d)", cudaGetErrorString(e), what, file, line);
+}
+extern "C" const char *sevp_last_error(void) { return g_err; }
+
+extern "C" const char *sevp_status_string(int s) {
+  switch (s) {
+    case SEVP_OK: return "ok";
+    case SEVP_MAXITER: return "iteration cap reached";
+    case SEVP_BREAKDOWN: return "Krylov breakdown";
+    case SEVP_NONFINITE: return "non-finite value";
+    case SEVP_TIMEOUT: return "device wait timed out";
+    case SEVP_BAD_ARG: return "bad argument";
+    case SEVP_CUDA_ERROR: return "CUDA error";
+    case SEVP_SINGULAR: return "singular influence matrix";
+    default: return "unknown status";
+  }
+}
+
+static int stencil_rpw(int ny) { return ny >= 2048 ? 32 : 16; }
+
+static dim3 stencil_grid(const sevp_ctx *ctx, int rpw) {
+  return dim3((unsigned)ceil_div(ctx->nx, 32), (unsigned)ceil_div(ctx->ny, rpw * (kStencilThreads / 32)));
+}
+
+static size_t tile_warps(const TileGeom &tg) { return (size_t)tg.ty * tg.txg; }
+
+template <class Op>
+static int launch_stencil(sevp_ctx *ctx, const Op &op, int ticket_slot) {
+  int rpw = stencil_rpw(ctx->ny);
+  dim3 grid = stencil_grid(ctx, rpw);
+  GridDims gd{ctx->nx, ctx->ny, ctx->periodic};
+  k_stencil<Op><<<grid, kStencilThreads, 0, ctx->stream>>>(gd, ctx->c, op, rpw, ctx->partials,
+                                                          ctx->tickets + ticket_slot, ctx->st);
+  ctx->launches++;
+  SEVP_CUDA_TRY(cudaGetLastError());
+  return SEVP_OK;
+}
+
+template <typename V, bool UPDATE, bool DOTS>
+static int launch_tile(sevp_ctx *ctx, V *x, const V *p, V *r, const V *q, V *z, int ticket_slot) {
+  size_t warps = tile_warps(ctx->tg);
+  unsigned blocks = (unsigned)((warps + kTileWarps - 1) / kTileWarps);
+  size_t smem = tile_smem_per_warp(ctx->tg.hmax, ctx->tg.nbmax, sizeof(V)) * kTileWarps;
+  auto kern = k_tile_apply<V, UPDATE, DOTS>;
+  static thread_local size_t set_smem[8] = {0};
+  const int key = (sizeof(V) == 8 ? 4 : 0) + (UPDATE ? 2 : 0) + (DOTS ? 1 : 0);
+  if (smem > 48 * 1024 && set_smem[key] < smem) {
+    SEVP_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    set_smem[key] = smem;
+  }
+  kern<<<blocks, kTileWarps * 32, smem, ctx->stream>>>(ctx->tg, ctx->c, ctx->d_mats, x, p, r, q, z,
+                                                      ctx->st, ctx->partials,
+                                                      ctx->tickets + ticket_slot);
+  ctx->launches++;
+  SEVP_CUDA_TRY(cudaGetLastError());
+  return SEVP_OK;
+}
+
+static void free_work(sevp_ctx *ctx) {
+  void *ptrs[] = {ctx->r64, ctx->z64, ctx->p64[0], ctx->p64[1], ctx->q64, ctx->x64s, ctx->r32,
+                  ctx->z32, ctx->p32[0], ctx->p32[1], ctx->q32, ctx->d32, ctx->bh, ctx->xh,
+                  ctx->d_row_nb, ctx->d_moff, ctx->d_mats, ctx->st, ctx->partials, ctx->tickets};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  if (ctx->h_st) cudaFreeHost(ctx->h_st);
+}
+
+extern "C" int sevp_create(sevp_ctx **out, int nx, int ny, int periodic, void *stream) {
+  if (!out || nx < 1 || ny < 1) return SEVP_BAD_ARG;
+  *out = nullptr;
+  sevp_ctx *ctx = new sevp_ctx();
+  ctx->nx = nx, ctx->ny = ny, ctx->periodic = periodic ? 1 : 0;
+  ctx->stream = (cudaStream_t)stream;
+  ctx->n = (size_t)nx * ny;
+  cudaGetDevice(&ctx->device);
+  size_t n = ctx->n;
+  auto fail = [&](cudaError_t e, const char *w) {
+    sevp_internal_set_error(e, w, __FILE__, __LINE__);
+    free_work(ctx);
+    delete ctx;
+    return SEVP_CUDA_ERROR;
+  };
+  cudaError_t e;
+#define ALLOC(ptr, bytes)                                          \
+  e = cudaMalloc((void **)&(ptr), (bytes));                        \
+  if (e != cudaSuccess) return fail(e, "cudaMalloc " #ptr);        \
+  e = cudaMemsetAsync((ptr), 0, (bytes), ctx->stream);             \
+  if (e != cudaSuccess) return fail(e, "cudaMemset " #ptr);
+  ALLOC(ctx->r64, n * 8);
+  ALLOC(ctx->z64, n * 8);
+  ALLOC(ctx->p64[0], n * 8);
+  ALLOC(ctx->p64[1], n * 8);
+  ALLOC(ctx->q64, n * 8);
+  ALLOC(ctx->x64s, n * 8);
+  ALLOC(ctx->r32, n * 4);
+  ALLOC(ctx->z32, n * 4);
+  ALLOC(ctx->p32[0], n * 4);
+  ALLOC(ctx->p32[1], n * 4);
+  ALLOC(ctx->q32, n * 4);
+  ALLOC(ctx->d32, n * 4);
+  ALLOC(ctx->st, sizeof(SolveState));
+  ALLOC(ctx->tickets, 16 * sizeof(unsigned));
+  // partial sums: enough for the larger of the stencil and tile grids
+  size_t sgrid = (size_t)ceil_div(nx, 32) * ceil_div(ny, 16 * 8);
+  size_t tgrid = (size_t)ceil_div(nx, 1) * ceil_div(ny, 1) / (kTileWarps) + 1024;
+  ctx->partials_n = std::max(sgrid, tgrid) * 2 + 64;
+  ALLOC(ctx->partials, ctx->partials_n * 8);
+#undef ALLOC
+  e = cudaMallocHost((void **)&ctx->h_st, sizeof(SolveState));
+  if (e != cudaSuccess) return fail(e, "cudaMallocHost");
+  cudaEventCreate(&ctx->ev0);
+  cudaEventCreate(&ctx->ev1);
+  e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return fail(e, "sync");
+  *out = ctx;
+  return SEVP_OK;
+}
+
+extern "C" int sevp_destroy(sevp_ctx *ctx) {
+  if (!ctx) return SEVP_OK;
+  cudaStreamSynchronize(ctx->stream);
+  free_work(ctx);
+  if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+  if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  delete ctx;
+  return SEVP_OK;
+}
+
+extern "C" long long sevp_kernel_launches(const sevp_ctx *ctx) { return ctx ? ctx->launches : 0; }
+extern "C" long long sevp_influence_bytes(const sevp_ctx *ctx) {
+  return ctx ? ctx->mats_elems * 8 : 0;
+}
+
+extern "C" int sevp_set_operator(sevp_ctx *ctx, const float *al, const float *ab, const float *ac,
+                                 const float *ar, const float *at, const sevp_tiling *tl) {
+  if (!ctx || !al || !ab || !ac || !ar || !at || !tl) return SEVP_BAD_ARG;
+  const int tm = tl->tile_m, th = tl->tile_h;
+  if (tm < 1 || tm > 32 || th < 1 || th > 32 || tl->sub_rows < 1) return SEVP_BAD_ARG;
+  ctx->c = Coeffs{al, ab, ac, ar, at};
+  TileGeom &tg = ctx->tg;
+  tg.nx = ctx->nx, tg.ny = ctx->ny, tg.tm = tm, tg.th = th;
+  tg.tx = ceil_div(ctx->nx, tm);
+  tg.ty = ceil_div(ctx->ny, th);
+  tg.wseg = tm <= 8 ? 8 : (tm <= 16 ? 16 : 32);
+  tg.tpw = 32 / tg.wseg;
+  tg.txg = ceil_div(tg.tx, tg.tpw);
+  tg.hmax = th;
+  ctx->row_nb.assign(tg.ty, 1);
+  int nbmax = 1;
+  for (int b = 0; b < tg.ty; ++b) {
+    int s = tl->sub_rows_by_tile_row ? tl->sub_rows_by_tile_row[b] : tl->sub_rows;
+    if (s < 1) return SEVP_BAD_ARG;
+    int hh = tile_height(tg, b);
+    int nb = ceil_div(hh, s);
+    ctx->row_nb[b] = nb;
+    nbmax = std::max(nbmax, nb);
+  }
+  tg.nbmax = nbmax;
+  std::vector<long long> moff((size_t)tg.ty * tg.tx);
+  long long off = 0;
+  for (int b = 0; b < tg.ty; ++b)
+    for (int a = 0; a < tg.tx; ++a) {
+      int mw = tile_width(tg, a), nb = ctx->row_nb[b];
+      moff[(size_t)b * tg.tx + a] = off;
+      off += (long long)(2 * nb - 1) * mw * mw;
+    }
+  ctx->mats_elems = off;
+  if (ctx->d_row_nb) cudaFree(ctx->d_row_nb), ctx->d_row_nb = nullptr;
+  if (ctx->d_moff) cudaFree(ctx->d_moff), ctx->d_moff = nullptr;
+  if (ctx->d_mats) cudaFree(ctx->d_mats), ctx->d_mats = nullptr;
+  SEVP_CUDA_TRY(cudaMalloc((void **)&ctx->d_row_nb, sizeof(int) * tg.ty));
+  SEVP_CUDA_TRY(cudaMalloc((void **)&ctx->d_moff, sizeof(long long) * moff.size()));
+  SEVP_CUDA_TRY(cudaMalloc((void **)&ctx->d_mats, sizeof(double) * std::max<long long>(off, 1)));
+  SEVP_CUDA_TRY(cudaMemcpyAsync(ctx->d_row_nb, ctx->row_nb.data(), sizeof(int) * tg.ty,
+                                cudaMemcpyHostToDevice, ctx->stream));
+  SEVP_CUDA_TRY(cudaMemcpyAsync(ctx->d_moff, moff.data(), sizeof(long long) * moff.size(),
+                                cudaMemcpyHostToDevice, ctx->stream));
+  tg.row_nb = ctx->d_row_nb;
+  tg.moff = ctx->d_moff;
+  // partial-sum capacity for the tile grid
+  size_t tblocks = (tile_warps(tg) + kTileWarps - 1) / kTileWarps;
+  if (tblocks * 2 + 64 > ctx->partials_n) {
+    cudaFree(ctx->partials);
+    ctx->partials_n = tblocks * 2 + 64;
+    SEVP_CUDA_TRY(cudaMalloc((void **)&ctx->partials, ctx->partials_n * 8));
+  }
+  // tile-apply shared memory must fit
+  size_t smem64 = tile_smem_per_warp(tg.hmax, tg.nbmax, 8) * kTileWarps;
+  if (smem64 > 220 * 1024) return SEVP_BAD_ARG;
+  // precompute
+  int *d_status = nullptr;
+  SEVP_CUDA_TRY(cudaMalloc((void **)&d_status, sizeof(int)));
+  SEVP_CUDA_TRY(cudaMemsetAsync(d_status, 0, sizeof(int), ctx->stream));
+  size_t psmem = (size_t)5 * tg.hmax * 32 * sizeof(float) + (size_t)(32 * 32 * 3 + 32 * 64 + 32) * 8;
+  SEVP_CUDA_TRY(cudaFuncSetAttribute(k_tile_precompute, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)psmem));
+  k_tile_precompute<<<tg.ty * tg.tx, 1024, psmem, ctx->stream>>>(tg, ctx->c, ctx->d_mats, d_status);
+  ctx->launches++;
+  SEVP_CUDA_TRY(cudaGetLastError());
+  int h_status = 0;
+  SEVP_CUDA_TRY(cudaMemcpyAsync(&h_status, d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  SEVP_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  cudaFree(d_status);
+  ctx->have_op = true;
+  return h_status ? SEVP_SINGULAR : SEVP_OK;
+}
+
+extern "C" int sevp_apply(sevp_ctx *ctx, const double *x, double *y) {
+  if (!ctx || !ctx->have_op || !x || !y) return SEVP_BAD_ARG;
+  OpApply<double> op{x, y};
+  return launch_stencil(ctx, op, 0);
+}
+
+extern "C" int sevp_precondition(sevp_ctx *ctx, const double *r, double *z) {
+  if (!ctx || !ctx->have_op || !r || !z) return SEVP_BAD_ARG;
+  return launch_tile<double, false, false>(ctx, nullptr, nullptr, const_cast<double *>(r), nullptr,
+                                           z, 1);
+}
+
+extern "C" int sevp_precondition_f32(sevp_ctx *ctx, const float *r, float *z) {
+  if (!ctx || !ctx->have_op || !r || !z) return SEVP_BAD_ARG;
+  return launch_tile<float, false, false>(ctx, nullptr, nullptr, const_cast<float *>(r), nullptr, z,
+                                          1);
+}
+
+static int read_state(sevp_ctx *ctx) {
+  SEVP_CUDA_TRY(cudaMemcpyAsync(ctx->h_st, ctx->st, sizeof(SolveState), cudaMemcpyDeviceToHost,
+                                ctx->stream));
+  SEVP_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return SEVP_OK;
+}
+
+// Residual pass: xout = x + d; r = b - A xout; ||r||^2, ||b||^2 into state.
+template <typename R>
+static int launch_residual(sevp_ctx *ctx, const double *x, const float *d, double *xout,
+                           const double *b, R *r, int set_inner, double tol2) {
+  OpResidual<R> op{x, d, xout, b, r, ctx->st, tol2, set_inner};
+  return launch_stencil(ctx, op, 2);
+}
+
+__global__ void k_state_init(SolveState *st, double tol2, int max_iter) {
+  SolveState s{};
+  s.tol2 = tol2;
+  s.max_iter = max_iter;
+  s.status = SEVP_OK;
+  *st = s;
+}
+
+// Copies the residual-pass norms into the PCG stopping reference.
+__global__ void k_state_from_residual(SolveState *st) {
+  st->bb = st->bb64;
+  st->rr = st->rr64;
+  st->iter = 0;
+  st->done = 0;
+  st->beta = 0.0;
+}
+
+// Runs PCG iterations on vectors of type V until the device state says done.
+// x, r hold the iterate and residual; the first z = M^{-1} r must already be
+// in place (with rz, beta = 0 set).  Returns iterations done.
+template <typename V>
+static int pcg_loop(sevp_ctx *ctx, V *x, V *r, V *z, V *p0, V *p1, V *q, int check_every,
+                    int *iters_out) {
+  V *pp[2] = {p0, p1};
+  int cur = 0;
+  for (;;) {
+    for (int k = 0; k < check_every; ++k) {
+      OpPassA<V> op{z, pp[cur], pp[cur ^ 1], q, ctx->st};
+      int s = launch_stencil(ctx, op, 3);
+      if (s) return s;
+      s = launch_tile<V, true, true>(ctx, x, pp[cur ^ 1], r, q, z, 4);
+      if (s) return s;
+      cur ^= 1;
+    }
+    int s = read_state(ctx);
+    if (s) return s;
+    if (ctx->h_st->done) break;
+  }
+  *iters_out = ctx->h_st->iter;
+  return SEVP_OK;
+}
+
+static int solve_fp64(sevp_ctx *ctx, const double *b, double *x, const sevp_solve_opts *o,
+                      sevp_report *rep) {
+  const double tol2 = o->tol * o->tol;
+  int total = 0, status = SEVP_OK;
+  for (int restart = 0; restart < 6; ++restart) {
+    k_state_init<<<1, 1, 0, ctx->stream>>>(ctx->st, tol2, std::max(o->max_iter - total, 0));
+    ctx->launches++;
+    // r = b - A x
+    int s = launch_residual<double>(ctx, x, nullptr, nullptr, b, ctx->r64, 0, tol2);
+    if (s) return s;
+    k_state_from_residual<<<1, 1, 0, ctx->stream>>>(ctx->st);
+    ctx->launches++;
+    s = read_state(ctx);
+    if (s) return s;
+    if (!std::isfinite(ctx->h_st->rr64) || !std::isfinite(ctx->h_st->bb64)) return SEVP_NONFINITE;
+    double rel = ctx->h_st->bb64 > 0 ? sqrt(ctx->h_st->rr64 / ctx->h_st->bb64) : 0.0;
+    rep->bnorm = sqrt(ctx->h_st->bb64);
+    rep->rel_residual = rel;
+    rep->refinements++;
+    if (rel <= o->tol || ctx->h_st->bb64 == 0.0) {
+      status = SEVP_OK;
+      break;
+    }
+    if (total >= o->max_iter) {
+      status = SEVP_MAXITER;
+      break;
+    }
+    // z = M^{-1} r, rz; then iterate
+    s = launch_tile<double, false, true>(ctx, nullptr, nullptr, ctx->r64, nullptr, ctx->z64, 4);
+    if (s) return s;
+    int it = 0;
+    s = pcg_loop<double>(ctx, x, ctx->r64, ctx->z64, ctx->p64[0], ctx->p64[1], ctx->q64,
+                         std::max(1, o->check_every), &it);
+    if (s) return s;
+    total += it;
+    status = ctx->h_st->status;
+    if (status != SEVP_OK && status != SEVP_MAXITER) break;
+  }
+  rep->iterations = total;
+  return status;
+}
+
+// FP32 PCG inside FP64 iterative refinement.
+static int solve_mixed(sevp_ctx *ctx, const double *b, double *x, const sevp_solve_opts *o,
+                       sevp_report *rep) {
+  const double inner2 = o->inner_tol * o->inner_tol;
+  int total = 0, status = SEVP_MAXITER;
+  double *xa = x, *xb = ctx->x64s;  // ping-pong: the residual kernel reads xa, writes xb
+  bool have_d = false;
+  for (int refine = 0; refine < 64; ++refine) {
+    k_state_init<<<1, 1, 0, ctx->stream>>>(ctx->st, inner2, std::max(o->max_iter - total, 0));
+    ctx->launches++;
+    int s;
+    if (have_d)
+      s = launch_residual<float>(ctx, xa, ctx->d32, xb, b, ctx->r32, 1, inner2);
+    else
+      s = launch_residual<float>(ctx, xa, nullptr, nullptr, b, ctx->r32, 1, inner2);
+    if (s) return s;
+    if (have_d) std::swap(xa, xb);
+    s = read_state(ctx);
+    if (s) return s;
+    if (!std::isfinite(ctx->h_st->rr64) || !std::isfinite(ctx->h_st->bb64)) {
+      status = SEVP_NONFINITE;
+      break;
+    }
+    double rel = ctx->h_st->bb64 > 0 ? sqrt(ctx->h_st->rr64 / ctx->h_st->bb64) : 0.0;
+    rep->bnorm = sqrt(ctx->h_st->bb64);
+    rep->rel_residual = rel;
+    rep->refinements++;
+    if (rel <= o->tol || ctx->h_st->bb64 == 0.0) {
+      status = SEVP_OK;
+      break;
+    }
+    if (total >= o->max_iter) {
+      status = SEVP_MAXITER;
+      break;
+    }
+    // inner solve A d = r32 from d = 0
+    SEVP_CUDA_TRY(cudaMemsetAsync(ctx->d32, 0, ctx->n * 4, ctx->stream));
+    s = launch_tile<float, false, true>(ctx, nullptr, nullptr, ctx->r32, nullptr, ctx->z32, 4);
+    if (s) return s;
+    int it = 0;
+    s = pcg_loop<float>(ctx, ctx->d32, ctx->r32, ctx->z32, ctx->p32[0], ctx->p32[1], ctx->q32,
+                        std::max(1, o->check_every), &it);
+    if (s) return s;
+    total += it;
+    have_d = true;
+    int ist = ctx->h_st->status;
+    if (ist != SEVP_OK && ist != SEVP_MAXITER) {
+      status = ist;
+      break;
+    }
+  }
+  if (xa != x) SEVP_CUDA_TRY(cudaMemcpyAsync(x, xa, ctx->n * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+  rep->iterations = total;
+  return status;
+}
+
+extern "C" int sevp_solve(sevp_ctx *ctx, const double *b, double *x, const sevp_solve_opts *o,
+                          sevp_report *rep) {
+  if (!ctx || !ctx->have_op || !b || !x || !o) return SEVP_BAD_ARG;
+  if (!(o->tol > 0.0) || o->max_iter < 0 || (o->precision != 0 && o->precision != 1))
+    return SEVP_BAD_ARG;
+  if (o->precision == 1 && !(o->inner_tol > 0.0 && o->inner_tol < 1.0)) return SEVP_BAD_ARG;
+  sevp_report local{};
+  sevp_report *r = rep ? rep : &local;
+  *r = sevp_report{};
+  if (!o->use_guess) SEVP_CUDA_TRY(cudaMemsetAsync(x, 0, ctx->n * 8, ctx->stream));
+  SEVP_CUDA_TRY(cudaEventRecord(ctx->ev0, ctx->stream));
+  int s = o->precision == 0 ? solve_fp64(ctx, b, x, o, r) : solve_mixed(ctx, b, x, o, r);
+  SEVP_CUDA_TRY(cudaEventRecord(ctx->ev1, ctx->stream));
+  SEVP_CUDA_TRY(cudaEventSynchronize(ctx->ev1));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  r->ms = ms;
+  r->status = s;
+  return s;
+}
+
+extern "C" int sevp_solve_host(sevp_ctx *ctx, const double *bh, double *xh,
+                               const sevp_solve_opts *o, sevp_report *rep) {
+  if (!ctx || !bh || !xh || !o) return SEVP_BAD_ARG;
+  if (!ctx->bh) SEVP_CUDA_TRY(cudaMalloc((void **)&ctx->bh, ctx->n * 8));
+  if (!ctx->xh) SEVP_CUDA_TRY(cudaMalloc((void **)&ctx->xh, ctx->n * 8));
+  SEVP_CUDA_TRY(cudaMemcpyAsync(ctx->bh, bh, ctx->n * 8, cudaMemcpyHostToDevice, ctx->stream));
+  if (o->use_guess)
+    SEVP_CUDA_TRY(cudaMemcpyAsync(ctx->xh, xh, ctx->n * 8, cudaMemcpyHostToDevice, ctx->stream));
+  int s = sevp_solve(ctx, ctx->bh, ctx->xh, o, rep);
+  cudaError_t e = cudaMemcpyAsync(xh, ctx->xh, ctx->n * 8, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) {
+    sevp_internal_set_error(e, "copy x to host", __FILE__, __LINE__);
+    return SEVP_CUDA_ERROR;
+  }
+  return s;
+}
+
+extern "C" int sevp_relative_residual(sevp_ctx *ctx, const double *b, const double *x,
+                                      double *relres) {
+  if (!ctx || !ctx->have_op || !b || !x || !relres) return SEVP_BAD_ARG;
+  int s = launch_residual<double>(ctx, x, nullptr, nullptr, b, (double *)nullptr, 0, 0.0);
+  if (s) return s;
+  s = read_state(ctx);
+  if (s) return s;
+  *relres = ctx->h_st->bb64 > 0 ? sqrt(ctx->h_st->rr64 / ctx->h_st->bb64) : 0.0;
+  return SEVP_OK;
+}

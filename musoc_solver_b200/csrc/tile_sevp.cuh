@@ -1,0 +1,47 @@
+// Block-Jacobi tile SEVP: device structures shared by the precompute and the
+// apply kernels.
+//
+// The grid (nx columns, ny rows; element (i, j) at j * nx + i, the memory
+// order of the reference's column-major (I2, J2) arrays) is cut into tiles of
+// at most tm x th points.  Tile (a, b) covers columns [a*tm, a*tm + mw) and
+// rows [b*th, b*th + hh), clipped at the domain edge.  Inside a tile the
+// equations are solved exactly with zero Dirichlet data outside the tile by
+// SEVP marching in the north direction.  A tile of hh rows is split into nb
+// sub-blocks whose boundaries are k_t = (t * hh) / nb, t = 0..nb; nb is set
+// per tile row (latitude band) so that the marching error growth, which
+// depends on the local coefficient anisotropy, stays bounded.
+//
+// Influence data per tile, all FP64, mw x mw, element [k][n] at k * mw + n
+// (k = input column, n = output column):
+//   Sinv_t  t = 0..nb-1  inverse of the guess-row -> last-equation map of
+//                        sub-block t (the reference's RINV after MATINV)
+//   R1_t    t = 0..nb-2  minus Sinv_t times the guess-row -> top-row map
+//                        (the reference's RINV1)
+// stored consecutively: Sinv_0..Sinv_{nb-1}, R1_0..R1_{nb-2}.
+#pragma once
+#include "common.cuh"
+
+namespace sevp {
+
+struct TileGeom {
+  int nx, ny, tm, th, tx, ty;
+  int wseg;   // lanes per tile segment: 8, 16 or 32 (>= tm)
+  int tpw;    // tiles per warp = 32 / wseg
+  int txg;    // tile groups per tile row = ceil(tx / tpw)
+  int hmax;   // max tile height (= th)
+  int nbmax;  // max sub-blocks per tile
+  const int *row_nb;         // [ty] sub-blocks per tile of tile row b
+  const long long *moff;     // [ty * tx] offset of each tile's influence data
+};
+
+__host__ __device__ inline int tile_width(const TileGeom &g, int a) {
+  int w = g.nx - a * g.tm;
+  return w < g.tm ? (w > 0 ? w : 0) : g.tm;
+}
+__host__ __device__ inline int tile_height(const TileGeom &g, int b) {
+  int h = g.ny - b * g.th;
+  return h < g.th ? h : g.th;
+}
+__host__ __device__ inline int sub_start(int t, int hh, int nb) { return (t * hh) / nb; }
+
+}  // namespace sevp

@@ -1,0 +1,154 @@
+"""Host-side interface of the native SEVP-PCG solver.
+
+``SevpSolver`` owns a device operator (five FP32 coefficient planes and the
+tile influence data) and solves ``A x = b`` on the GPU with the block-Jacobi
+tile SEVP preconditioned conjugate gradient, either all in FP64 or as FP32
+inner solves inside FP64 iterative refinement.
+
+Device memory, streams and the upload of inputs use PyTorch (plumbing); every
+arithmetic step runs in ``libsevp_b200.so``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import native as N
+
+
+def default_sub_rows(problem_or_ratio, tile_h: int, growth_limit: float = 1e6) -> list[int]:
+    """Sub-block heights per tile row from the marching amplification bound.
+
+    Marching north multiplies the worst Fourier mode by z per row, where
+    z + 1/z = (2|AL+AR| + |AB+AT| + |gamma|)/|AT| (largest over the band).
+    The height is the largest s with z**s <= growth_limit (at least 1).
+    """
+    p = problem_or_ratio
+    al, ab, ac, ar, at = (np.abs(a.astype(np.float64)) for a in p.coeffs())
+    ny = p.ny
+    ty = -(-ny // tile_h)
+    out = []
+    for b in range(ty):
+        sl = slice(b * tile_h, min(ny, (b + 1) * tile_h))
+        atn = np.maximum(at[sl], 1e-300)
+        # use the interior rows (the last domain row has AT = 0 and is not marched)
+        ratio = (np.abs(ac[sl]) + al[sl] + ar[sl]) / atn
+        valid = at[sl] > 0
+        c = float(ratio[valid].max()) if valid.any() else 2.0
+        c = max(c, 2.0 + 1e-12)
+        z = 0.5 * (c + np.sqrt(c * c - 4.0))
+        s = int(np.floor(np.log(growth_limit) / np.log(z))) if z > 1.0 else tile_h
+        out.append(max(1, min(tile_h, s)))
+    return out
+
+
+@dataclass
+class SolveResult:
+    status: int
+    iterations: int
+    refinements: int
+    rel_residual: float
+    bnorm: float
+    ms: float
+
+
+class SevpSolver:
+    """Device operator + solver context (one GPU, one CUDA stream)."""
+
+    def __init__(self, problem, tile_m: int = 16, tile_h: int = 16, sub_rows=None,
+                 growth_limit: float = 1e10, device: str = "cuda", stream=None):
+        import torch
+
+        self.torch = torch
+        self.p = problem
+        self.nx, self.ny = problem.nx, problem.ny
+        self.device = torch.device(device)
+        self.stream = stream or torch.cuda.current_stream(self.device)
+        dev = self.device
+        self.coef = [torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(dev)
+                     for a in problem.coeffs()]
+        torch.cuda.synchronize(dev)
+        h = C.c_void_p()
+        N.check(N.lib().sevp_create(C.byref(h), self.nx, self.ny, int(problem.periodic),
+                                    C.c_void_p(self.stream.cuda_stream)), "sevp_create")
+        self.h = h
+        if sub_rows is None:
+            sub_rows = default_sub_rows(problem, tile_h, growth_limit)
+        sub_rows = list(np.broadcast_to(np.asarray(sub_rows, np.int32), (-(-self.ny // tile_h),)))
+        self._srow = (C.c_int * len(sub_rows))(*sub_rows)
+        self.sub_rows = sub_rows
+        self.tiling = N.Tiling(tile_m, tile_h, int(max(sub_rows)), self._srow)
+        N.check(N.lib().sevp_set_operator(self.h, *[N.ptr(t) for t in self.coef],
+                                          C.byref(self.tiling)), "sevp_set_operator")
+
+    def close(self):
+        if getattr(self, "h", None):
+            N.lib().sevp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ------------------------------------------------------------------
+    def influence_bytes(self) -> int:
+        return int(N.lib().sevp_influence_bytes(self.h))
+
+    def launches(self) -> int:
+        return int(N.lib().sevp_kernel_launches(self.h))
+
+    def opts(self, precision=0, tol=1e-12, max_iter=5000, inner_tol=1e-5, use_guess=False,
+             check_every=4):
+        return N.SolveOpts(int(precision), float(tol), int(max_iter), float(inner_tol),
+                           int(use_guess), int(check_every))
+
+    def solve(self, b, x=None, precision=0, tol=1e-12, max_iter=5000, inner_tol=1e-5,
+              check_every=4):
+        """Solves on device tensors (float64, shape (ny, nx)).  ``x`` holds the
+        initial guess when given and receives the solution."""
+        torch = self.torch
+        use_guess = x is not None
+        if x is None:
+            x = torch.zeros((self.ny, self.nx), dtype=torch.float64, device=self.device)
+        o = self.opts(precision, tol, max_iter, inner_tol, use_guess, check_every)
+        rep = N.Report()
+        s = N.lib().sevp_solve(self.h, N.ptr(b), N.ptr(x), C.byref(o), C.byref(rep))
+        if s not in (N.SEVP_OK, N.SEVP_MAXITER):
+            raise N.SevpError(s, "sevp_solve")
+        return x, SolveResult(rep.status, rep.iterations, rep.refinements, rep.rel_residual,
+                              rep.bnorm, rep.ms)
+
+    def solve_host(self, b: np.ndarray, x: np.ndarray | None = None, precision=0, tol=1e-12,
+                   max_iter=5000, inner_tol=1e-5, check_every=4):
+        """Solves with host arrays (copies in and out inside the call)."""
+        b = np.ascontiguousarray(b, np.float64)
+        use_guess = x is not None
+        out = np.ascontiguousarray(x, np.float64).copy() if use_guess else np.zeros_like(b)
+        o = self.opts(precision, tol, max_iter, inner_tol, use_guess, check_every)
+        rep = N.Report()
+        s = N.lib().sevp_solve_host(self.h, N.ptr(b), N.ptr(out), C.byref(o), C.byref(rep))
+        if s not in (N.SEVP_OK, N.SEVP_MAXITER):
+            raise N.SevpError(s, "sevp_solve_host")
+        return out, SolveResult(rep.status, rep.iterations, rep.refinements, rep.rel_residual,
+                                rep.bnorm, rep.ms)
+
+    def apply(self, x):
+        y = self.torch.empty_like(x)
+        N.check(N.lib().sevp_apply(self.h, N.ptr(x), N.ptr(y)), "sevp_apply")
+        return y
+
+    def precondition(self, r):
+        z = self.torch.empty_like(r)
+        fn = N.lib().sevp_precondition if r.dtype == self.torch.float64 else N.lib().sevp_precondition_f32
+        N.check(fn(self.h, N.ptr(r), N.ptr(z)), "sevp_precondition")
+        return z
+
+    def relative_residual(self, b, x) -> float:
+        v = C.c_double()
+        N.check(N.lib().sevp_relative_residual(self.h, N.ptr(b), N.ptr(x), C.byref(v)),
+                "sevp_relative_residual")
+        return v.value

@@ -1,0 +1,148 @@
+"""Parity of the native sm_100a SEVP-PCG path against the CPU oracle.
+
+Tolerances:
+  * operator apply: relative 1e-13 (FP64; the GPU fuses multiply-adds);
+  * tile preconditioner z = M^-1 r: relative 1e-8 of max|z| (marching
+    amplifies rounding by at most the growth bound used to pick sub-block
+    heights, 1e6, on top of ~1e-16);
+  * solves: ||b - A x|| / ||b|| <= 1e-12 (FP64), and max|x - x_oracle| <=
+    1e-8 max|x_oracle| (both satisfy the same residual bound).
+"""
+import numpy as np
+import pytest
+
+from musoc_solver_b200 import problems as P
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from musoc_solver_b200 import build
+
+    build.build()
+    return torch
+
+
+def _solver(p, tm, th, srow=None):
+    from musoc_solver_b200.solver import SevpSolver
+
+    # growth bound 1e6: marching rounding stays ~1e-10, so the GPU and the
+    # oracle preconditioners agree tightly
+    return SevpSolver(p, tile_m=tm, tile_h=th, sub_rows=srow, growth_limit=1e6)
+
+
+CASES = [
+    ("basin", lambda: P.basin(0), 24, 24),
+    ("basin16", lambda: P.basin(1), 16, 16),
+    ("global_small", lambda: P.global_grid(180, 90, seed=2), 16, 16),
+    ("ragged", lambda: P.global_grid(100, 70, seed=3), 12, 9),
+    ("ragged32", lambda: P.global_grid(150, 77, seed=4), 32, 20),
+    ("tiny", lambda: P.basin(2, n=7), 8, 3),
+]
+
+
+@pytest.mark.parametrize("name,mk,tm,th", CASES)
+def test_apply_matches_oracle(torch_cuda, oracle, name, mk, tm, th):
+    torch = torch_cuda
+    p = mk()
+    s = _solver(p, tm, th)
+    rng = np.random.default_rng(0)
+    x = rng.standard_normal((p.ny, p.nx))
+    y = s.apply(torch.from_numpy(x).cuda()).cpu().numpy()
+    yo = oracle.apply(p, x)
+    assert np.abs(y - yo).max() <= 1e-13 * np.abs(yo).max()
+
+
+@pytest.mark.parametrize("name,mk,tm,th", CASES)
+def test_precondition_matches_oracle(torch_cuda, oracle, name, mk, tm, th):
+    torch = torch_cuda
+    p = mk()
+    s = _solver(p, tm, th)
+    pc = oracle.TilePC(p, tm, th, s.sub_rows)
+    assert pc.status == 0
+    rng = np.random.default_rng(1)
+    r = rng.standard_normal((p.ny, p.nx))
+    z = s.precondition(torch.from_numpy(r).cuda()).cpu().numpy()
+    zo = pc.apply(r)
+    assert np.isfinite(z).all()
+    assert np.abs(z - zo).max() <= 1e-8 * np.abs(zo).max()
+    # FP32 vectors, FP64 marching: rounding of r and z only
+    z32 = s.precondition(torch.from_numpy(r.astype(np.float32)).cuda()).cpu().numpy()
+    assert np.abs(z32 - zo).max() <= 1e-5 * np.abs(zo).max()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("name,mk,tm,th", CASES[:5])
+def test_solve_matches_oracle(torch_cuda, oracle, name, mk, tm, th, precision):
+    torch = torch_cuda
+    p = mk()
+    s = _solver(p, tm, th)
+    b = torch.from_numpy(p.b).cuda()
+    x, rep = s.solve(b, precision=precision, tol=1e-12)
+    assert rep.status == 0
+    assert rep.rel_residual <= 1e-12
+    xg = x.cpu().numpy()
+    # independent FP64 residual on the host
+    res = np.linalg.norm(p.b - P.apply_operator(p, xg)) / np.linalg.norm(p.b)
+    assert res <= 2e-12
+    pc = oracle.TilePC(p, tm, th, s.sub_rows)
+    xo, it, rel = pc.pcg(p.b, tol=1e-12)
+    assert rel <= 1e-12
+    assert np.abs(xg - xo).max() <= 1e-8 * np.abs(xo).max()
+    if precision == 0:
+        # same method, same arithmetic up to reduction order: same iteration count +-2
+        assert abs(rep.iterations - it) <= 2
+
+
+def test_solve_host_and_guess(torch_cuda, oracle):
+    p = P.global_grid(180, 90, seed=5)
+    s = _solver(p, 16, 16)
+    x, rep = s.solve_host(p.b, precision=1)
+    assert rep.rel_residual <= 1e-12
+    # warm start from the solution converges immediately
+    x2, rep2 = s.solve_host(p.b, x=x, precision=0)
+    assert rep2.iterations == 0 and rep2.rel_residual <= 1e-12
+    # warm start from a perturbed solution needs fewer iterations than zero
+    xp = x * (1.0 + 1e-6 * np.random.default_rng(0).standard_normal(x.shape))
+    x3, rep3 = s.solve_host(p.b, x=xp, precision=0)
+    _, rep0 = s.solve_host(p.b, precision=0)
+    assert rep3.rel_residual <= 1e-12 and rep3.iterations < rep0.iterations
+
+
+def test_relative_residual_and_zero_rhs(torch_cuda):
+    torch = torch_cuda
+    p = P.basin(3)
+    s = _solver(p, 24, 24)
+    b = torch.zeros((p.ny, p.nx), dtype=torch.float64, device="cuda")
+    x, rep = s.solve(b, precision=0)
+    assert rep.status == 0 and rep.iterations == 0
+    assert float(x.abs().max()) == 0.0
+
+
+def test_nonfinite_rhs_reports_status(torch_cuda):
+    torch = torch_cuda
+    from musoc_solver_b200 import native as N
+
+    p = P.basin(4)
+    s = _solver(p, 24, 24)
+    b = torch.from_numpy(p.b).cuda()
+    b[5, 5] = float("nan")
+    with pytest.raises(N.SevpError) as e:
+        s.solve(b, precision=0)
+    assert e.value.status == N.SEVP_NONFINITE
+    # context stays usable
+    x, rep = s.solve(torch.from_numpy(p.b).cuda(), precision=0)
+    assert rep.status == 0
+
+
+def test_max_iter_status(torch_cuda):
+    torch = torch_cuda
+    p = P.global_grid(180, 90, seed=6)
+    s = _solver(p, 16, 16)
+    b = torch.from_numpy(p.b).cuda()
+    x, rep = s.solve(b, precision=0, max_iter=3)
+    assert rep.status == 1 and rep.iterations == 3 and rep.rel_residual > 1e-12
