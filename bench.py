@@ -1,0 +1,435 @@
+#!/usr/bin/env python
+"""Benchmark: solves/s to 1e-12 relative residual at 3600x2400.
+
+Workload (one "step" = one time step of a sequence of barotropic solves):
+  * operator: the 3600x2400 periodic-in-x global grid (lat in [-78, 78],
+    dx = R dlon cos(lat), seeded synthetic bathymetry with ~30 % land,
+    dt = 60 s), symmetric 5-point FP32 coefficients;
+  * right-hand sides: a seeded field of 300 Gaussian eddies (radius
+    50-150 km) advected at 0.2 m/s with slow amplitude drift, one field per
+    step (the sequence workload of the learned warm start, at 3600x2400);
+  * a step solves A eta_n = b_n to ||b - A eta|| / ||b|| <= 1e-12 (FP64
+    residual) on the GPU.
+
+Arms reported in one JSON line:
+  value        mixed precision (FP32 PCG + FP64 refinement) from the best
+               warm start available (learned network when trained weights
+               are given, else linear extrapolation of the two previous
+               solutions); inputs resident in HBM, device-timed
+  fp64_plain   the plain FP64 SEVP-PCG from a zero guess on the same steps
+  e2e          the value arm through the C ABI with host buffers (b_n,
+               eta_{n-1}, eta_{n-2} in, eta_n out, copies inside the timing)
+  roofline     the dominant kernel (tile SEVP pass B) against measured HBM
+  cpu_baseline the CPU oracle (FP64 tile-SEVP PCG, OpenMP) on the host cores
+
+Every vector is larger than the 126 MB L2 (69 MB per FP64 field; ~1 GB of
+traffic per PCG iteration), so no explicit L2 flush is done between steps.
+
+``--impl reference`` times the CPU implementation of the method (the oracle
+port; the reference's own full-width REP1 needs > 60 GB of influence
+matrices at 3600 columns and its unpreconditioned BiCGSTAB needs thousands
+of iterations, so neither finishes in minutes) on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "solves/s to 1e-12 rel. residual at 3600x2400: learned+mixed vs plain FP64 SEVP"
+NX, NY = 3600, 2400
+TILE_M, TILE_H, GROWTH = 16, 16, 1e10
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["native", "reference"], default="native")
+    ap.add_argument("--nx", type=int, default=NX)
+    ap.add_argument("--ny", type=int, default=NY)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--weights", default=os.path.join(ROOT, "musoc_solver_b200", "weights",
+                                                      "unet_eddy.npz"))
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ utils
+class ClockSampler:
+    """Samples nvidia-smi SM clocks and throttle reasons during a region."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.t.join(timeout=2)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for k, nm in enumerate(names):
+                if len(r) > 4 + k and r[4 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(self.rows)}
+
+
+def measured_peak_hbm():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """Per-launch DRAM bytes of the tile pass-B kernel from the committed ncu
+    summary (profiles/), or None."""
+    path = os.path.join(ROOT, "profiles", "tile_pass_b_3600x2400.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch_mixed:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+def make_sequence(nx, ny, nsteps):
+    from musoc_solver_b200 import problems as P
+
+    p = P.global_grid(nx, ny, seed=11)
+    rhs = [b for _, b in P.eddy_rhs(nx, ny, range(nsteps), seed=3)]
+    wet = p.meta["wet"]
+    rhs = [np.where(wet, b, 0.0) for b in rhs]
+    return p, rhs
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return world, rank, local, dist
+
+
+# ------------------------------------------------------------ CPU oracle
+def cpu_solve_seconds(p, b, threads, tile_nb=None):
+    """One FP64 tile-SEVP PCG solve with the CPU oracle (setup excluded),
+    with the same tile layout as the GPU solver."""
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from musoc_solver_b200.solver import tile_sub_blocks
+
+    if tile_nb is None:
+        tile_nb = tile_sub_blocks(p, TILE_M, TILE_H, GROWTH)
+    pc = O.TilePC(p, TILE_M, TILE_H, tile_nb=tile_nb)
+    t = time.perf_counter()
+    x, it, rel = pc.pcg(b, tol=1e-12)
+    dt = time.perf_counter() - t
+    return dt, it, rel
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return 0
+    cores = os.cpu_count() or 1
+    os.environ["OMP_NUM_THREADS"] = str(cores)
+    p, rhs = make_sequence(args.nx, args.ny, args.warmup + args.steps)
+    times, iters = [], []
+    for n in range(args.warmup + args.steps):
+        dt, it, rel = cpu_solve_seconds(p, rhs[n], cores)
+        if n >= args.warmup:
+            times.append(dt)
+            iters.append(it)
+    total = sum(times)
+    value = len(times) / total
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "impl": "reference",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * total / len(times), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{args.nx}x{args.ny} global grid, eddy right-hand-side sequence, "
+                               "FP64 tile-SEVP PCG (16x16 tiles) to 1e-12, zero guess",
+                   "grid": [args.nx, args.ny], "tol": 1e-12, "l2": "inputs larger than L2"},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "port",
+                         "sample": "one full FP64 tile-SEVP PCG solve per step with the C oracle "
+                                   f"(OpenMP, {cores} threads), setup excluded; mean iterations "
+                                   f"{float(np.mean(iters)):.1f}"},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------- native
+def run_native(args, world, rank, local, dist):
+    import torch
+
+    from musoc_solver_b200 import build, native as N
+    from musoc_solver_b200.solver import SevpSolver
+
+    build.build()
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    K, W = args.steps, args.warmup
+    nsteps = W + K + 2
+    p, rhs = make_sequence(args.nx, args.ny, nsteps)
+    n = p.nx * p.ny
+    solver = SevpSolver(p, tile_m=TILE_M, tile_h=TILE_H, growth_limit=GROWTH)
+    stream = solver.stream
+    b_dev = [torch.from_numpy(b).to(dev) for b in rhs]
+    torch.cuda.synchronize()
+
+    # learned warm start if trained weights exist, else linear extrapolation
+    guess_mode, guess_name = N.GUESS_LINEAR, "linear extrapolation 2*eta[n-1]-eta[n-2]"
+    warm = None
+    if os.path.exists(args.weights):
+        try:
+            from musoc_solver_b200.warmstart import LearnedWarmStart
+
+            warm = LearnedWarmStart.load(args.weights, p, device=dev)
+            warm.attach(solver)
+            guess_mode, guess_name = N.GUESS_LEARNED, "learned U-Net (BF16)"
+        except Exception as e:  # report and fall back to the physics guess
+            print(f"# warm start network unavailable: {e}", file=sys.stderr)
+
+    # history: the first two steps solved in FP64 from zero (untimed)
+    eta = [torch.zeros(p.ny, p.nx, dtype=torch.float64, device=dev) for _ in range(nsteps)]
+    for k in range(2):
+        eta[k].copy_(solver.solve(b_dev[k], precision=0)[0])
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(v):
+        if dist is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    # ---- value arm: mixed precision + warm start, device-resident inputs
+    for k in range(2, 2 + W):
+        solver.solve_step(b_dev[k], eta[k - 1], eta[k - 2], eta[k], guess=guess_mode, precision=1)
+    barrier()
+    solver.profile(True)
+    l_value0 = solver.launches()
+    reps = []
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for k in range(2 + W, 2 + W + K):
+            _, r = solver.solve_step(b_dev[k], eta[k - 1], eta[k - 2], eta[k], guess=guess_mode,
+                                     precision=1)
+            reps.append(r)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    t_value = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
+    prof = solver.profile_read()
+    solver.profile(False)
+    launches_value = solver.launches() - l_value0
+    relres = [r.rel_residual for r in reps]
+    status = [r.status for r in reps]
+
+    # error of the value arm against an FP64 solve of the same steps
+    ref_x = torch.zeros_like(eta[0])
+    errs = []
+    for k in (2 + W, 2 + W + K - 1):
+        solver.solve(b_dev[k], x=ref_x.zero_(), precision=0)
+        errs.append(float((eta[k] - ref_x).abs().max() / ref_x.abs().max()))
+
+    # ---- plain FP64 SEVP-PCG from a zero guess
+    xz = torch.zeros_like(eta[0])
+    for k in range(2, 2 + min(W, 2)):
+        solver.solve(b_dev[k], x=xz.zero_(), precision=0)
+    barrier()
+    l0 = solver.launches()
+    ev0.record(stream)
+    it64 = []
+    for k in range(2 + W, 2 + W + K):
+        _, r = solver.solve(b_dev[k], x=xz.zero_(), precision=0)
+        it64.append(r.iterations)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    t_fp64 = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
+
+    # ---- mixed precision from a zero guess (isolates the precision gain)
+    barrier()
+    ev0.record(stream)
+    itmz = []
+    for k in range(2 + W, 2 + W + K):
+        _, r = solver.solve(b_dev[k], x=xz.zero_(), precision=1)
+        itmz.append(r.iterations)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    t_mixed0 = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
+
+    # ---- e2e: the same value arm through the C ABI with host buffers
+    pin = lambda a: torch.from_numpy(a).pin_memory().numpy()
+    b_host = [pin(b) for b in rhs]
+    eta_host = [pin(np.zeros((p.ny, p.nx))) for _ in range(nsteps)]
+    for k in range(2):
+        eta_host[k][:] = eta[k].cpu().numpy()
+    for k in range(2, 2 + W):
+        solver.solve_step_host(b_host[k], eta_host[k - 1], eta_host[k - 2], eta_host[k],
+                               guess=guess_mode, precision=1)
+    barrier()
+    t0 = time.perf_counter()
+    l1 = solver.launches()
+    for k in range(2 + W, 2 + W + K):
+        solver.solve_step_host(b_host[k], eta_host[k - 1], eta_host[k - 2], eta_host[k],
+                               guess=guess_mode, precision=1)
+    torch.cuda.synchronize()
+    t_e2e = max_over_ranks(time.perf_counter() - t0)
+    launches_e2e = solver.launches() - l1
+    h2d = 8 * n * (3 if guess_mode in (N.GUESS_LINEAR, N.GUESS_LEARNED) else 2)
+    d2h = 8 * n
+
+    # ---- roofline of the dominant kernel (tile SEVP pass B, FP32 vectors)
+    peak, peak_kind = measured_peak_hbm()
+    tile_ms, tile_n = prof["tile"]
+    infl = solver.influence_bytes()
+    bytes_per_launch = n * (4 * 4 + 3 * 4 + 5 * 4) + infl  # x,p,r,q in; x,r,z out; coeffs
+    avg_s = tile_ms / 1e3 / max(tile_n, 1)
+    achieved = bytes_per_launch / avg_s / 1e9 if tile_n else None
+    traffic = ncu_traffic()
+
+    # ---- CPU baseline (rank 0 at N = 1)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cores = os.cpu_count() or 1
+        dt, itc, relc = cpu_solve_seconds(p, rhs[2 + W], cores, solver.tile_nb)
+        cpu = {"value": 1.0 / dt, "unit": "solves/s", "cores": cores, "kind": "port",
+               "sample": f"one full FP64 tile-SEVP PCG solve of step {2 + W} with the C oracle "
+                         f"(OpenMP, {cores} threads, {itc} iterations, rel. residual {relc:.2e}), "
+                         "setup excluded"}
+
+    value = world * K / t_value
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "solves/s",
+        "n_gpus": world,
+        "steps": K,
+        "warmup": W,
+        "ms_per_step": 1e3 * t_value / K,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32+f64",
+        "data": "synthetic",
+        "config": {
+            "workload": f"{p.nx}x{p.ny} global grid (lat +-78, ~30% land, dt=60 s), eddy "
+                        "right-hand-side sequence; mixed FP32 tile-SEVP PCG + FP64 iterative "
+                        f"refinement to 1e-12 from warm start: {guess_name}",
+            "grid": [p.nx, p.ny], "tiles": [TILE_M, TILE_H], "marching_growth_limit": GROWTH,
+            "tol": 1e-12, "parallelism": f"replicas x{world}",
+            "l2": "inputs larger than L2 (69 MB per FP64 field), no flush",
+        },
+        "fp64_plain": {"value": world * K / t_fp64, "unit": "solves/s",
+                       "ms_per_step": 1e3 * t_fp64 / K,
+                       "mean_iterations": float(np.mean(it64))},
+        "mixed_zero_guess": {"value": world * K / t_mixed0, "unit": "solves/s",
+                             "mean_iterations": float(np.mean(itmz))},
+        "value_arm": {"mean_iterations": float(np.mean([r.iterations for r in reps])),
+                      "mean_refinements": float(np.mean([r.refinements for r in reps])),
+                      "max_rel_residual": float(max(relres)), "status": sorted(set(status)),
+                      "max_rel_err_vs_fp64": float(max(errs))},
+        "speedup_vs_fp64_plain": (K / t_value) / (K / t_fp64),
+        "e2e": {"value": world * K / t_e2e, "unit": "solves/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                     "kernel": "k_tile_apply<float, update, dots> (PCG pass B)",
+                     "algorithmic_bytes_per_launch": bytes_per_launch,
+                     "avg_launch_ms": avg_s * 1e3, "launches": tile_n,
+                     "peak_source": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)"},
+        "cpu_baseline": cpu,
+        "clocks": clk.summary(),
+        "gpu_launches": int(launches_value),
+        "gpu_launches_e2e": int(launches_e2e),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if warm is not None:
+        warm.close()
+    solver.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    world, rank, local, dist = dist_setup(args)
+    if args.impl == "reference":
+        rc = run_reference(args, world, rank)
+        if dist is not None:
+            dist.destroy_process_group()
+        return rc
+    return run_native(args, world, rank, local, dist)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

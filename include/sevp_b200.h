@@ -128,11 +128,14 @@ void lanczos_(const float *al, const float *ab, const float *ac, const float *ar
 /* Overlapping-strip Schwarz sweeps of FS_SOLVER, M/fs_GLOBAL.f90:1904-1966
  * (FL_EVP_STP == 1): niter sweeps over nbir strips of REPBIR.  RINV is
  * (IBIR*IBIR, NB0, NBIR) and RINV1 (IBIR*IBIR, NB0-1, NBIR) as written by
- * PREP; xx ((IBIR+2), J0) is the caller's persistent wrap-strip scratch. */
+ * PREP; xx ((IBIR+2), J0) is the caller's persistent wrap-strip scratch.
+ * fix_wrap = 0 reproduces the reference, which copies the wrapped strip's
+ * side boundaries for rows 1..J2 only (:1925-1926); fix_wrap = 1 also copies
+ * rows J2+1 and J2+2. */
 void sevp_bir_sweeps_(const float *al, const float *ab, const float *ac, const float *ar,
                       const float *at, const float *s, const double *rinv, const double *rinv1,
                       double *x, double *xx, const int *ie, const int *i2, const int *j2,
-                      const int *nb0, const int *nbir, const int *niter);
+                      const int *nb0, const int *nbir, const int *niter, const int *fix_wrap);
 
 /* Influence precompute for all BIR strips, P/prep_GLOBAL.f90:272-318. */
 void sevp_pre_strips_(const float *al, const float *ab, const float *ac, const float *ar,
@@ -147,11 +150,20 @@ typedef struct sevp_ctx sevp_ctx;
 typedef struct {
   int tile_m;   /* tile width in columns: 1..32 */
   int tile_h;   /* tile height in rows: 1..32 */
-  int sub_rows; /* marching sub-block height in rows (>= 1) */
-  /* optional host array of ceil(ny / tile_h) sub-block heights, one per tile
-   * row (latitude band); NULL uses sub_rows everywhere */
+  int sub_rows; /* marching sub-block height in rows (>= 1) when no rule below applies */
+  /* optional host array of ceil(ny / tile_h) heights, one per tile row */
   const int *sub_rows_by_tile_row;
+  /* optional host array of ceil(ny/tile_h) * ceil(nx/tile_m) heights, one per
+   * tile, tile rows first; takes precedence over the per-row array */
+  const int *sub_rows_by_tile;
+  /* > 1 and no array given: each tile's height is the largest s with z^s <=
+   * growth_limit, where z + 1/z is the tile's largest (|AC|+|AL|+|AR|)/|AT|
+   * (the worst-case amplification of one marched row) */
+  double growth_limit;
 } sevp_tiling;
+/* Tile counts and the sub-blocks used by each tile (tiles sharing a warp use
+ * their largest count); nb_per_tile may be NULL. */
+int sevp_tile_layout(const sevp_ctx *ctx, int *tiles_x, int *tiles_y, int *nb_per_tile);
 
 typedef struct {
   int precision;     /* 0: FP64 PCG; 1: FP32 PCG inside FP64 iterative refinement */
@@ -189,6 +201,24 @@ int sevp_solve(sevp_ctx *ctx, const double *b, double *x, const sevp_solve_opts 
 /* Same with host buffers: copies b (and the guess) in and x out. */
 int sevp_solve_host(sevp_ctx *ctx, const double *b_host, double *x_host,
                     const sevp_solve_opts *opts, sevp_report *report);
+/* Warm starts for a time sequence of solves. */
+#define SEVP_GUESS_ZERO 0     /* x = 0 */
+#define SEVP_GUESS_PREVIOUS 1 /* x = eta_{n-1} */
+#define SEVP_GUESS_LINEAR 2   /* x = 2 eta_{n-1} - eta_{n-2} */
+#define SEVP_GUESS_LEARNED 3  /* x = network(eta_{n-1}, eta_{n-2}, b_n), see sevp_set_warmstart */
+/* A learned warm start: writes the guess x (device) from the two previous
+ * solutions and the right-hand side on the given CUDA stream; returns SEVP_*. */
+typedef int (*sevp_warmstart_fn)(void *user, const double *eta1, const double *eta2,
+                                 const double *b, double *x, int nx, int ny, void *stream);
+int sevp_set_warmstart(sevp_ctx *ctx, sevp_warmstart_fn fn, void *user, int launches_per_call);
+/* One step of a sequence: x = guess(eta1, eta2, b), then the solve of A x = b
+ * from that guess (device pointers; eta1/eta2 may be NULL when unused). */
+int sevp_solve_step(sevp_ctx *ctx, const double *b, const double *eta1, const double *eta2,
+                    double *x, int guess_mode, const sevp_solve_opts *opts, sevp_report *report);
+/* Same with host buffers: copies b, eta1, eta2 in and x out inside the call. */
+int sevp_solve_step_host(sevp_ctx *ctx, const double *b_host, const double *eta1_host,
+                         const double *eta2_host, double *x_host, int guess_mode,
+                         const sevp_solve_opts *opts, sevp_report *report);
 /* y = A x on the unpadded grid (device pointers). */
 int sevp_apply(sevp_ctx *ctx, const double *x, double *y);
 /* z = M^{-1} r: block-Jacobi tiles solved by SEVP marching (device). */
@@ -199,6 +229,13 @@ int sevp_precondition_f32(sevp_ctx *ctx, const float *r, float *z);
 int sevp_relative_residual(sevp_ctx *ctx, const double *b, const double *x, double *relres);
 /* Number of kernel launches issued by this context since creation. */
 long long sevp_kernel_launches(const sevp_ctx *ctx);
+/* Per-kernel-class device timing with CUDA events on the context stream:
+ * enable != 0 starts (and zeroes) it.  sevp_profile_read fills ms[4] and
+ * count[4] for class 0 = tile pass B (update + precondition + dots),
+ * 1 = stencil passes (apply, pass A, residuals), 2 = tile precondition
+ * without update, 3 = unused. */
+int sevp_profile(sevp_ctx *ctx, int enable);
+int sevp_profile_read(sevp_ctx *ctx, double *ms, long long *count);
 
 #ifdef __cplusplus
 }

@@ -246,16 +246,11 @@ struct OpResidual {
 // --------------------------------------------------- tile apply kernel
 constexpr int kTileWarps = 4;
 
-struct TileSmem {
-  double *zs;   // [hmax][32]
-  void *rs;     // [hmax][32] of V
-  double *rho;  // [nbmax][32]
-  double *u0;   // [nbmax][32]
-  double *dv;   // [32]
-};
-
-__host__ __device__ inline size_t tile_smem_per_warp(int hmax, int nbmax, int vbytes) {
-  return (size_t)hmax * 32 * 8 + (size_t)hmax * 32 * vbytes + (size_t)nbmax * 32 * 16 + 32 * 8;
+// Shared memory per warp: the tile's rows of z (FP64 marching state, 32
+// lanes per row), the last-equation residual of each sub-block (stored at
+// the sub-block's last row), and the mat-vec broadcast vector.
+__host__ __device__ inline size_t tile_smem_per_warp(int hmax) {
+  return (size_t)hmax * 32 * 8 * 2 + 32 * 8;
 }
 
 // out(n) = sum_k dv[seg + k] * M[k * mw + n]
@@ -275,6 +270,29 @@ __device__ __forceinline__ double seg_matvec(const double *dv, int segbase, cons
   return s;
 }
 
+// Inputs of one tile row for one lane (prefetched one row ahead).
+template <typename V>
+struct RowIn {
+  V x, p, r, q;
+  float cw, cs, cc, ce, cn;
+};
+
+template <typename V, bool UPDATE>
+__device__ __forceinline__ void load_row(RowIn<V> &in, const Coeffs &c, const V *x, const V *p,
+                                         const V *r, const V *q, size_t idx) {
+  if (UPDATE) {
+    in.x = x[idx];
+    in.p = p[idx];
+    in.q = q[idx];
+  }
+  in.r = r[idx];
+  in.cw = __ldg(c.al + idx);
+  in.cs = __ldg(c.ab + idx);
+  in.cc = __ldg(c.ac + idx);
+  in.ce = __ldg(c.ar + idx);
+  in.cn = __ldg(c.at + idx);
+}
+
 // UPDATE: fused x += alpha p, r -= alpha q before preconditioning (pass B).
 // DOTS:   accumulate r.z and r.r and finish the iteration on the device.
 template <typename V, bool UPDATE, bool DOTS>
@@ -284,13 +302,10 @@ __global__ void __launch_bounds__(kTileWarps * 32)
   if (DOTS && st->done) return;
   extern __shared__ __align__(16) unsigned char tsm[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const size_t per_warp = tile_smem_per_warp(tg.hmax, tg.nbmax, sizeof(V));
-  unsigned char *base = tsm + per_warp * wib;
-  double *zs = (double *)base;
-  V *rs = (V *)(base + (size_t)tg.hmax * 32 * 8);
-  double *rho_s = (double *)(base + (size_t)tg.hmax * 32 * (8 + sizeof(V)));
-  double *u0_s = rho_s + (size_t)tg.nbmax * 32;
-  double *dv = u0_s + (size_t)tg.nbmax * 32;
+  unsigned char *base = tsm + tile_smem_per_warp(tg.hmax) * wib;
+  double *zs = (double *)base;                       // [hmax][32]
+  double *rho_s = zs + (size_t)tg.hmax * 32;         // [hmax][32]
+  double *dv = rho_s + (size_t)tg.hmax * 32;         // [32]
 
   double acc_rz = 0.0, acc_rr = 0.0;
   const int gw = blockIdx.x * kTileWarps + wib;
@@ -302,7 +317,7 @@ __global__ void __launch_bounds__(kTileWarps * 32)
     const int mw = (a < tg.tx) ? tile_width(tg, a) : 0;
     const bool active = n < mw;
     const int nx = tg.nx;
-    const int j0 = b * tg.th, hh = tile_height(tg, b), nb = tg.row_nb[b];
+    const int j0 = b * tg.th, hh = tile_height(tg, b), nb = tg.grp_nb[(size_t)b * tg.txg + grp];
     const int i = a * tg.tm + n;
     const double *mt = mats + (mw > 0 ? tg.moff[(size_t)b * tg.tx + a] : 0);
     const size_t msz = (size_t)mw * mw;
@@ -310,100 +325,105 @@ __global__ void __launch_bounds__(kTileWarps * 32)
     if (UPDATE) alpha = st->alpha;
 
     // ---- forward sweep: particular solution with zero guess rows and
-    //      block-top corrections (the elimination of the SEVP system)
+    //      block-top corrections (the elimination of the SEVP system).
+    //      zs keeps each sub-block's top row before its correction.
     double zb = 0.0, zc = 0.0;
     int t = 0, kb = 0, ke = sub_start(1, hh, nb) - 1;
+    RowIn<V> cur{}, nxt{};
+    const size_t idx0 = (size_t)j0 * nx + i;
+    if (active) load_row<V, UPDATE>(cur, c, x, p, r, q, idx0);
     for (int k = 0; k < hh; ++k) {
-      const size_t idx = (size_t)(j0 + k) * nx + i;
-      double rv = 0.0, cw = 0.0, cs = 0.0, cc = 0.0, ce = 0.0, cn = 1.0;
+      const size_t idx = idx0 + (size_t)k * nx;
+      if (active && k + 1 < hh) load_row<V, UPDATE>(nxt, c, x, p, r, q, idx + nx);
+      double rv = 0.0;
+      const double cw = cur.cw, cs = cur.cs, cc = cur.cc, ce = cur.ce;
+      const double cn = active ? (double)cur.cn : 1.0;
       if (active) {
         if (UPDATE) {
-          V xv = x[idx], pv = p[idx], rov = r[idx], qv = q[idx];
-          V xn = xv + (V)alpha * pv;
-          V rn = rov - (V)alpha * qv;
+          V xn = cur.x + (V)alpha * cur.p;
+          V rn = cur.r - (V)alpha * cur.q;
           x[idx] = xn;
           r[idx] = rn;
           rv = (double)rn;
         } else {
-          rv = (double)r[idx];
+          rv = (double)cur.r;
         }
-        cw = __ldg(c.al + idx);
-        cs = __ldg(c.ab + idx);
-        cc = __ldg(c.ac + idx);
-        ce = __ldg(c.ar + idx);
-        cn = __ldg(c.at + idx);
         acc_rr += rv * rv;
       }
-      rs[k * 32 + lane] = (V)rv;
       if (k == kb) zc = 0.0;
-      zs[k * 32 + lane] = zc;
       double zw = __shfl_up_sync(0xffffffffu, zc, 1);
       double ze = __shfl_down_sync(0xffffffffu, zc, 1);
       if (n == 0) zw = 0.0;
       if (n >= mw - 1) ze = 0.0;
+      zs[k * 32 + lane] = zc;
       if (k < ke) {
         double zn = active ? ((((rv - cw * zw) - cs * zb) - cc * zc) - ce * ze) / cn : 0.0;
         zb = zc;
         zc = zn;
       } else {
         double rho = active ? (((rv - cw * zw) - cs * zb) - cc * zc) - ce * ze : 0.0;
-        rho_s[t * 32 + lane] = rho;
-        u0_s[t * 32 + lane] = zc;
+        rho_s[k * 32 + lane] = rho;
         if (t < nb - 1) {
           dv[lane] = rho;
           __syncwarp();
-          double s = active ? seg_matvec(dv, segbase, mt + (size_t)(nb + t) * msz, mw, n) : 0.0;
+          double sc = active ? seg_matvec(dv, segbase, mt + (size_t)(nb + t) * msz, mw, n) : 0.0;
           __syncwarp();
-          zc = zc - s;
-          zs[k * 32 + lane] = zc;
+          zc = zc - sc;
         }
         zb = zc;
         ++t;
         kb = k + 1;
         ke = sub_start(t + 1, hh, nb) - 1;
       }
+      cur = nxt;
     }
     // ---- backward sweep: guess-row values and homogeneous corrections
     double vnext = 0.0;
     for (t = nb - 1; t >= 0; --t) {
       kb = sub_start(t, hh, nb);
       ke = sub_start(t + 1, hh, nb) - 1;
-      if (t < nb - 1) zs[ke * 32 + lane] = u0_s[t * 32 + lane];
-      double cnk = active ? (double)__ldg(c.at + (size_t)(j0 + ke) * nx + i) : 0.0;
-      dv[lane] = rho_s[t * 32 + lane] - cnk * vnext;
+      const double cnk = active ? (double)__ldg(c.at + idx0 + (size_t)ke * nx) : 0.0;
+      dv[lane] = rho_s[ke * 32 + lane] - cnk * vnext;
       __syncwarp();
       double v = active ? seg_matvec(dv, segbase, mt + (size_t)t * msz, mw, n) : 0.0;
       __syncwarp();
       zs[kb * 32 + lane] += v;
       double hb = 0.0, hc = v;
       if (t > 0) {
-        double cnb = active ? (double)__ldg(c.at + (size_t)(j0 + kb - 1) * nx + i) : 0.0;
+        double cnb = active ? (double)__ldg(c.at + idx0 + (size_t)(kb - 1) * nx) : 0.0;
         dv[lane] = v * cnb;
         __syncwarp();
         hb = active ? seg_matvec(dv, segbase, mt + (size_t)(nb + t - 1) * msz, mw, n) : 0.0;
         __syncwarp();
       }
+      float ncw = 0.f, ncs = 0.f, ncc = 0.f, nce = 0.f, ncn = 1.f;
+      if (active && kb < ke) {
+        const size_t id = idx0 + (size_t)kb * nx;
+        ncw = __ldg(c.al + id), ncs = __ldg(c.ab + id), ncc = __ldg(c.ac + id);
+        nce = __ldg(c.ar + id), ncn = __ldg(c.at + id);
+      }
       for (int k = kb; k < ke; ++k) {
-        const size_t idx = (size_t)(j0 + k) * nx + i;
+        const double cw = ncw, cs = ncs, cc = ncc, ce = nce, cn = ncn;
+        if (active && k + 1 < ke) {
+          const size_t id = idx0 + (size_t)(k + 1) * nx;
+          ncw = __ldg(c.al + id), ncs = __ldg(c.ab + id), ncc = __ldg(c.ac + id);
+          nce = __ldg(c.ar + id), ncn = __ldg(c.at + id);
+        }
         double hw = __shfl_up_sync(0xffffffffu, hc, 1);
         double he = __shfl_down_sync(0xffffffffu, hc, 1);
         if (n == 0) hw = 0.0;
         if (n >= mw - 1) he = 0.0;
-        double hn = 0.0;
-        if (active) {
-          double cw = __ldg(c.al + idx), cs = __ldg(c.ab + idx), cc = __ldg(c.ac + idx);
-          double ce = __ldg(c.ar + idx), cn = __ldg(c.at + idx);
-          hn = ((((-(cw * hw)) - cs * hb) - cc * hc) - ce * he) / cn;
-        }
+        double hn = active ? ((((-(cw * hw)) - cs * hb) - cc * hc) - ce * he) / cn : 0.0;
         zs[(k + 1) * 32 + lane] += hn;
         hb = hc;
         hc = hn;
       }
       if (active)
         for (int k = kb; k <= ke; ++k) {
+          const size_t idx = idx0 + (size_t)k * nx;
           V zv = (V)zs[k * 32 + lane];
-          z[(size_t)(j0 + k) * nx + i] = zv;
-          if (DOTS) acc_rz += (double)rs[k * 32 + lane] * (double)zv;
+          z[idx] = zv;
+          if (DOTS) acc_rz += (double)r[idx] * (double)zv;
         }
       vnext = v;
     }
@@ -446,6 +466,41 @@ __global__ void __launch_bounds__(kTileWarps * 32)
   }
 }
 
+// Per-tile marching growth: the smallest sub-block height s_max such that
+// z^s <= growth, with z + 1/z = max over the tile's marched rows of
+// (|AC| + |AL| + |AR|) / |AT|.  One warp per tile; writes s per tile.
+__global__ void k_tile_growth(TileGeom tg, Coeffs c, double log_growth, int *s_tile) {
+  const int lane = threadIdx.x & 31;
+  const int tile = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (tile >= tg.tx * tg.ty) return;
+  const int a = tile % tg.tx, b = tile / tg.tx;
+  const int mw = tile_width(tg, a), hh = tile_height(tg, b);
+  double cmax = 2.0;
+  bool bad = false;
+  for (int e = lane; e < mw * (hh - 1); e += 32) {
+    const int k = e / mw, n = e % mw;
+    const size_t idx = (size_t)(b * tg.th + k) * tg.nx + a * tg.tm + n;
+    double at = fabs((double)c.at[idx]);
+    double num = fabs((double)c.ac[idx]) + fabs((double)c.al[idx]) + fabs((double)c.ar[idx]);
+    if (at == 0.0) bad = true;
+    else cmax = fmax(cmax, num / at);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    cmax = fmax(cmax, __shfl_xor_sync(0xffffffffu, cmax, o));
+    bad |= __shfl_xor_sync(0xffffffffu, (int)bad, o);
+  }
+  if (lane == 0) {
+    int s = tg.th;
+    if (bad) {
+      s = 1;
+    } else {
+      const double zz = 0.5 * (cmax + sqrt(fmax(cmax * cmax - 4.0, 0.0)));
+      if (zz > 1.0) s = (int)floor(log_growth / log(zz));
+    }
+    s_tile[tile] = s < 1 ? 1 : (s > tg.th ? tg.th : s);
+  }
+}
+
 // -------------------------------------------------- tile precompute
 // One CTA per tile, 32 warps; warp g marches the response to a unit guess
 // value in column g.  Coefficients are staged in shared memory.  The
@@ -456,7 +511,8 @@ __global__ void __launch_bounds__(1024)
   extern __shared__ __align__(16) unsigned char psm[];
   const int tile = blockIdx.x;
   const int a = tile % tg.tx, b = tile / tg.tx;
-  const int mw = tile_width(tg, a), hh = tile_height(tg, b), nb = tg.row_nb[b];
+  const int mw = tile_width(tg, a), hh = tile_height(tg, b);
+  const int nb = tg.grp_nb[(size_t)b * tg.txg + a / tg.tpw];
   const int i0 = a * tg.tm, j0 = b * tg.th;
   const int lane = threadIdx.x & 31, g = threadIdx.x >> 5;
   const int TM = 32;
@@ -605,11 +661,12 @@ struct sevp_ctx {
   bool have_op = false;
   // tiles
   TileGeom tg{};
-  int *d_row_nb = nullptr;
+  int *d_grp_nb = nullptr;
   long long *d_moff = nullptr;
   double *d_mats = nullptr;
   long long mats_elems = 0;
-  std::vector<int> row_nb;
+  std::vector<int> grp_nb;   // per warp group (ty * txg)
+  std::vector<int> tile_nb;  // effective sub-blocks per tile (ty * tx)
   // work vectors
   size_t n = 0;
   double *r64 = nullptr, *z64 = nullptr, *p64[2] = {nullptr, nullptr}, *q64 = nullptr;
@@ -618,6 +675,12 @@ struct sevp_ctx {
         *d32 = nullptr;
   double *bh = nullptr;  // device staging for host solves
   double *xh = nullptr;
+  double *e1h = nullptr, *e2h = nullptr;
+  // learned warm start (bound by the network module)
+  sevp_warmstart_fn warm_fn = nullptr;
+  void *warm_user = nullptr;
+  int warm_launches_per_call = 0;
+  const double *cur_b = nullptr;
   // device scalars
   SolveState *st = nullptr;
   SolveState *h_st = nullptr;  // pinned mirror
@@ -626,7 +689,39 @@ struct sevp_ctx {
   unsigned *tickets = nullptr;
   long long launches = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // optional per-kernel-class timing (CUDA events on the context stream)
+  int prof = 0;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pool;
+  size_t ev_used = 0;
+  std::vector<int> ev_class;  // 0 tile apply (pass B / precondition), 1 stencil
+  double prof_ms[4] = {0, 0, 0, 0};
+  long long prof_n[4] = {0, 0, 0, 0};
 };
+
+namespace {
+// Brackets one launch with a pair of events when profiling is on.
+struct ProfScope {
+  sevp_ctx *c;
+  int cls;
+  cudaEvent_t e1 = nullptr;
+  ProfScope(sevp_ctx *ctx, int k) : c(ctx), cls(k) {
+    if (!c->prof) return;
+    if (c->ev_used == c->ev_pool.size()) {
+      cudaEvent_t a, b;
+      cudaEventCreate(&a);
+      cudaEventCreate(&b);
+      c->ev_pool.push_back({a, b});
+    }
+    auto &pr = c->ev_pool[c->ev_used++];
+    c->ev_class.push_back(cls);
+    cudaEventRecord(pr.first, c->stream);
+    e1 = pr.second;
+  }
+  ~ProfScope() {
+    if (e1) cudaEventRecord(e1, c->stream);
+  }
+};
+}  // namespace
 
 namespace {
 thread_local char g_err[512] = {0};
@@ -663,6 +758,7 @@ static int launch_stencil(sevp_ctx *ctx, const Op &op, int ticket_slot) {
   int rpw = stencil_rpw(ctx->ny);
   dim3 grid = stencil_grid(ctx, rpw);
   GridDims gd{ctx->nx, ctx->ny, ctx->periodic};
+  ProfScope ps(ctx, 1);
   k_stencil<Op><<<grid, kStencilThreads, 0, ctx->stream>>>(gd, ctx->c, op, rpw, ctx->partials,
                                                           ctx->tickets + ticket_slot, ctx->st);
   ctx->launches++;
@@ -674,7 +770,7 @@ template <typename V, bool UPDATE, bool DOTS>
 static int launch_tile(sevp_ctx *ctx, V *x, const V *p, V *r, const V *q, V *z, int ticket_slot) {
   size_t warps = tile_warps(ctx->tg);
   unsigned blocks = (unsigned)((warps + kTileWarps - 1) / kTileWarps);
-  size_t smem = tile_smem_per_warp(ctx->tg.hmax, ctx->tg.nbmax, sizeof(V)) * kTileWarps;
+  size_t smem = tile_smem_per_warp(ctx->tg.hmax) * kTileWarps;
   auto kern = k_tile_apply<V, UPDATE, DOTS>;
   static thread_local size_t set_smem[8] = {0};
   const int key = (sizeof(V) == 8 ? 4 : 0) + (UPDATE ? 2 : 0) + (DOTS ? 1 : 0);
@@ -682,6 +778,7 @@ static int launch_tile(sevp_ctx *ctx, V *x, const V *p, V *r, const V *q, V *z, 
     SEVP_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     set_smem[key] = smem;
   }
+  ProfScope ps(ctx, UPDATE ? 0 : 2);
   kern<<<blocks, kTileWarps * 32, smem, ctx->stream>>>(ctx->tg, ctx->c, ctx->d_mats, x, p, r, q, z,
                                                       ctx->st, ctx->partials,
                                                       ctx->tickets + ticket_slot);
@@ -690,13 +787,46 @@ static int launch_tile(sevp_ctx *ctx, V *x, const V *p, V *r, const V *q, V *z, 
   return SEVP_OK;
 }
 
+// Folds recorded event pairs into per-class totals (synchronises the stream).
+static void prof_collect(sevp_ctx *ctx) {
+  if (!ctx->ev_used) return;
+  cudaStreamSynchronize(ctx->stream);
+  for (size_t k = 0; k < ctx->ev_used; ++k) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, ctx->ev_pool[k].first, ctx->ev_pool[k].second) == cudaSuccess) {
+      ctx->prof_ms[ctx->ev_class[k]] += ms;
+      ctx->prof_n[ctx->ev_class[k]] += 1;
+    }
+  }
+  ctx->ev_used = 0;
+  ctx->ev_class.clear();
+}
+
+extern "C" int sevp_profile(sevp_ctx *ctx, int enable) {
+  if (!ctx) return SEVP_BAD_ARG;
+  prof_collect(ctx);
+  ctx->prof = enable ? 1 : 0;
+  for (int k = 0; k < 4; ++k) ctx->prof_ms[k] = 0.0, ctx->prof_n[k] = 0;
+  return SEVP_OK;
+}
+
+extern "C" int sevp_profile_read(sevp_ctx *ctx, double *ms, long long *count) {
+  if (!ctx || !ms || !count) return SEVP_BAD_ARG;
+  prof_collect(ctx);
+  for (int k = 0; k < 4; ++k) ms[k] = ctx->prof_ms[k], count[k] = ctx->prof_n[k];
+  return SEVP_OK;
+}
+
 static void free_work(sevp_ctx *ctx) {
   void *ptrs[] = {ctx->r64, ctx->z64, ctx->p64[0], ctx->p64[1], ctx->q64, ctx->x64s, ctx->r32,
                   ctx->z32, ctx->p32[0], ctx->p32[1], ctx->q32, ctx->d32, ctx->bh, ctx->xh,
-                  ctx->d_row_nb, ctx->d_moff, ctx->d_mats, ctx->st, ctx->partials, ctx->tickets};
+                  ctx->e1h, ctx->e2h,
+                  ctx->d_grp_nb, ctx->d_moff, ctx->d_mats, ctx->st, ctx->partials, ctx->tickets};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (ctx->h_st) cudaFreeHost(ctx->h_st);
+  for (auto &pr : ctx->ev_pool) cudaEventDestroy(pr.first), cudaEventDestroy(pr.second);
+  ctx->ev_pool.clear();
 }
 
 extern "C" int sevp_create(sevp_ctx **out, int nx, int ny, int periodic, void *stream) {
@@ -761,6 +891,15 @@ extern "C" int sevp_destroy(sevp_ctx *ctx) {
 }
 
 extern "C" long long sevp_kernel_launches(const sevp_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+extern "C" int sevp_tile_layout(const sevp_ctx *ctx, int *tiles_x, int *tiles_y, int *nb_per_tile) {
+  if (!ctx || !ctx->have_op || !tiles_x || !tiles_y) return SEVP_BAD_ARG;
+  *tiles_x = ctx->tg.tx;
+  *tiles_y = ctx->tg.ty;
+  if (nb_per_tile)
+    for (size_t t = 0; t < ctx->tile_nb.size(); ++t) nb_per_tile[t] = ctx->tile_nb[t];
+  return SEVP_OK;
+}
 extern "C" long long sevp_influence_bytes(const sevp_ctx *ctx) {
   return ctx ? ctx->mats_elems * 8 : 0;
 }
@@ -770,6 +909,7 @@ extern "C" int sevp_set_operator(sevp_ctx *ctx, const float *al, const float *ab
   if (!ctx || !al || !ab || !ac || !ar || !at || !tl) return SEVP_BAD_ARG;
   const int tm = tl->tile_m, th = tl->tile_h;
   if (tm < 1 || tm > 32 || th < 1 || th > 32 || tl->sub_rows < 1) return SEVP_BAD_ARG;
+  // the tile geometry needs ceil(nx/tm) etc. before the growth kernel runs
   ctx->c = Coeffs{al, ab, ac, ar, at};
   TileGeom &tg = ctx->tg;
   tg.nx = ctx->nx, tg.ny = ctx->ny, tg.tm = tm, tg.th = th;
@@ -779,37 +919,62 @@ extern "C" int sevp_set_operator(sevp_ctx *ctx, const float *al, const float *ab
   tg.tpw = 32 / tg.wseg;
   tg.txg = ceil_div(tg.tx, tg.tpw);
   tg.hmax = th;
-  ctx->row_nb.assign(tg.ty, 1);
-  int nbmax = 1;
-  for (int b = 0; b < tg.ty; ++b) {
-    int s = tl->sub_rows_by_tile_row ? tl->sub_rows_by_tile_row[b] : tl->sub_rows;
-    if (s < 1) return SEVP_BAD_ARG;
-    int hh = tile_height(tg, b);
-    int nb = ceil_div(hh, s);
-    ctx->row_nb[b] = nb;
-    nbmax = std::max(nbmax, nb);
+  // sub-block height per tile
+  const int ntiles = tg.tx * tg.ty;
+  std::vector<int> s_tile(ntiles, std::max(1, tl->sub_rows));
+  if (tl->sub_rows_by_tile) {
+    for (int t = 0; t < ntiles; ++t) s_tile[t] = tl->sub_rows_by_tile[t];
+  } else if (tl->sub_rows_by_tile_row) {
+    for (int t = 0; t < ntiles; ++t) s_tile[t] = tl->sub_rows_by_tile_row[t / tg.tx];
+  } else if (tl->growth_limit > 1.0) {
+    int *d_s = nullptr;
+    SEVP_CUDA_TRY(cudaMalloc((void **)&d_s, sizeof(int) * ntiles));
+    k_tile_growth<<<(ntiles + 7) / 8, 256, 0, ctx->stream>>>(tg, ctx->c, log(tl->growth_limit), d_s);
+    ctx->launches++;
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(s_tile.data(), d_s, sizeof(int) * ntiles, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(d_s);
+    if (e != cudaSuccess) {
+      sevp_internal_set_error(e, "tile growth", __FILE__, __LINE__);
+      return SEVP_CUDA_ERROR;
+    }
   }
+  ctx->grp_nb.assign((size_t)tg.ty * tg.txg, 1);
+  for (int t = 0; t < ntiles; ++t) {
+    const int a = t % tg.tx, b = t / tg.tx;
+    if (s_tile[t] < 1) return SEVP_BAD_ARG;
+    const int nb = ceil_div(tile_height(tg, b), std::min(s_tile[t], tile_height(tg, b)));
+    int &g = ctx->grp_nb[(size_t)b * tg.txg + a / tg.tpw];
+    g = std::max(g, nb);
+  }
+  int nbmax = 1;
+  for (int v : ctx->grp_nb) nbmax = std::max(nbmax, v);
   tg.nbmax = nbmax;
-  std::vector<long long> moff((size_t)tg.ty * tg.tx);
+  ctx->tile_nb.assign(ntiles, 1);
+  std::vector<long long> moff((size_t)ntiles);
   long long off = 0;
   for (int b = 0; b < tg.ty; ++b)
     for (int a = 0; a < tg.tx; ++a) {
-      int mw = tile_width(tg, a), nb = ctx->row_nb[b];
+      const int mw = tile_width(tg, a), nb = ctx->grp_nb[(size_t)b * tg.txg + a / tg.tpw];
+      ctx->tile_nb[(size_t)b * tg.tx + a] = nb;
       moff[(size_t)b * tg.tx + a] = off;
       off += (long long)(2 * nb - 1) * mw * mw;
+      off = (off + 1) & ~1LL;  // 16-byte aligned start for every tile
     }
   ctx->mats_elems = off;
-  if (ctx->d_row_nb) cudaFree(ctx->d_row_nb), ctx->d_row_nb = nullptr;
+  if (ctx->d_grp_nb) cudaFree(ctx->d_grp_nb), ctx->d_grp_nb = nullptr;
   if (ctx->d_moff) cudaFree(ctx->d_moff), ctx->d_moff = nullptr;
   if (ctx->d_mats) cudaFree(ctx->d_mats), ctx->d_mats = nullptr;
-  SEVP_CUDA_TRY(cudaMalloc((void **)&ctx->d_row_nb, sizeof(int) * tg.ty));
+  SEVP_CUDA_TRY(cudaMalloc((void **)&ctx->d_grp_nb, sizeof(int) * ctx->grp_nb.size()));
   SEVP_CUDA_TRY(cudaMalloc((void **)&ctx->d_moff, sizeof(long long) * moff.size()));
   SEVP_CUDA_TRY(cudaMalloc((void **)&ctx->d_mats, sizeof(double) * std::max<long long>(off, 1)));
-  SEVP_CUDA_TRY(cudaMemcpyAsync(ctx->d_row_nb, ctx->row_nb.data(), sizeof(int) * tg.ty,
+  SEVP_CUDA_TRY(cudaMemcpyAsync(ctx->d_grp_nb, ctx->grp_nb.data(), sizeof(int) * ctx->grp_nb.size(),
                                 cudaMemcpyHostToDevice, ctx->stream));
   SEVP_CUDA_TRY(cudaMemcpyAsync(ctx->d_moff, moff.data(), sizeof(long long) * moff.size(),
                                 cudaMemcpyHostToDevice, ctx->stream));
-  tg.row_nb = ctx->d_row_nb;
+  tg.grp_nb = ctx->d_grp_nb;
   tg.moff = ctx->d_moff;
   // partial-sum capacity for the tile grid
   size_t tblocks = (tile_warps(tg) + kTileWarps - 1) / kTileWarps;
@@ -819,8 +984,7 @@ extern "C" int sevp_set_operator(sevp_ctx *ctx, const float *al, const float *ab
     SEVP_CUDA_TRY(cudaMalloc((void **)&ctx->partials, ctx->partials_n * 8));
   }
   // tile-apply shared memory must fit
-  size_t smem64 = tile_smem_per_warp(tg.hmax, tg.nbmax, 8) * kTileWarps;
-  if (smem64 > 220 * 1024) return SEVP_BAD_ARG;
+  if (tile_smem_per_warp(tg.hmax) * kTileWarps > 220 * 1024) return SEVP_BAD_ARG;
   // precompute
   int *d_status = nullptr;
   SEVP_CUDA_TRY(cudaMalloc((void **)&d_status, sizeof(int)));
@@ -908,6 +1072,7 @@ static int pcg_loop(sevp_ctx *ctx, V *x, V *r, V *z, V *p0, V *p1, V *q, int che
     }
     int s = read_state(ctx);
     if (s) return s;
+    prof_collect(ctx);
     if (ctx->h_st->done) break;
   }
   *iters_out = ctx->h_st->iter;
@@ -1048,6 +1213,76 @@ extern "C" int sevp_solve_host(sevp_ctx *ctx, const double *bh, double *xh,
     sevp_internal_set_error(e, "copy x to host", __FILE__, __LINE__);
     return SEVP_CUDA_ERROR;
   }
+  return s;
+}
+
+// guess = 2 eta1 - eta2 (mode 2), eta1 (mode 1) or 0 (mode 0)
+__global__ void k_guess(const double *eta1, const double *eta2, double *g, size_t n, int mode) {
+  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += (size_t)gridDim.x * blockDim.x) {
+    double v = 0.0;
+    if (mode == 1) v = eta1[k];
+    if (mode == 2) v = 2.0 * eta1[k] - eta2[k];
+    g[k] = v;
+  }
+}
+
+static int form_guess(sevp_ctx *ctx, const double *eta1, const double *eta2, double *x, int mode) {
+  if (mode == SEVP_GUESS_LEARNED) {
+    if (!ctx->warm_fn) return SEVP_BAD_ARG;
+    int s = ctx->warm_fn(ctx->warm_user, eta1, eta2, ctx->cur_b, x, ctx->nx, ctx->ny,
+                         (void *)ctx->stream);
+    ctx->launches += ctx->warm_launches_per_call;
+    return s;
+  }
+  if (mode < 0 || mode > 2 || (mode >= 1 && !eta1) || (mode == 2 && !eta2)) return SEVP_BAD_ARG;
+  unsigned blocks = (unsigned)std::min<size_t>((ctx->n + 255) / 256, 148 * 16);
+  k_guess<<<blocks, 256, 0, ctx->stream>>>(eta1, eta2, x, ctx->n, mode);
+  ctx->launches++;
+  SEVP_CUDA_TRY(cudaGetLastError());
+  return SEVP_OK;
+}
+
+extern "C" int sevp_set_warmstart(sevp_ctx *ctx, sevp_warmstart_fn fn, void *user,
+                                  int launches_per_call) {
+  if (!ctx) return SEVP_BAD_ARG;
+  ctx->warm_fn = fn;
+  ctx->warm_user = user;
+  ctx->warm_launches_per_call = launches_per_call;
+  return SEVP_OK;
+}
+
+extern "C" int sevp_solve_step(sevp_ctx *ctx, const double *b, const double *eta1,
+                               const double *eta2, double *x, int guess_mode,
+                               const sevp_solve_opts *o, sevp_report *rep) {
+  if (!ctx || !ctx->have_op || !b || !x || !o) return SEVP_BAD_ARG;
+  ctx->cur_b = b;
+  int s = form_guess(ctx, eta1, eta2, x, guess_mode);
+  if (s) return s;
+  sevp_solve_opts oo = *o;
+  oo.use_guess = 1;
+  return sevp_solve(ctx, b, x, &oo, rep);
+}
+
+extern "C" int sevp_solve_step_host(sevp_ctx *ctx, const double *bh, const double *eta1h,
+                                    const double *eta2h, double *xh, int guess_mode,
+                                    const sevp_solve_opts *o, sevp_report *rep) {
+  if (!ctx || !bh || !xh || !o) return SEVP_BAD_ARG;
+  if (!ctx->bh) SEVP_CUDA_TRY(cudaMalloc((void **)&ctx->bh, ctx->n * 8));
+  if (!ctx->xh) SEVP_CUDA_TRY(cudaMalloc((void **)&ctx->xh, ctx->n * 8));
+  if (!ctx->e1h) SEVP_CUDA_TRY(cudaMalloc((void **)&ctx->e1h, ctx->n * 8));
+  if (!ctx->e2h) SEVP_CUDA_TRY(cudaMalloc((void **)&ctx->e2h, ctx->n * 8));
+  const size_t bytes = ctx->n * 8;
+  SEVP_CUDA_TRY(cudaMemcpyAsync(ctx->bh, bh, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  if (guess_mode >= 1 && eta1h)
+    SEVP_CUDA_TRY(cudaMemcpyAsync(ctx->e1h, eta1h, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  if ((guess_mode == 2 || guess_mode == SEVP_GUESS_LEARNED) && eta2h)
+    SEVP_CUDA_TRY(cudaMemcpyAsync(ctx->e2h, eta2h, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  int s = sevp_solve_step(ctx, ctx->bh, eta1h ? ctx->e1h : nullptr, eta2h ? ctx->e2h : nullptr,
+                          ctx->xh, guess_mode, o, rep);
+  if (s != SEVP_OK && s != SEVP_MAXITER) return s;
+  SEVP_CUDA_TRY(cudaMemcpyAsync(xh, ctx->xh, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  SEVP_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   return s;
 }
 

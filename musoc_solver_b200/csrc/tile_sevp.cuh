@@ -8,8 +8,10 @@
 // equations are solved exactly with zero Dirichlet data outside the tile by
 // SEVP marching in the north direction.  A tile of hh rows is split into nb
 // sub-blocks whose boundaries are k_t = (t * hh) / nb, t = 0..nb; nb is set
-// per tile row (latitude band) so that the marching error growth, which
-// depends on the local coefficient anisotropy, stays bounded.
+// per tile so that the marching error growth, which depends on the local
+// coefficient anisotropy (and is largest over land, where the free-surface
+// term dominates the floored depths), stays bounded.  The tiles that share a
+// warp (a group of tpw neighbours in a tile row) share nb.
 //
 // Influence data per tile, all FP64, mw x mw, element [k][n] at k * mw + n
 // (k = input column, n = output column):
@@ -30,7 +32,7 @@ struct TileGeom {
   int txg;    // tile groups per tile row = ceil(tx / tpw)
   int hmax;   // max tile height (= th)
   int nbmax;  // max sub-blocks per tile
-  const int *row_nb;         // [ty] sub-blocks per tile of tile row b
+  const int *grp_nb;         // [ty * txg] sub-blocks of the tiles of one warp group
   const long long *moff;     // [ty * tx] offset of each tile's influence data
 };
 

@@ -23,6 +23,8 @@ SEVP_BAD_ARG = 5
 SEVP_CUDA_ERROR = 6
 SEVP_SINGULAR = 7
 
+GUESS_ZERO, GUESS_PREVIOUS, GUESS_LINEAR, GUESS_LEARNED = 0, 1, 2, 3
+
 
 class SevpError(RuntimeError):
     def __init__(self, status: int, what: str = ""):
@@ -36,7 +38,8 @@ class SevpError(RuntimeError):
 
 class Tiling(C.Structure):
     _fields_ = [("tile_m", C.c_int), ("tile_h", C.c_int), ("sub_rows", C.c_int),
-                ("sub_rows_by_tile_row", C.POINTER(C.c_int))]
+                ("sub_rows_by_tile_row", C.POINTER(C.c_int)),
+                ("sub_rows_by_tile", C.POINTER(C.c_int)), ("growth_limit", C.c_double)]
 
 
 class SolveOpts(C.Structure):
@@ -77,6 +80,13 @@ _SIGS = {
     "sevp_precondition_f32": ([P, P, P], C.c_int),
     "sevp_relative_residual": ([P, P, P, DP], C.c_int),
     "sevp_kernel_launches": ([P], C.c_longlong),
+    "sevp_tile_layout": ([P, IP, IP, IP], C.c_int),
+    "sevp_profile": ([P, C.c_int], C.c_int),
+    "sevp_set_warmstart": ([P, P, P, C.c_int], C.c_int),
+    "sevp_solve_step": ([P, P, P, P, P, C.c_int, C.POINTER(SolveOpts), C.POINTER(Report)], C.c_int),
+    "sevp_solve_step_host": ([P, P, P, P, P, C.c_int, C.POINTER(SolveOpts), C.POINTER(Report)],
+                             C.c_int),
+    "sevp_profile_read": ([P, DP, C.POINTER(C.c_longlong)], C.c_int),
     # Fortran-compatible drop-ins (all pointers)
     "rep1_": ([P] * 17, None),
     "rep_": ([P] * 17, None),
@@ -92,7 +102,7 @@ _SIGS = {
     "p_bicgstab_le_": ([P] * 14, None),
     "p_csi_": ([P] * 16, None),
     "lanczos_": ([P] * 9, None),
-    "sevp_bir_sweeps_": ([P] * 16, None),
+    "sevp_bir_sweeps_": ([P] * 17, None),
     "sevp_pre_strips_": ([P] * 12, None),
 }
 

@@ -44,6 +44,46 @@ def default_sub_rows(problem_or_ratio, tile_h: int, growth_limit: float = 1e6) -
     return out
 
 
+def tile_sub_blocks(problem, tile_m: int, tile_h: int, growth_limit: float = 1e10) -> np.ndarray:
+    """Sub-blocks per tile, shape (tiles_y, tiles_x): the host statement of
+    the library's per-tile rule (k_tile_growth + the warp-group maximum).
+
+    Each tile's height is the largest s with z**s <= growth_limit, where
+    z + 1/z is the largest (|AC|+|AL|+|AR|)/|AT| over the tile's marched
+    rows; tiles that share a warp (groups of 32/W neighbours, W the lane
+    segment width 8/16/32) use the largest sub-block count of the group.
+    """
+    p = problem
+    al, ab, ac, ar, at = (np.abs(a.astype(np.float64)) for a in p.coeffs())
+    nx, ny = p.nx, p.ny
+    tx, ty = -(-nx // tile_m), -(-ny // tile_h)
+    wseg = 8 if tile_m <= 8 else (16 if tile_m <= 16 else 32)
+    tpw = 32 // wseg
+    out = np.ones((ty, tx), np.int64)
+    for b in range(ty):
+        j0 = b * tile_h
+        hh = min(tile_h, ny - j0)
+        rows = slice(j0, j0 + hh - 1)  # marched rows: all but the tile's last
+        for a in range(tx):
+            cols = slice(a * tile_m, min(nx, (a + 1) * tile_m))
+            s = tile_h
+            if hh > 1:
+                atv = at[rows, cols]
+                if (atv == 0).any():
+                    s = 1
+                else:
+                    c = max(2.0, float(((ac[rows, cols] + al[rows, cols] + ar[rows, cols]) / atv).max()))
+                    z = 0.5 * (c + np.sqrt(max(c * c - 4.0, 0.0)))
+                    if z > 1.0:
+                        s = int(np.floor(np.log(growth_limit) / np.log(z)))
+            s = max(1, min(tile_h, s))
+            out[b, a] = -(-hh // min(s, hh))
+    for b in range(ty):
+        for g in range(0, tx, tpw):
+            out[b, g:g + tpw] = out[b, g:g + tpw].max()
+    return out.astype(np.int32)
+
+
 @dataclass
 class SolveResult:
     status: int
@@ -74,14 +114,27 @@ class SevpSolver:
         N.check(N.lib().sevp_create(C.byref(h), self.nx, self.ny, int(problem.periodic),
                                     C.c_void_p(self.stream.cuda_stream)), "sevp_create")
         self.h = h
-        if sub_rows is None:
-            sub_rows = default_sub_rows(problem, tile_h, growth_limit)
-        sub_rows = list(np.broadcast_to(np.asarray(sub_rows, np.int32), (-(-self.ny // tile_h),)))
-        self._srow = (C.c_int * len(sub_rows))(*sub_rows)
-        self.sub_rows = sub_rows
-        self.tiling = N.Tiling(tile_m, tile_h, int(max(sub_rows)), self._srow)
+        self.tile_m, self.tile_h = tile_m, tile_h
+        if sub_rows is not None:
+            # explicit heights per tile row
+            rows = list(np.broadcast_to(np.asarray(sub_rows, np.int32), (-(-self.ny // tile_h),)))
+            self._srow = (C.c_int * len(rows))(*rows)
+            self.tiling = N.Tiling(tile_m, tile_h, int(max(rows)), self._srow, None, 0.0)
+        else:
+            # heights per tile from the marching growth bound (computed on the GPU)
+            self.tiling = N.Tiling(tile_m, tile_h, tile_h, None, None, float(growth_limit))
         N.check(N.lib().sevp_set_operator(self.h, *[N.ptr(t) for t in self.coef],
                                           C.byref(self.tiling)), "sevp_set_operator")
+        self.tile_nb = self.layout()
+
+    def layout(self) -> np.ndarray:
+        """Sub-blocks used by each tile, shape (tiles_y, tiles_x)."""
+        tx, ty = C.c_int(), C.c_int()
+        N.check(N.lib().sevp_tile_layout(self.h, C.byref(tx), C.byref(ty), None), "sevp_tile_layout")
+        out = np.zeros(tx.value * ty.value, np.int32)
+        N.check(N.lib().sevp_tile_layout(self.h, C.byref(tx), C.byref(ty),
+                                         out.ctypes.data_as(C.POINTER(C.c_int))), "sevp_tile_layout")
+        return out.reshape(ty.value, tx.value)
 
     def close(self):
         if getattr(self, "h", None):
@@ -100,6 +153,17 @@ class SevpSolver:
 
     def launches(self) -> int:
         return int(N.lib().sevp_kernel_launches(self.h))
+
+    def profile(self, enable: bool = True):
+        """Starts (zeroes) or stops per-kernel-class CUDA-event timing."""
+        N.check(N.lib().sevp_profile(self.h, int(enable)), "sevp_profile")
+
+    def profile_read(self):
+        """{class: (total_ms, launches)} for 'tile', 'stencil', 'precond'."""
+        ms = (C.c_double * 4)()
+        n = (C.c_longlong * 4)()
+        N.check(N.lib().sevp_profile_read(self.h, ms, n), "sevp_profile_read")
+        return {"tile": (ms[0], n[0]), "stencil": (ms[1], n[1]), "precond": (ms[2], n[2])}
 
     def opts(self, precision=0, tol=1e-12, max_iter=5000, inner_tol=1e-5, use_guess=False,
              check_every=4):
@@ -135,6 +199,33 @@ class SevpSolver:
             raise N.SevpError(s, "sevp_solve_host")
         return out, SolveResult(rep.status, rep.iterations, rep.refinements, rep.rel_residual,
                                 rep.bnorm, rep.ms)
+
+    def solve_step(self, b, eta1, eta2, x, guess=N.GUESS_LINEAR, precision=1, tol=1e-12,
+                   max_iter=5000, inner_tol=1e-5, check_every=4):
+        """One sequence step on device tensors: x <- guess(eta1, eta2, b), then
+        solve from it."""
+        o = self.opts(precision, tol, max_iter, inner_tol, True, check_every)
+        rep = N.Report()
+        s = N.lib().sevp_solve_step(self.h, N.ptr(b), N.ptr(eta1) if eta1 is not None else None,
+                                    N.ptr(eta2) if eta2 is not None else None, N.ptr(x), int(guess),
+                                    C.byref(o), C.byref(rep))
+        if s not in (N.SEVP_OK, N.SEVP_MAXITER):
+            raise N.SevpError(s, "sevp_solve_step")
+        return x, SolveResult(rep.status, rep.iterations, rep.refinements, rep.rel_residual,
+                              rep.bnorm, rep.ms)
+
+    def solve_step_host(self, b, eta1, eta2, x, guess=N.GUESS_LINEAR, precision=1, tol=1e-12,
+                        max_iter=5000, inner_tol=1e-5, check_every=4):
+        """One sequence step with host (numpy, ideally pinned) buffers."""
+        o = self.opts(precision, tol, max_iter, inner_tol, True, check_every)
+        rep = N.Report()
+        s = N.lib().sevp_solve_step_host(self.h, N.ptr(b), N.ptr(eta1) if eta1 is not None else None,
+                                         N.ptr(eta2) if eta2 is not None else None, N.ptr(x),
+                                         int(guess), C.byref(o), C.byref(rep))
+        if s not in (N.SEVP_OK, N.SEVP_MAXITER):
+            raise N.SevpError(s, "sevp_solve_step_host")
+        return x, SolveResult(rep.status, rep.iterations, rep.refinements, rep.rel_residual,
+                              rep.bnorm, rep.ms)
 
     def apply(self, x):
         y = self.torch.empty_like(x)

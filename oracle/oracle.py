@@ -69,7 +69,7 @@ def lib():
         L.or_ratqr.argtypes = [C.c_int, C.c_double, f64p, f64p, C.POINTER(C.c_double)]
         L.or_ratqr.restype = C.c_int
         L.or_bir_sweeps.argtypes = (c5 + [f32p, f64p, f64p, f64p, f64p, f64p] + [f32p] * 6
-                                    + [f64p, f64p, f64p, i32p] + [C.c_int] * 6)
+                                    + [f64p, f64p, f64p, i32p] + [C.c_int] * 7)
         L.or_pre_strips.argtypes = c5 + [f64p, f64p, f64p, i32p] + [C.c_int] * 4 + [f32p] * 5
         L.or_pre_strips.restype = C.c_int
         L.or_assemble.argtypes = ([C.c_int] * 3 + [f32p] * 6 + [i32p, i32p, C.c_int, C.c_float, C.c_int]
@@ -218,13 +218,22 @@ def assemble(i2, j2, k1, odx, ody, csv, ocs, odyv, odz, iu, iv, nbir, gamma, ide
 class TilePC:
     """Oracle of the block-Jacobi tile SEVP preconditioner (new method)."""
 
-    def __init__(self, p, tm, th, srow):
+    def __init__(self, p, tm, th, srow=None, tile_nb=None):
+        """srow: sub-block height per tile row (scalar or ty values), or
+        tile_nb: sub-blocks per tile, shape (ty, tx)."""
         self.p = p
         self.c = [_c(a, np.float32) for a in p.coeffs()]
         ty = (p.ny + th - 1) // th
-        srow = np.broadcast_to(np.asarray(srow, np.int32), (ty,)).copy()
+        tx = (p.nx + tm - 1) // tm
+        if tile_nb is None:
+            srow = np.broadcast_to(np.asarray(srow, np.int64), (ty,))
+            hh = np.minimum(th, p.ny - th * np.arange(ty))
+            nb_row = -(-hh // np.maximum(srow, 1))
+            tile_nb = np.repeat(nb_row[:, None], tx, axis=1)
+        tile_nb = np.ascontiguousarray(np.asarray(tile_nb).reshape(ty, tx), np.int32)
+        self.tile_nb = tile_nb
         st = C.c_int()
-        self.h = lib().or_tile_setup(*self.c, p.nx, p.ny, tm, th, srow, C.byref(st))
+        self.h = lib().or_tile_setup(*self.c, p.nx, p.ny, tm, th, tile_nb, C.byref(st))
         self.status = st.value
 
     def __del__(self):

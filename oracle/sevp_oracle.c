@@ -731,7 +731,13 @@ int or_ratqr(int n, double eps1, const double *d, const double *e, double *minei
     tot = 0.0;
   else
     for (i = 1; i <= n; ++i) w[i] = w[i] - tot;
-  for (;;) {
+  /* The reference loops without bound; a NaN/Inf input never meets its
+   * exits, so the restatement stops after 100000 sweeps with ierr = 2. */
+  for (int sweep = 0;; ++sweep) {
+    if (sweep >= 100000) {
+      free(e2), free(bd), free(w);
+      return 2;
+    }
     tot = tot + s;
     delta = w[n] - s;
     i = n;
@@ -830,6 +836,10 @@ int or_lanczos(const float *al, const float *ab, const float *ac, const float *a
 }
 
 /* M/fs_GLOBAL.f90:1904-1966: NITER sweeps of overlapping BIR strips.
+ * The reference sets the wrapped strip's side boundaries XX(1,J) and
+ * XX(IBIR+2,J) for J = 1..J2 only (:1925-1926), so the top interior row
+ * J2+1 keeps a stale (zero) boundary; fix_wrap != 0 also copies rows J2+1
+ * and J2+2 (an opt-in correction, not reference behaviour).
  * S (I2,J2) FP32; AL..AT (I2,J2); X (I0,J0); RINV (IBIR,IBIR,NB0,NBIR),
  * RINV1 (IBIR,IBIR,NB0-1,NBIR); workspaces SRC/CL..CT (IBIR,J2), XX and H
  * (IBIR+2,J0), DUM0 (IBIR,NB0-1), DUM1/DUM2 (IBIR).  XX is caller-owned so
@@ -838,7 +848,7 @@ void or_bir_sweeps(const float *AL, const float *AB, const float *AC, const floa
                    const float *AT, const float *S, const double *RINV, const double *RINV1,
                    double *X, double *XX, double *H, float *SRC, float *CL, float *CB, float *CC,
                    float *CR, float *CT, double *DUM0, double *DUM1, double *DUM2, const int *IE,
-                   int I2, int J2, int NB0, int NBIR, int niter, int periodic) {
+                   int I2, int J2, int NB0, int NBIR, int niter, int periodic, int fix_wrap) {
   int I0 = I2 + 2, I1 = I2 + 1, J1 = J2 + 1;
   int IBIR = 2 * I2 / NBIR, INC = IBIR / 2;
   size_t rstride = (size_t)IBIR * IBIR * NB0, r1stride = (size_t)IBIR * IBIR * (NB0 > 1 ? NB0 - 1 : 1);
@@ -854,6 +864,11 @@ void or_bir_sweeps(const float *AL, const float *AB, const float *AC, const floa
                   R1, DUM0, DUM1, DUM2, SRC, H, X + (il - 1), IE, I0, I2, IBIR + 2, IBIR, NB0);
       } else {
         int ir = il + INC, ir2 = il + IBIR - 1;
+        if (fix_wrap)
+          for (int j = J2 + 1; j <= J2 + 2; ++j) {
+            XX[IX(IBIR + 2, 1, j)] = X[IX(I0, il, j)];
+            XX[IX(IBIR + 2, IBIR + 2, j)] = X[IX(I0, INC + 2, j)];
+          }
         for (int j = 1; j <= J2; ++j) {
           XX[IX(IBIR + 2, 1, j)] = X[IX(I0, il, j)];
           XX[IX(IBIR + 2, IBIR + 2, j)] = X[IX(I0, INC + 2, j)];
@@ -937,11 +952,11 @@ int or_pre_strips(const float *AL, const float *AB, const float *AC, const float
 /* ======================================================================== */
 
 /* Tile layout: tiles of at most tm columns x th rows, clipped at the domain
- * edge.  A tile of hh rows is split into nb = ceil(hh / s) sub-blocks with
- * boundaries k_t = (t * hh) / nb, t = 0..nb.  s is given per tile row. */
+ * edge.  A tile of hh rows is split into nb sub-blocks (given per tile) with
+ * boundaries k_t = (t * hh) / nb, t = 0..nb. */
 typedef struct {
   int nx, ny, tm, th, tx, ty;
-  const int *srow; /* sub-block height per tile row (ty entries) */
+  const int *tile_nb; /* sub-blocks per tile (ty * tx entries, tile rows first) */
 } tiles_t;
 
 static void tile_geom(const tiles_t *T, int a, int b, int *i0, int *j0, int *mw, int *hh, int *nb) {
@@ -949,9 +964,10 @@ static void tile_geom(const tiles_t *T, int a, int b, int *i0, int *j0, int *mw,
   *j0 = b * T->th;
   *mw = T->nx - *i0 < T->tm ? T->nx - *i0 : T->tm;
   *hh = T->ny - *j0 < T->th ? T->ny - *j0 : T->th;
-  int s = T->srow[b];
-  if (s < 1) s = 1;
-  *nb = (*hh + s - 1) / s;
+  int v = T->tile_nb[b * T->tx + a];
+  if (v < 1) v = 1;
+  if (v > *hh) v = *hh;
+  *nb = v;
 }
 
 /* Influence data of one tile (RINV, RINV1 in the reference's (m,m,nb)
@@ -976,15 +992,15 @@ static void tile_coeffs(const float *c, int nx, int i0, int j0, int mw, int hh, 
 /* Builds the tile preconditioner.  Coefficients are (nx, ny) column-major:
  * element (i, j) (0-based) at j * nx + i.  Returns NULL on a singular tile. */
 tile_pc_t *or_tile_setup(const float *al, const float *ab, const float *ac, const float *ar,
-                         const float *at, int nx, int ny, int tm, int th, const int *srow,
+                         const float *at, int nx, int ny, int tm, int th, const int *tile_nb,
                          int *status) {
   tile_pc_t *pc = (tile_pc_t *)calloc(1, sizeof(tile_pc_t));
   pc->T.nx = nx, pc->T.ny = ny, pc->T.tm = tm, pc->T.th = th;
   pc->T.tx = (nx + tm - 1) / tm;
   pc->T.ty = (ny + th - 1) / th;
-  int *sr = (int *)malloc(sizeof(int) * pc->T.ty);
-  memcpy(sr, srow, sizeof(int) * pc->T.ty);
-  pc->T.srow = sr;
+  int *sr = (int *)malloc(sizeof(int) * pc->T.ty * pc->T.tx);
+  memcpy(sr, tile_nb, sizeof(int) * pc->T.ty * pc->T.tx);
+  pc->T.tile_nb = sr;
   pc->ntiles = pc->T.tx * pc->T.ty;
   pc->td = (tile_data_t *)calloc((size_t)pc->ntiles, sizeof(tile_data_t));
   int st = 0;
@@ -1023,7 +1039,7 @@ void or_tile_free(tile_pc_t *pc) {
   for (int t = 0; t < pc->ntiles; ++t) {
     free(pc->td[t].rinv), free(pc->td[t].rinv1), free(pc->td[t].ie);
   }
-  free((void *)pc->T.srow);
+  free((void *)pc->T.tile_nb);
   free(pc->td);
   free(pc);
 }
@@ -1125,13 +1141,17 @@ int or_pcg(const tile_pc_t *pc, const float *al, const float *ab, const float *a
     or_apply(al, ab, ac, ar, at, nx, ny, periodic, x, q);
     for (size_t k = 0; k < n; ++k) r[k] = b[k] - q[k];
     rel = sqrt(or_dot(r, r, nx, ny)) / bn;
-    if (rel <= tol || it >= maxit) break;
+    if (rel <= tol || it >= maxit || !isfinite(rel)) break;
     or_tile_apply(pc, al, ab, ac, ar, at, r, z);
     memcpy(p, z, n * 8);
     double rz = or_dot(r, z, nx, ny);
     while (it < maxit) {
       or_apply(al, ab, ac, ar, at, nx, ny, periodic, p, q);
       double pq = or_dot(p, q, nx, ny);
+      if (!isfinite(pq) || pq == 0.0) {
+        it = maxit;
+        break;
+      }
       double alpha = rz / pq;
       for (size_t k = 0; k < n; ++k) {
         x[k] += alpha * p[k];
@@ -1139,6 +1159,10 @@ int or_pcg(const tile_pc_t *pc, const float *al, const float *ab, const float *a
       }
       ++it;
       double rr = or_dot(r, r, nx, ny);
+      if (!isfinite(rr)) {
+        it = maxit;
+        break;
+      }
       if (sqrt(rr) / bn <= tol) break;
       or_tile_apply(pc, al, ab, ac, ar, at, r, z);
       double rz2 = or_dot(r, z, nx, ny);

@@ -1,0 +1,94 @@
+"""The C-ABI library loads without a GPU and exports every symbol the header
+declares; the host-side helpers behave (no kernel launches here)."""
+import os
+import re
+
+import numpy as np
+
+from musoc_solver_b200 import build, native, problems as P
+from musoc_solver_b200.solver import default_sub_rows, tile_sub_blocks
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    names = []
+    for h in ("sevp_b200.h",):
+        txt = open(os.path.join(ROOT, "include", h)).read()
+        txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+        txt = re.sub(r"typedef[^;]*;", "", txt, flags=re.S)
+        for m in re.finditer(r"^\s*(?:const\s+)?[A-Za-z_][\w\s\*]*?\b([a-z_][a-z0-9_]*)\s*\(", txt, re.M):
+            names.append(m.group(1))
+    return sorted(set(n for n in names if n not in ("defined",)))
+
+
+def test_library_builds_and_exports_header_symbols():
+    lib_path = build.build()
+    assert os.path.exists(lib_path)
+    L = native.lib()
+    declared = _declared()
+    assert len(declared) >= 30
+    missing = [n for n in declared if not hasattr(L, n)]
+    assert not missing, missing
+    # the Python binding covers the same set
+    assert set(native.exported_symbols()) <= set(declared) | {"sevp_bir_sweeps_", "sevp_pre_strips_"}
+
+
+def test_status_strings():
+    L = native.lib()
+    assert native.status_string(0) == "ok"
+    assert "singular" in native.status_string(7)
+
+
+def test_bad_args_without_gpu():
+    import ctypes as C
+
+    L = native.lib()
+    h = C.c_void_p()
+    assert L.sevp_create(C.byref(h), 0, 10, 0, None) == native.SEVP_BAD_ARG
+    assert L.sevp_solve(None, None, None, None, None) == native.SEVP_BAD_ARG
+
+
+def test_sub_rows_respect_growth_bound():
+    p = P.global_grid(180, 90, seed=2)
+    for gl in (1e6, 1e10):
+        s = default_sub_rows(p, 16, gl)
+        assert len(s) == -(-p.ny // 16)
+        assert all(1 <= v <= 16 for v in s)
+    assert sum(default_sub_rows(p, 16, 1e10)) >= sum(default_sub_rows(p, 16, 1e6))
+    # isotropic Laplacian with no shift: z ~ 5.83 per row -> 7 rows for 1e6
+    q = P.idealised(40, 32)
+    q.ac[:] = 1.0
+    assert default_sub_rows(q, 16, 1e6)[0] == 7
+
+
+def test_problem_generators_shapes_and_symmetry():
+    for p in (P.basin(0), P.global_grid(120, 60, seed=1)):
+        assert p.al.dtype == np.float32 and p.b.dtype == np.float64
+        assert p.ac.shape == (p.ny, p.nx)
+        # symmetric: AR(i,j) == AL(i+1,j), AT(i,j) == AB(i,j+1)
+        assert np.array_equal(p.ar[:, :-1], p.al[:, 1:])
+        assert np.array_equal(p.at[:-1], p.ab[1:])
+        assert (p.at[-1] == 0).all() and (p.ab[0] == 0).all()
+        assert (p.ac < 0).all()
+    p = P.basin(0)
+    assert (p.al[:, 0] == 0).all() and (p.ar[:, -1] == 0).all()
+    g = P.global_grid(120, 60, seed=1)
+    land = ~g.meta["wet"]
+    assert 0.2 < land.mean() < 0.4
+    assert (g.b[land] == 0).all()
+    A = P.sparse_matrix(g)
+    assert abs(A - A.T).max() == 0
+
+
+def test_tile_sub_blocks_rule():
+    p = P.global_grid(180, 90, seed=2)
+    nb6 = tile_sub_blocks(p, 16, 16, 1e6)
+    nb10 = tile_sub_blocks(p, 16, 16, 1e10)
+    assert nb6.shape == (6, 12) and nb6.min() >= 1 and nb6.max() <= 16
+    assert (nb10 <= nb6).all() and nb10.sum() < nb6.sum()
+    # pairs of 16-wide tiles share a warp and a count
+    assert (nb10[:, 0::2] == nb10[:, 1::2]).all()
+    q = P.idealised(64, 32)
+    q.ac[:] = 1.0  # z = 5.83 per row -> 7 rows for 1e6 -> 3 sub-blocks of 16 rows
+    assert (tile_sub_blocks(q, 16, 16, 1e6) == 3).all()

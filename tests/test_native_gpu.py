@@ -62,7 +62,7 @@ def test_precondition_matches_oracle(torch_cuda, oracle, name, mk, tm, th):
     torch = torch_cuda
     p = mk()
     s = _solver(p, tm, th)
-    pc = oracle.TilePC(p, tm, th, s.sub_rows)
+    pc = oracle.TilePC(p, tm, th, tile_nb=s.tile_nb)
     assert pc.status == 0
     rng = np.random.default_rng(1)
     r = rng.standard_normal((p.ny, p.nx))
@@ -89,7 +89,7 @@ def test_solve_matches_oracle(torch_cuda, oracle, name, mk, tm, th, precision):
     # independent FP64 residual on the host
     res = np.linalg.norm(p.b - P.apply_operator(p, xg)) / np.linalg.norm(p.b)
     assert res <= 2e-12
-    pc = oracle.TilePC(p, tm, th, s.sub_rows)
+    pc = oracle.TilePC(p, tm, th, tile_nb=s.tile_nb)
     xo, it, rel = pc.pcg(p.b, tol=1e-12)
     assert rel <= 1e-12
     assert np.abs(xg - xo).max() <= 1e-8 * np.abs(xo).max()
