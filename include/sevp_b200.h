@@ -237,6 +237,24 @@ long long sevp_kernel_launches(const sevp_ctx *ctx);
 int sevp_profile(sevp_ctx *ctx, int enable);
 int sevp_profile_read(sevp_ctx *ctx, double *ms, long long *count);
 
+/* ------------------------------------------------- allocation-free entry */
+
+/* Interior dot product of two padded (i2+2, j2+2) FP64 fields, the sum that
+ * p_inprod computes, written to *result.  r, p and result are DEVICE
+ * pointers; stream may be NULL.  This entry point has no counterpart in the
+ * reference.  It is for callers that cannot let a library allocate GPU
+ * memory: a model whose memory pool owns the device, or one that overlaps
+ * this call with work on other streams (cudaFree would synchronise the
+ * device).  It calls no cudaMalloc or cudaFree; its scratch is a static
+ * device array of 16384 + 32 doubles (128 KB) that every GPU loading the
+ * library holds until exit.  Limit: j2 <= 16384 (larger grids get
+ * SEVP_BAD_ARG and a message in sevp_last_error).  The first call on a
+ * device looks up the array's device address; make that first call before
+ * any stream capture.  Calls share the array, so calls that overlap on the
+ * GPU race; calls ordered in one stream do not. */
+int sevp_inprod_noalloc(const double *r, const double *p, int i2, int j2, double *result,
+                        void *stream);
+
 #ifdef __cplusplus
 }
 #endif

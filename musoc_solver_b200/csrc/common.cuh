@@ -16,6 +16,7 @@
   } while (0)
 
 void sevp_internal_set_error(cudaError_t e, const char *what, const char *file, int line);
+void sevp_internal_set_message(const char *msg);
 
 namespace sevp {
 

@@ -729,6 +729,7 @@ thread_local char g_err[512] = {0};
 void sevp_internal_set_error(cudaError_t e, const char *what, const char *file, int line) {
   snprintf(g_err, sizeof g_err, "%s: %s (%s:%d)", cudaGetErrorString(e), what, file, line);
 }
+void sevp_internal_set_message(const char *msg) { snprintf(g_err, sizeof g_err, "%s", msg); }
 extern "C" const char *sevp_last_error(void) { return g_err; }
 
 extern "C" const char *sevp_status_string(int s) {

@@ -81,6 +81,7 @@ _SIGS = {
     "sevp_relative_residual": ([P, P, P, DP], C.c_int),
     "sevp_kernel_launches": ([P], C.c_longlong),
     "sevp_tile_layout": ([P, IP, IP, IP], C.c_int),
+    "sevp_inprod_noalloc": ([P, P, C.c_int, C.c_int, P, P], C.c_int),
     "sevp_profile": ([P, C.c_int], C.c_int),
     "sevp_set_warmstart": ([P, P, P, C.c_int], C.c_int),
     "sevp_solve_step": ([P, P, P, P, P, C.c_int, C.POINTER(SolveOpts), C.POINTER(Report)], C.c_int),
