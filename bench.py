@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--nx", type=int, default=NX)
     ap.add_argument("--ny", type=int, default=NY)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precond-fp32", type=int, default=0,
+                    help="FP32 influence matrices in the inner FP32 solve of the mixed arms")
     ap.add_argument("--weights", default=os.path.join(ROOT, "musoc_solver_b200", "weights",
                                                       "unet_eddy.npz"))
     return ap.parse_args()
@@ -232,7 +234,8 @@ def run_native(args, world, rank, local, dist):
     nsteps = W + K + 2
     p, rhs = make_sequence(args.nx, args.ny, nsteps)
     n = p.nx * p.ny
-    solver = SevpSolver(p, tile_m=TILE_M, tile_h=TILE_H, growth_limit=GROWTH)
+    solver = SevpSolver(p, tile_m=TILE_M, tile_h=TILE_H, growth_limit=GROWTH,
+                        precond_fp32=args.precond_fp32)
     stream = solver.stream
     b_dev = [torch.from_numpy(b).to(dev) for b in rhs]
     torch.cuda.synchronize()
@@ -349,7 +352,10 @@ def run_native(args, world, rank, local, dist):
     peak, peak_kind = measured_peak_hbm()
     tile_ms, tile_n = prof["tile"]
     infl = solver.influence_bytes()
-    bytes_per_launch = n * (4 * 4 + 3 * 4 + 5 * 4) + infl  # x,p,r,q in; x,r,z out; coeffs
+    ncoef = 3 if solver.symmetric else 5
+    infl_bytes = infl // 2 if args.precond_fp32 else infl
+    # x,p,r,q in; x,r,z out; coefficient planes; influence data
+    bytes_per_launch = n * (4 * 4 + 3 * 4 + 4 * ncoef) + infl_bytes
     avg_s = tile_ms / 1e3 / max(tile_n, 1)
     achieved = bytes_per_launch / avg_s / 1e9 if tile_n else None
     traffic = ncu_traffic()
@@ -383,6 +389,8 @@ def run_native(args, world, rank, local, dist):
                         "right-hand-side sequence; mixed FP32 tile-SEVP PCG + FP64 iterative "
                         f"refinement to 1e-12 from warm start: {guess_name}",
             "grid": [p.nx, p.ny], "tiles": [TILE_M, TILE_H], "marching_growth_limit": GROWTH,
+            "coefficient_planes": 3 if solver.symmetric else 5,
+            "influence_fp32_in_inner_solve": bool(args.precond_fp32),
             "tol": 1e-12, "parallelism": f"replicas x{world}",
             "l2": "inputs larger than L2 (69 MB per FP64 field), no flush",
         },
@@ -404,6 +412,11 @@ def run_native(args, world, rank, local, dist):
                      "algorithmic_bytes_per_launch": bytes_per_launch,
                      "avg_launch_ms": avg_s * 1e3, "launches": tile_n,
                      "peak_source": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)"},
+        "kernels": {"tile_pass_b": {"launches": tile_n, "avg_ms": avg_s * 1e3},
+                    "stencil": {"launches": prof["stencil"][1],
+                                "avg_ms": prof["stencil"][0] / max(prof["stencil"][1], 1)},
+                    "precondition_start": {"launches": prof["precond"][1],
+                                           "avg_ms": prof["precond"][0] / max(prof["precond"][1], 1)}},
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
         "gpu_launches": int(launches_value),

@@ -172,6 +172,7 @@ typedef struct {
   double inner_tol;  /* precision 1: relative reduction asked of each FP32 solve */
   int use_guess;     /* 1: x holds the initial guess on entry; 0: start from zero */
   int check_every;   /* PCG iterations between convergence reads by the host */
+  int precond_fp32;  /* precision 1: FP32 copy of the influence matrices in the inner solve */
 } sevp_solve_opts;
 
 typedef struct {
@@ -193,6 +194,11 @@ int sevp_destroy(sevp_ctx *ctx);
  * computes the tile influence data on the GPU. */
 int sevp_set_operator(sevp_ctx *ctx, const float *al, const float *ab, const float *ac,
                       const float *ar, const float *at, const sevp_tiling *tiling);
+/* 1 when the bound operator is exactly symmetric (AR(i,j) = AL(i+1,j),
+ * AT(i,j) = AB(i,j+1)); the kernels then read only AC, AR and AT. */
+int sevp_operator_symmetric(const sevp_ctx *ctx);
+/* force != 0: always read all five planes (call before sevp_set_operator). */
+int sevp_set_full_coefficients(sevp_ctx *ctx, int force);
 /* Device bytes held by the tile influence data. */
 long long sevp_influence_bytes(const sevp_ctx *ctx);
 /* Solves A x = b (device pointers, (nx, ny) column-major FP64). */

@@ -96,17 +96,23 @@ __device__ __forceinline__ void reduce_and_finish(double (&v)[NV], double *parti
 // lanes, which evaluate the neighbour column directly (periodic wrap in x).
 constexpr int kStencilThreads = 256;
 
-template <class Op>
+// SYM: the operator is symmetric (AL(i,j) = AR(i-1,j), AB(i,j) = AT(i,j-1)),
+// so only AC, AR and AT are read; AL comes from the west lane's AR and AB
+// from the previous row's AT.
+template <class Op, bool SYM>
 __global__ void __launch_bounds__(kStencilThreads)
     k_stencil(GridDims g, Coeffs c, Op op, int rpw, double *partials, unsigned *ticket,
               SolveState *st) {
   using T = typename Op::T;
+  constexpr int U = 4;  // rows per unrolled step: all their loads are issued together
   if (Op::kUsesState && st->done) return;
   op.prepare(st);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int nx = g.nx, ny = g.ny;
-  const int i = blockIdx.x * 32 + lane;
-  const int j0 = (blockIdx.y * (kStencilThreads / 32) + w) * rpw;
+  // the CTA's warps sit side by side: each row is read as one contiguous
+  // span of 256 columns, which keeps DRAM pages open across the warps
+  const int i = (blockIdx.x * (kStencilThreads / 32) + w) * 32 + lane;
+  const int j0 = blockIdx.y * rpw;
   const int j1 = min(j0 + rpw, ny);
   const bool col_ok = i < nx;
   double acc[Op::NV];
@@ -121,27 +127,76 @@ __global__ void __launch_bounds__(kStencilThreads)
     const bool own_e = (lane == 31) || (i + 1 >= nx);
     T vb = (j0 > 0 && col_ok) ? op.value((size_t)(j0 - 1) * nx + i) : T(0);
     T vc = col_ok ? op.value((size_t)j0 * nx + i) : T(0);
-    for (int j = j0; j < j1; ++j) {
-      const size_t row = (size_t)j * nx;
-      T va = (j + 1 < ny && col_ok) ? op.value(row + nx + i) : T(0);
-      T vw = __shfl_up_sync(0xffffffffu, vc, 1);
-      T ve = __shfl_down_sync(0xffffffffu, vc, 1);
-      if (own_w) vw = (iw >= 0 && col_ok) ? op.value(row + iw) : T(0);
-      if (own_e) ve = (ie >= 0 && col_ok) ? op.value(row + ie) : T(0);
-      if (col_ok) {
+    float at_prev = (SYM && j0 > 0 && col_ok) ? __ldg(c.at + (size_t)(j0 - 1) * nx + i) : 0.f;
+    for (int jb = j0; jb < j1; jb += U) {
+      // loads: the next U rows of the field, U rows of coefficients, edge columns
+      T va[U], vwe[U], vee[U];
+      float cb[U], cw[U], ccn[U], ce[U], cn[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int j = jb + u;
+        const size_t row = (size_t)j * nx;
+        const bool rok = (j < j1) && col_ok;
+        va[u] = (rok && j + 1 < ny) ? op.value(row + nx + i) : T(0);
+        vwe[u] = (rok && own_w && iw >= 0) ? op.value(row + iw) : T(0);
+        vee[u] = (rok && own_e && ie >= 0) ? op.value(row + ie) : T(0);
         const size_t idx = row + i;
-        T av = T(__ldg(c.ab + idx)) * vb;
-        av += T(__ldg(c.al + idx)) * vw;
-        av += T(__ldg(c.ac + idx)) * vc;
-        av += T(__ldg(c.ar + idx)) * ve;
-        av += T(__ldg(c.at + idx)) * va;
-        op.emit(idx, vc, av, acc);
+        ccn[u] = rok ? __ldg(c.ac + idx) : 0.f;
+        ce[u] = rok ? __ldg(c.ar + idx) : 0.f;
+        cn[u] = rok ? __ldg(c.at + idx) : 0.f;
+        if (SYM) {
+          cw[u] = (rok && own_w && iw >= 0) ? __ldg(c.ar + row + iw) : 0.f;  // edge lanes only
+          cb[u] = 0.f;
+        } else {
+          cb[u] = rok ? __ldg(c.ab + idx) : 0.f;
+          cw[u] = rok ? __ldg(c.al + idx) : 0.f;
+        }
       }
-      vb = vc;
-      vc = va;
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int j = jb + u;
+        if (j >= j1) break;
+        T vw = __shfl_up_sync(0xffffffffu, vc, 1);
+        T ve = __shfl_down_sync(0xffffffffu, vc, 1);
+        if (own_w) vw = vwe[u];
+        if (own_e) ve = vee[u];
+        float cwu = cw[u], cbu = cb[u];
+        if (SYM) {
+          const float arw = __shfl_up_sync(0xffffffffu, ce[u], 1);
+          if (!own_w) cwu = arw;
+          cbu = (u == 0) ? at_prev : cn[u - 1];
+        }
+        if (col_ok) {
+          T av = T(cbu) * vb;
+          av += T(cwu) * vw;
+          av += T(ccn[u]) * vc;
+          av += T(ce[u]) * ve;
+          av += T(cn[u]) * va[u];
+          op.emit((size_t)j * nx + i, vc, av, acc);
+        }
+        vb = vc;
+        vc = va[u];
+      }
+      if (SYM) at_prev = cn[U - 1];
     }
   }
-  if (Op::NV > 0) reduce_and_finish<Op::NV>(acc, partials, ticket, op);
+  reduce_and_finish<Op::NV>(acc, partials, ticket, op);
+}
+
+// Exact symmetry test of the five planes: AR(i,j) == AL(i+1,j) (with the
+// periodic wrap) and AT(i,j) == AB(i,j+1).  Coefficients that multiply
+// values outside the domain are not compared.
+__global__ void k_check_symmetry(Coeffs c, int nx, int ny, int periodic, int *asym) {
+  const size_t n = (size_t)nx * ny;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n;
+       e += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(e % nx), j = (int)(e / nx);
+    bool bad = false;
+    if (i < nx - 1) bad |= c.ar[e] != c.al[e + 1];
+    else if (periodic) bad |= c.ar[e] != c.al[e + 1 - nx];
+    if (j < ny - 1) bad |= c.at[e] != c.ab[e + nx];
+    if (bad) atomicOr(asym, 1);
+  }
 }
 
 // y = A x
@@ -244,7 +299,7 @@ struct OpResidual {
 };
 
 // --------------------------------------------------- tile apply kernel
-constexpr int kTileWarps = 4;
+constexpr int kTileWarps = 8;
 
 // Shared memory per warp: the tile's rows of z (FP64 marching state, 32
 // lanes per row), the last-equation residual of each sub-block (stored at
@@ -253,21 +308,35 @@ __host__ __device__ inline size_t tile_smem_per_warp(int hmax) {
   return (size_t)hmax * 32 * 8 * 2 + 32 * 8;
 }
 
-// out(n) = sum_k dv[seg + k] * M[k * mw + n]
-__device__ __forceinline__ double seg_matvec(const double *dv, int segbase, const double *M, int mw,
-                                             int n) {
-  double s = 0.0;
-  int k = 0;
-  for (; k + 4 <= mw; k += 4) {
-    double m0 = __ldg(M + (size_t)k * mw + n), m1 = __ldg(M + (size_t)(k + 1) * mw + n);
-    double m2 = __ldg(M + (size_t)(k + 2) * mw + n), m3 = __ldg(M + (size_t)(k + 3) * mw + n);
-    s += dv[segbase + k] * m0;
-    s += dv[segbase + k + 1] * m1;
-    s += dv[segbase + k + 2] * m2;
-    s += dv[segbase + k + 3] * m3;
+// out(n) = sum_k dv[seg + k] * M[k * mw + n].  All loads of the column are
+// issued before the first multiply-add, so a mat-vec costs one memory round
+// trip instead of one per group of rows.  MT is the stored matrix type.
+template <int WMAX, typename MT>
+__device__ __forceinline__ double seg_matvec_w(const double *dv, int segbase, const MT *M, int mw,
+                                               int n) {
+  MT m[WMAX];
+#pragma unroll
+  for (int k = 0; k < WMAX; ++k) m[k] = (k < mw) ? __ldg(M + (size_t)k * mw + n) : MT(0);
+  if (sizeof(MT) == 4) {
+    // FP32 influence data: multiply-add in FP32 (the mixed-precision mode)
+    float s = 0.f;
+#pragma unroll
+    for (int k = 0; k < WMAX; ++k)
+      if (k < mw) s += (float)dv[segbase + k] * (float)m[k];
+    return (double)s;
   }
-  for (; k < mw; ++k) s += dv[segbase + k] * __ldg(M + (size_t)k * mw + n);
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < WMAX; ++k)
+    if (k < mw) s += dv[segbase + k] * (double)m[k];
   return s;
+}
+template <typename MT>
+__device__ __forceinline__ double seg_matvec(const double *dv, int segbase, const MT *M, int mw,
+                                             int n) {
+  if (mw <= 8) return seg_matvec_w<8, MT>(dv, segbase, M, mw, n);
+  if (mw <= 16) return seg_matvec_w<16, MT>(dv, segbase, M, mw, n);
+  return seg_matvec_w<32, MT>(dv, segbase, M, mw, n);
 }
 
 // Inputs of one tile row for one lane (prefetched one row ahead).
@@ -277,7 +346,7 @@ struct RowIn {
   float cw, cs, cc, ce, cn;
 };
 
-template <typename V, bool UPDATE>
+template <typename V, bool UPDATE, bool SYM>
 __device__ __forceinline__ void load_row(RowIn<V> &in, const Coeffs &c, const V *x, const V *p,
                                          const V *r, const V *q, size_t idx) {
   if (UPDATE) {
@@ -286,8 +355,10 @@ __device__ __forceinline__ void load_row(RowIn<V> &in, const Coeffs &c, const V 
     in.q = q[idx];
   }
   in.r = r[idx];
-  in.cw = __ldg(c.al + idx);
-  in.cs = __ldg(c.ab + idx);
+  if (!SYM) {
+    in.cw = __ldg(c.al + idx);
+    in.cs = __ldg(c.ab + idx);
+  }
   in.cc = __ldg(c.ac + idx);
   in.ce = __ldg(c.ar + idx);
   in.cn = __ldg(c.at + idx);
@@ -295,9 +366,14 @@ __device__ __forceinline__ void load_row(RowIn<V> &in, const Coeffs &c, const V 
 
 // UPDATE: fused x += alpha p, r -= alpha q before preconditioning (pass B).
 // DOTS:   accumulate r.z and r.r and finish the iteration on the device.
-template <typename V, bool UPDATE, bool DOTS>
+// SYM:    symmetric operator: AL and AB are taken from the west lane's AR and
+//         the previous row's AT (inside a tile the couplings that cross the
+//         tile edge are dropped, so the edge values are never needed).
+// MT:     stored type of the influence matrices (double, or float for the
+//         FP32 inner solve).
+template <typename V, typename MT, bool UPDATE, bool DOTS, bool SYM>
 __global__ void __launch_bounds__(kTileWarps * 32)
-    k_tile_apply(TileGeom tg, Coeffs c, const double *__restrict__ mats, V *x, const V *p, V *r,
+    k_tile_apply(TileGeom tg, Coeffs c, const MT *__restrict__ mats, V *x, const V *p, V *r,
                  const V *q, V *z, SolveState *st, double *partials, unsigned *ticket) {
   if (DOTS && st->done) return;
   extern __shared__ __align__(16) unsigned char tsm[];
@@ -319,7 +395,7 @@ __global__ void __launch_bounds__(kTileWarps * 32)
     const int nx = tg.nx;
     const int j0 = b * tg.th, hh = tile_height(tg, b), nb = tg.grp_nb[(size_t)b * tg.txg + grp];
     const int i = a * tg.tm + n;
-    const double *mt = mats + (mw > 0 ? tg.moff[(size_t)b * tg.tx + a] : 0);
+    const MT *mt = mats + (mw > 0 ? tg.moff[(size_t)b * tg.tx + a] : 0);
     const size_t msz = (size_t)mw * mw;
     double alpha = 0.0;
     if (UPDATE) alpha = st->alpha;
@@ -328,15 +404,26 @@ __global__ void __launch_bounds__(kTileWarps * 32)
     //      block-top corrections (the elimination of the SEVP system).
     //      zs keeps each sub-block's top row before its correction.
     double zb = 0.0, zc = 0.0;
+    float cn_prev = 0.f;  // AT of the previous row (AB of this row when SYM)
     int t = 0, kb = 0, ke = sub_start(1, hh, nb) - 1;
     RowIn<V> cur{}, nxt{};
     const size_t idx0 = (size_t)j0 * nx + i;
-    if (active) load_row<V, UPDATE>(cur, c, x, p, r, q, idx0);
+    if (active) load_row<V, UPDATE, SYM>(cur, c, x, p, r, q, idx0);
     for (int k = 0; k < hh; ++k) {
       const size_t idx = idx0 + (size_t)k * nx;
-      if (active && k + 1 < hh) load_row<V, UPDATE>(nxt, c, x, p, r, q, idx + nx);
+      if (active && k + 1 < hh) load_row<V, UPDATE, SYM>(nxt, c, x, p, r, q, idx + nx);
       double rv = 0.0;
-      const double cw = cur.cw, cs = cur.cs, cc = cur.cc, ce = cur.ce;
+      double cw, cs;
+      if (SYM) {
+        const float arw = __shfl_up_sync(0xffffffffu, cur.ce, 1);
+        cw = (n == 0) ? 0.0 : (double)arw;
+        cs = (double)cn_prev;
+        cn_prev = cur.cn;
+      } else {
+        cw = cur.cw;
+        cs = cur.cs;
+      }
+      const double cc = cur.cc, ce = cur.ce;
       const double cn = active ? (double)cur.cn : 1.0;
       if (active) {
         if (UPDATE) {
@@ -366,7 +453,7 @@ __global__ void __launch_bounds__(kTileWarps * 32)
         if (t < nb - 1) {
           dv[lane] = rho;
           __syncwarp();
-          double sc = active ? seg_matvec(dv, segbase, mt + (size_t)(nb + t) * msz, mw, n) : 0.0;
+          double sc = active ? seg_matvec<MT>(dv, segbase, mt + (size_t)(nb + t) * msz, mw, n) : 0.0;
           __syncwarp();
           zc = zc - sc;
         }
@@ -385,29 +472,41 @@ __global__ void __launch_bounds__(kTileWarps * 32)
       const double cnk = active ? (double)__ldg(c.at + idx0 + (size_t)ke * nx) : 0.0;
       dv[lane] = rho_s[ke * 32 + lane] - cnk * vnext;
       __syncwarp();
-      double v = active ? seg_matvec(dv, segbase, mt + (size_t)t * msz, mw, n) : 0.0;
+      double v = active ? seg_matvec<MT>(dv, segbase, mt + (size_t)t * msz, mw, n) : 0.0;
       __syncwarp();
       zs[kb * 32 + lane] += v;
       double hb = 0.0, hc = v;
+      float cnb = 0.f;  // AT of row kb-1
       if (t > 0) {
-        double cnb = active ? (double)__ldg(c.at + idx0 + (size_t)(kb - 1) * nx) : 0.0;
-        dv[lane] = v * cnb;
+        cnb = active ? __ldg(c.at + idx0 + (size_t)(kb - 1) * nx) : 0.f;
+        dv[lane] = v * (double)cnb;
         __syncwarp();
-        hb = active ? seg_matvec(dv, segbase, mt + (size_t)(nb + t - 1) * msz, mw, n) : 0.0;
+        hb = active ? seg_matvec<MT>(dv, segbase, mt + (size_t)(nb + t - 1) * msz, mw, n) : 0.0;
         __syncwarp();
       }
       float ncw = 0.f, ncs = 0.f, ncc = 0.f, nce = 0.f, ncn = 1.f;
       if (active && kb < ke) {
         const size_t id = idx0 + (size_t)kb * nx;
-        ncw = __ldg(c.al + id), ncs = __ldg(c.ab + id), ncc = __ldg(c.ac + id);
-        nce = __ldg(c.ar + id), ncn = __ldg(c.at + id);
+        if (!SYM) ncw = __ldg(c.al + id), ncs = __ldg(c.ab + id);
+        ncc = __ldg(c.ac + id), nce = __ldg(c.ar + id), ncn = __ldg(c.at + id);
       }
+      float cn_prev_b = cnb;
       for (int k = kb; k < ke; ++k) {
-        const double cw = ncw, cs = ncs, cc = ncc, ce = nce, cn = ncn;
+        double cw, cs;
+        const double cc = ncc, ce = nce, cn = ncn;
+        if (SYM) {
+          const float arw = __shfl_up_sync(0xffffffffu, nce, 1);
+          cw = (n == 0) ? 0.0 : (double)arw;
+          cs = (double)cn_prev_b;
+          cn_prev_b = ncn;
+        } else {
+          cw = ncw;
+          cs = ncs;
+        }
         if (active && k + 1 < ke) {
           const size_t id = idx0 + (size_t)(k + 1) * nx;
-          ncw = __ldg(c.al + id), ncs = __ldg(c.ab + id), ncc = __ldg(c.ac + id);
-          nce = __ldg(c.ar + id), ncn = __ldg(c.at + id);
+          if (!SYM) ncw = __ldg(c.al + id), ncs = __ldg(c.ab + id);
+          ncc = __ldg(c.ac + id), nce = __ldg(c.ar + id), ncn = __ldg(c.at + id);
         }
         double hw = __shfl_up_sync(0xffffffffu, hc, 1);
         double he = __shfl_down_sync(0xffffffffu, hc, 1);
@@ -418,13 +517,15 @@ __global__ void __launch_bounds__(kTileWarps * 32)
         hb = hc;
         hc = hn;
       }
-      if (active)
+      if (active) {
+#pragma unroll 4
         for (int k = kb; k <= ke; ++k) {
           const size_t idx = idx0 + (size_t)k * nx;
           V zv = (V)zs[k * 32 + lane];
           z[idx] = zv;
           if (DOTS) acc_rz += (double)r[idx] * (double)zv;
         }
+      }
       vnext = v;
     }
   }
@@ -464,6 +565,12 @@ __global__ void __launch_bounds__(kTileWarps * 32)
     } fin{st};
     reduce_and_finish<2>(v2, partials, ticket, fin);
   }
+}
+
+__global__ void k_to_float(const double *a, float *b, size_t n) {
+  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += (size_t)gridDim.x * blockDim.x)
+    b[k] = (float)a[k];
 }
 
 // Per-tile marching growth: the smallest sub-block height s_max such that
@@ -662,6 +769,10 @@ struct sevp_ctx {
   // tiles
   TileGeom tg{};
   int *d_grp_nb = nullptr;
+  int sym = 0;                  // operator exactly symmetric: 3-plane kernels
+  int force_full = 0;           // use the 5-plane kernels regardless
+  float *d_mats32 = nullptr;    // FP32 copy of the influence data (built on demand)
+  bool infl32_active = false;   // current solve uses d_mats32 for FP32 vectors
   long long *d_moff = nullptr;
   double *d_mats = nullptr;
   long long mats_elems = 0;
@@ -746,10 +857,10 @@ extern "C" const char *sevp_status_string(int s) {
   }
 }
 
-static int stencil_rpw(int ny) { return ny >= 2048 ? 32 : 16; }
+static int stencil_rpw(int ny) { return ny >= 1024 ? 16 : 8; }
 
 static dim3 stencil_grid(const sevp_ctx *ctx, int rpw) {
-  return dim3((unsigned)ceil_div(ctx->nx, 32), (unsigned)ceil_div(ctx->ny, rpw * (kStencilThreads / 32)));
+  return dim3((unsigned)ceil_div(ctx->nx, kStencilThreads), (unsigned)ceil_div(ctx->ny, rpw));
 }
 
 static size_t tile_warps(const TileGeom &tg) { return (size_t)tg.ty * tg.txg; }
@@ -760,32 +871,51 @@ static int launch_stencil(sevp_ctx *ctx, const Op &op, int ticket_slot) {
   dim3 grid = stencil_grid(ctx, rpw);
   GridDims gd{ctx->nx, ctx->ny, ctx->periodic};
   ProfScope ps(ctx, 1);
-  k_stencil<Op><<<grid, kStencilThreads, 0, ctx->stream>>>(gd, ctx->c, op, rpw, ctx->partials,
-                                                          ctx->tickets + ticket_slot, ctx->st);
+  if (ctx->sym)
+    k_stencil<Op, true><<<grid, kStencilThreads, 0, ctx->stream>>>(
+        gd, ctx->c, op, rpw, ctx->partials, ctx->tickets + ticket_slot, ctx->st);
+  else
+    k_stencil<Op, false><<<grid, kStencilThreads, 0, ctx->stream>>>(
+        gd, ctx->c, op, rpw, ctx->partials, ctx->tickets + ticket_slot, ctx->st);
   ctx->launches++;
   SEVP_CUDA_TRY(cudaGetLastError());
   return SEVP_OK;
 }
 
-template <typename V, bool UPDATE, bool DOTS>
-static int launch_tile(sevp_ctx *ctx, V *x, const V *p, V *r, const V *q, V *z, int ticket_slot) {
-  size_t warps = tile_warps(ctx->tg);
-  unsigned blocks = (unsigned)((warps + kTileWarps - 1) / kTileWarps);
-  size_t smem = tile_smem_per_warp(ctx->tg.hmax) * kTileWarps;
-  auto kern = k_tile_apply<V, UPDATE, DOTS>;
-  static thread_local size_t set_smem[8] = {0};
-  const int key = (sizeof(V) == 8 ? 4 : 0) + (UPDATE ? 2 : 0) + (DOTS ? 1 : 0);
-  if (smem > 48 * 1024 && set_smem[key] < smem) {
+template <typename V, typename MT, bool UPDATE, bool DOTS, bool SYM>
+static int launch_tile_k(sevp_ctx *ctx, const MT *mats, V *x, const V *p, V *r, const V *q, V *z,
+                         int ticket_slot) {
+  const size_t warps = tile_warps(ctx->tg);
+  const unsigned blocks = (unsigned)((warps + kTileWarps - 1) / kTileWarps);
+  const size_t smem = tile_smem_per_warp(ctx->tg.hmax) * kTileWarps;
+  auto kern = k_tile_apply<V, MT, UPDATE, DOTS, SYM>;
+  static size_t set_smem = 0;  // per instantiation (one device per process is assumed)
+  if (smem > 48 * 1024 && set_smem < smem) {
     SEVP_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    set_smem[key] = smem;
+    set_smem = smem;
   }
   ProfScope ps(ctx, UPDATE ? 0 : 2);
-  kern<<<blocks, kTileWarps * 32, smem, ctx->stream>>>(ctx->tg, ctx->c, ctx->d_mats, x, p, r, q, z,
-                                                      ctx->st, ctx->partials,
-                                                      ctx->tickets + ticket_slot);
+  kern<<<blocks, kTileWarps * 32, smem, ctx->stream>>>(ctx->tg, ctx->c, mats, x, p, r, q, z, ctx->st,
+                                                      ctx->partials, ctx->tickets + ticket_slot);
   ctx->launches++;
   SEVP_CUDA_TRY(cudaGetLastError());
   return SEVP_OK;
+}
+
+// Dispatch: symmetric-coefficient variant when the operator is symmetric;
+// FP32 influence matrices only for FP32 vectors when the solve asks for them.
+template <typename V, bool UPDATE, bool DOTS>
+static int launch_tile(sevp_ctx *ctx, V *x, const V *p, V *r, const V *q, V *z, int ticket_slot) {
+  if constexpr (sizeof(V) == 4) {
+    if (ctx->infl32_active && ctx->d_mats32) {
+      if (ctx->sym)
+        return launch_tile_k<V, float, UPDATE, DOTS, true>(ctx, ctx->d_mats32, x, p, r, q, z, ticket_slot);
+      return launch_tile_k<V, float, UPDATE, DOTS, false>(ctx, ctx->d_mats32, x, p, r, q, z, ticket_slot);
+    }
+  }
+  if (ctx->sym)
+    return launch_tile_k<V, double, UPDATE, DOTS, true>(ctx, ctx->d_mats, x, p, r, q, z, ticket_slot);
+  return launch_tile_k<V, double, UPDATE, DOTS, false>(ctx, ctx->d_mats, x, p, r, q, z, ticket_slot);
 }
 
 // Folds recorded event pairs into per-class totals (synchronises the stream).
@@ -822,7 +952,8 @@ static void free_work(sevp_ctx *ctx) {
   void *ptrs[] = {ctx->r64, ctx->z64, ctx->p64[0], ctx->p64[1], ctx->q64, ctx->x64s, ctx->r32,
                   ctx->z32, ctx->p32[0], ctx->p32[1], ctx->q32, ctx->d32, ctx->bh, ctx->xh,
                   ctx->e1h, ctx->e2h,
-                  ctx->d_grp_nb, ctx->d_moff, ctx->d_mats, ctx->st, ctx->partials, ctx->tickets};
+                  ctx->d_grp_nb, ctx->d_moff, ctx->d_mats, ctx->st, ctx->partials, ctx->tickets,
+                  ctx->d_mats32};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (ctx->h_st) cudaFreeHost(ctx->h_st);
@@ -866,7 +997,8 @@ extern "C" int sevp_create(sevp_ctx **out, int nx, int ny, int periodic, void *s
   ALLOC(ctx->st, sizeof(SolveState));
   ALLOC(ctx->tickets, 16 * sizeof(unsigned));
   // partial sums: enough for the larger of the stencil and tile grids
-  size_t sgrid = (size_t)ceil_div(nx, 32) * ceil_div(ny, 16 * 8);
+  // stencil grid: ceil(nx / 256) x ceil(ny / rpw), rpw >= 8
+  size_t sgrid = (size_t)ceil_div(nx, kStencilThreads) * ceil_div(ny, 8);
   size_t tgrid = (size_t)ceil_div(nx, 1) * ceil_div(ny, 1) / (kTileWarps) + 1024;
   ctx->partials_n = std::max(sgrid, tgrid) * 2 + 64;
   ALLOC(ctx->partials, ctx->partials_n * 8);
@@ -893,6 +1025,15 @@ extern "C" int sevp_destroy(sevp_ctx *ctx) {
 
 extern "C" long long sevp_kernel_launches(const sevp_ctx *ctx) { return ctx ? ctx->launches : 0; }
 
+extern "C" int sevp_operator_symmetric(const sevp_ctx *ctx) { return ctx ? ctx->sym : 0; }
+
+extern "C" int sevp_set_full_coefficients(sevp_ctx *ctx, int force) {
+  if (!ctx) return SEVP_BAD_ARG;
+  ctx->force_full = force ? 1 : 0;
+  if (force) ctx->sym = 0;
+  return SEVP_OK;
+}
+
 extern "C" int sevp_tile_layout(const sevp_ctx *ctx, int *tiles_x, int *tiles_y, int *nb_per_tile) {
   if (!ctx || !ctx->have_op || !tiles_x || !tiles_y) return SEVP_BAD_ARG;
   *tiles_x = ctx->tg.tx;
@@ -912,6 +1053,27 @@ extern "C" int sevp_set_operator(sevp_ctx *ctx, const float *al, const float *ab
   if (tm < 1 || tm > 32 || th < 1 || th > 32 || tl->sub_rows < 1) return SEVP_BAD_ARG;
   // the tile geometry needs ceil(nx/tm) etc. before the growth kernel runs
   ctx->c = Coeffs{al, ab, ac, ar, at};
+  {
+    int *d_asym = nullptr;
+    SEVP_CUDA_TRY(cudaMalloc((void **)&d_asym, sizeof(int)));
+    SEVP_CUDA_TRY(cudaMemsetAsync(d_asym, 0, sizeof(int), ctx->stream));
+    const size_t n = (size_t)ctx->nx * ctx->ny;
+    k_check_symmetry<<<(unsigned)std::min<size_t>((n + 255) / 256, 148 * 32), 256, 0, ctx->stream>>>(
+        ctx->c, ctx->nx, ctx->ny, ctx->periodic, d_asym);
+    ctx->launches++;
+    int h_asym = 1;
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(&h_asym, d_asym, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(d_asym);
+    if (e != cudaSuccess) {
+      sevp_internal_set_error(e, "symmetry check", __FILE__, __LINE__);
+      return SEVP_CUDA_ERROR;
+    }
+    ctx->sym = (!h_asym && !ctx->force_full) ? 1 : 0;
+  }
+  if (ctx->d_mats32) cudaFree(ctx->d_mats32), ctx->d_mats32 = nullptr;
   TileGeom &tg = ctx->tg;
   tg.nx = ctx->nx, tg.ny = ctx->ny, tg.tm = tm, tg.th = th;
   tg.tx = ceil_div(ctx->nx, tm);
@@ -1123,8 +1285,28 @@ static int solve_fp64(sevp_ctx *ctx, const double *b, double *x, const sevp_solv
 }
 
 // FP32 PCG inside FP64 iterative refinement.
+static int ensure_mats32(sevp_ctx *ctx) {
+  if (ctx->d_mats32) return SEVP_OK;
+  const size_t n = (size_t)std::max<long long>(ctx->mats_elems, 1);
+  SEVP_CUDA_TRY(cudaMalloc((void **)&ctx->d_mats32, n * sizeof(float)));
+  k_to_float<<<(unsigned)std::min<size_t>((n + 255) / 256, 148 * 32), 256, 0, ctx->stream>>>(
+      ctx->d_mats, ctx->d_mats32, n);
+  ctx->launches++;
+  SEVP_CUDA_TRY(cudaGetLastError());
+  return SEVP_OK;
+}
+
 static int solve_mixed(sevp_ctx *ctx, const double *b, double *x, const sevp_solve_opts *o,
                        sevp_report *rep) {
+  if (o->precond_fp32) {
+    int s = ensure_mats32(ctx);
+    if (s) return s;
+  }
+  struct Flag {
+    sevp_ctx *c;
+    ~Flag() { c->infl32_active = false; }
+  } flag{ctx};
+  ctx->infl32_active = o->precond_fp32 != 0;
   const double inner2 = o->inner_tol * o->inner_tol;
   int total = 0, status = SEVP_MAXITER;
   double *xa = x, *xb = ctx->x64s;  // ping-pong: the residual kernel reads xa, writes xb

@@ -44,7 +44,8 @@ class Tiling(C.Structure):
 
 class SolveOpts(C.Structure):
     _fields_ = [("precision", C.c_int), ("tol", C.c_double), ("max_iter", C.c_int),
-                ("inner_tol", C.c_double), ("use_guess", C.c_int), ("check_every", C.c_int)]
+                ("inner_tol", C.c_double), ("use_guess", C.c_int), ("check_every", C.c_int),
+                ("precond_fp32", C.c_int)]
 
 
 class Report(C.Structure):
@@ -81,6 +82,8 @@ _SIGS = {
     "sevp_relative_residual": ([P, P, P, DP], C.c_int),
     "sevp_kernel_launches": ([P], C.c_longlong),
     "sevp_tile_layout": ([P, IP, IP, IP], C.c_int),
+    "sevp_operator_symmetric": ([P], C.c_int),
+    "sevp_set_full_coefficients": ([P, C.c_int], C.c_int),
     "sevp_inprod_noalloc": ([P, P, C.c_int, C.c_int, P, P], C.c_int),
     "sevp_profile": ([P, C.c_int], C.c_int),
     "sevp_set_warmstart": ([P, P, P, C.c_int], C.c_int),

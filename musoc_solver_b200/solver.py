@@ -98,8 +98,11 @@ class SevpSolver:
     """Device operator + solver context (one GPU, one CUDA stream)."""
 
     def __init__(self, problem, tile_m: int = 16, tile_h: int = 16, sub_rows=None,
-                 growth_limit: float = 1e10, device: str = "cuda", stream=None):
+                 growth_limit: float = 1e10, device: str = "cuda", stream=None,
+                 full_coefficients: bool = False, precond_fp32: bool = False):
         import torch
+
+        self.precond_fp32 = bool(precond_fp32)
 
         self.torch = torch
         self.p = problem
@@ -114,6 +117,8 @@ class SevpSolver:
         N.check(N.lib().sevp_create(C.byref(h), self.nx, self.ny, int(problem.periodic),
                                     C.c_void_p(self.stream.cuda_stream)), "sevp_create")
         self.h = h
+        if full_coefficients:
+            N.check(N.lib().sevp_set_full_coefficients(self.h, 1), "sevp_set_full_coefficients")
         self.tile_m, self.tile_h = tile_m, tile_h
         if sub_rows is not None:
             # explicit heights per tile row
@@ -166,9 +171,15 @@ class SevpSolver:
         return {"tile": (ms[0], n[0]), "stencil": (ms[1], n[1]), "precond": (ms[2], n[2])}
 
     def opts(self, precision=0, tol=1e-12, max_iter=5000, inner_tol=1e-5, use_guess=False,
-             check_every=4):
+             check_every=4, precond_fp32=None):
+        if precond_fp32 is None:
+            precond_fp32 = self.precond_fp32
         return N.SolveOpts(int(precision), float(tol), int(max_iter), float(inner_tol),
-                           int(use_guess), int(check_every))
+                           int(use_guess), int(check_every), int(precond_fp32))
+
+    @property
+    def symmetric(self) -> bool:
+        return bool(N.lib().sevp_operator_symmetric(self.h))
 
     def solve(self, b, x=None, precision=0, tol=1e-12, max_iter=5000, inner_tol=1e-5,
               check_every=4):

@@ -146,3 +146,59 @@ def test_max_iter_status(torch_cuda):
     b = torch.from_numpy(p.b).cuda()
     x, rep = s.solve(b, precision=0, max_iter=3)
     assert rep.status == 1 and rep.iterations == 3 and rep.rel_residual > 1e-12
+
+
+def test_symmetric_storage_matches_full(torch_cuda, oracle):
+    """The 3-plane kernels (exactly symmetric operators) give the same apply,
+    preconditioner and solve as the 5-plane kernels."""
+    torch = torch_cuda
+    from musoc_solver_b200.solver import SevpSolver
+
+    p = P.global_grid(180, 90, seed=12)
+    s3 = SevpSolver(p, tile_m=16, tile_h=16, growth_limit=1e6)
+    s5 = SevpSolver(p, tile_m=16, tile_h=16, growth_limit=1e6, full_coefficients=True)
+    assert s3.symmetric and not s5.symmetric
+    rng = np.random.default_rng(3)
+    x = torch.from_numpy(rng.standard_normal((p.ny, p.nx))).cuda()
+    a3, a5 = s3.apply(x).cpu().numpy(), s5.apply(x).cpu().numpy()
+    assert np.abs(a3 - a5).max() <= 1e-14 * np.abs(a5).max()
+    z3, z5 = s3.precondition(x).cpu().numpy(), s5.precondition(x).cpu().numpy()
+    assert np.abs(z3 - z5).max() <= 1e-12 * np.abs(z5).max()
+    b = torch.from_numpy(p.b).cuda()
+    for prec in (0, 1):
+        x3, r3 = s3.solve(b, precision=prec)
+        x5, r5 = s5.solve(b, precision=prec)
+        assert r3.rel_residual <= 1e-12 and r5.rel_residual <= 1e-12
+        assert np.abs((x3 - x5).cpu().numpy()).max() <= 1e-9 * float(x5.abs().max())
+
+
+def test_nonsymmetric_operator_uses_full_planes(torch_cuda, oracle):
+    torch = torch_cuda
+    from musoc_solver_b200.solver import SevpSolver
+
+    p = P.basin(5, n=64)
+    rng = np.random.default_rng(5)
+    p.al *= (1.0 + 0.01 * rng.random(p.al.shape)).astype(np.float32)  # break symmetry
+    s = SevpSolver(p, tile_m=16, tile_h=16, growth_limit=1e6)
+    assert not s.symmetric
+    x = rng.standard_normal((p.ny, p.nx))
+    y = s.apply(torch.from_numpy(x).cuda()).cpu().numpy()
+    yo = oracle.apply(p, x)
+    assert np.abs(y - yo).max() <= 1e-13 * np.abs(yo).max()
+    pc = oracle.TilePC(p, 16, 16, tile_nb=s.tile_nb)
+    z = s.precondition(torch.from_numpy(x).cuda()).cpu().numpy()
+    zo = pc.apply(x)
+    assert np.abs(z - zo).max() <= 1e-8 * np.abs(zo).max()
+
+
+def test_mixed_with_fp32_influence(torch_cuda):
+    torch = torch_cuda
+    from musoc_solver_b200.solver import SevpSolver
+
+    p = P.global_grid(240, 120, seed=13)
+    s = SevpSolver(p, tile_m=16, tile_h=16, precond_fp32=True)
+    b = torch.from_numpy(p.b).cuda()
+    x, rep = s.solve(b, precision=1, tol=1e-12)
+    assert rep.status == 0 and rep.rel_residual <= 1e-12
+    res = np.linalg.norm(p.b - P.apply_operator(p, x.cpu().numpy())) / np.linalg.norm(p.b)
+    assert res <= 2e-12
