@@ -24,6 +24,8 @@
 #include <string>
 #include <vector>
 
+#include <cuda_bf16.h>
+
 #include "common.cuh"
 #include "tile_sevp.cuh"
 
@@ -95,16 +97,33 @@ __device__ __forceinline__ void reduce_and_finish(double (&v)[NV], double *parti
 // east/west neighbours come from warp shuffles, except at the warp's edge
 // lanes, which evaluate the neighbour column directly (periodic wrap in x).
 constexpr int kStencilThreads = 256;
+// Launch shape, chosen by measurement at 3600x2400 on a B200: the minimum
+// resident CTAs cap the registers (64 for the stencil, 85 for the tile
+// kernel) so that enough warps keep memory requests in flight; FP32 fields
+// load 4 rows per step, FP64 fields 2.
+#ifndef SEVP_STENCIL_UNROLL
+#define SEVP_STENCIL_UNROLL 0
+#endif
+#ifndef SEVP_STENCIL_MINB
+#define SEVP_STENCIL_MINB 4
+#endif
+#ifndef SEVP_TILE_MINB
+#define SEVP_TILE_MINB 3
+#endif
+#ifndef SEVP_STENCIL_RPW
+#define SEVP_STENCIL_RPW 16
+#endif
 
 // SYM: the operator is symmetric (AL(i,j) = AR(i-1,j), AB(i,j) = AT(i,j-1)),
 // so only AC, AR and AT are read; AL comes from the west lane's AR and AB
 // from the previous row's AT.
 template <class Op, bool SYM>
-__global__ void __launch_bounds__(kStencilThreads)
+__global__ void __launch_bounds__(kStencilThreads, SEVP_STENCIL_MINB)
     k_stencil(GridDims g, Coeffs c, Op op, int rpw, double *partials, unsigned *ticket,
               SolveState *st) {
   using T = typename Op::T;
-  constexpr int U = 4;  // rows per unrolled step: all their loads are issued together
+  // rows per step: all their loads are issued together
+  constexpr int U = SEVP_STENCIL_UNROLL > 0 ? SEVP_STENCIL_UNROLL : (sizeof(T) == 4 ? 4 : 2);
   if (Op::kUsesState && st->done) return;
   op.prepare(st);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -372,7 +391,7 @@ __device__ __forceinline__ void load_row(RowIn<V> &in, const Coeffs &c, const V 
 // MT:     stored type of the influence matrices (double, or float for the
 //         FP32 inner solve).
 template <typename V, typename MT, bool UPDATE, bool DOTS, bool SYM>
-__global__ void __launch_bounds__(kTileWarps * 32)
+__global__ void __launch_bounds__(kTileWarps * 32, SEVP_TILE_MINB)
     k_tile_apply(TileGeom tg, Coeffs c, const MT *__restrict__ mats, V *x, const V *p, V *r,
                  const V *q, V *z, SolveState *st, double *partials, unsigned *ticket) {
   if (DOTS && st->done) return;
@@ -857,7 +876,7 @@ extern "C" const char *sevp_status_string(int s) {
   }
 }
 
-static int stencil_rpw(int ny) { return ny >= 1024 ? 16 : 8; }
+static int stencil_rpw(int ny) { return ny >= 1024 ? SEVP_STENCIL_RPW : 8; }
 
 static dim3 stencil_grid(const sevp_ctx *ctx, int rpw) {
   return dim3((unsigned)ceil_div(ctx->nx, kStencilThreads), (unsigned)ceil_div(ctx->ny, rpw));
@@ -1406,6 +1425,7 @@ __global__ void k_guess(const double *eta1, const double *eta2, double *g, size_
     double v = 0.0;
     if (mode == 1) v = eta1[k];
     if (mode == 2) v = 2.0 * eta1[k] - eta2[k];
+    if (mode == 3) v = eta1[k] - eta2[k];
     g[k] = v;
   }
 }
@@ -1467,6 +1487,112 @@ extern "C" int sevp_solve_step_host(sevp_ctx *ctx, const double *bh, const doubl
   SEVP_CUDA_TRY(cudaMemcpyAsync(xh, ctx->xh, bytes, cudaMemcpyDeviceToHost, ctx->stream));
   SEVP_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   return s;
+}
+
+// ---------------------------------------------------- learned warm start
+// Features of the network from (eta1, eta2, b): e = 2 eta1 - eta2 (the
+// linear extrapolation), r = b - A e, m = M^{-1} r (one tile-SEVP solve),
+// d = eta1 - eta2.  scales[0..2] = RMS of r, m, d; the packed input is
+// BF16 NHWC with 16 channels: r/s0, m/s1, d/s2, then zeros.
+__global__ void k_rms3(const double *a, const double *b, const double *c, size_t n,
+                       double *partials, unsigned *ticket, float *scales) {
+  double s[3] = {0.0, 0.0, 0.0};
+  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += (size_t)gridDim.x * blockDim.x) {
+    s[0] += a[k] * a[k];
+    s[1] += b[k] * b[k];
+    s[2] += c[k] * c[k];
+  }
+  struct Fin {
+    float *scales;
+    size_t n;
+    __device__ void operator()(double (&v)[3]) {
+      for (int q = 0; q < 3; ++q) {
+        double r = sqrt(v[q] / (double)n);
+        scales[q] = (float)(r > 0.0 ? r : 1.0);
+      }
+    }
+  } fin{scales, n};
+  reduce_and_finish<3>(s, partials, ticket, fin);
+}
+
+__global__ void k_pack_features(const double *r, const double *m, const double *d,
+                                const float *scales, __nv_bfloat16 *feat, size_t n) {
+  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += (size_t)gridDim.x * blockDim.x) {
+    __nv_bfloat16 v[16];
+    v[0] = __float2bfloat16((float)(r[k] / scales[0]));
+    v[1] = __float2bfloat16((float)(m[k] / scales[1]));
+    v[2] = __float2bfloat16((float)(d[k] / scales[2]));
+#pragma unroll
+    for (int q = 3; q < 16; ++q) v[q] = __float2bfloat16(0.f);
+    uint4 *dst = reinterpret_cast<uint4 *>(feat + k * 16);
+    dst[0] = *reinterpret_cast<uint4 *>(&v[0]);
+    dst[1] = *reinterpret_cast<uint4 *>(&v[8]);
+  }
+}
+
+// target of training: (eta - e - m) / scale_m ; combine: x = e + m + scale_m * y
+__global__ void k_nn_target(const double *eta, const double *e, const double *m,
+                            const float *scales, float *t, size_t n) {
+  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += (size_t)gridDim.x * blockDim.x)
+    t[k] = (float)((eta[k] - e[k] - m[k]) / scales[1]);
+}
+__global__ void k_nn_combine(const double *e, const double *m, const float *y, const float *scales,
+                             double *x, size_t n) {
+  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += (size_t)gridDim.x * blockDim.x)
+    x[k] = e[k] + m[k] + (double)scales[1] * (double)y[k];
+}
+
+static unsigned grid_for(size_t n) { return (unsigned)std::min<size_t>((n + 255) / 256, 148 * 16); }
+
+extern "C" int sevp_nn_features(sevp_ctx *ctx, const double *eta1, const double *eta2,
+                                const double *b, double *e, double *m, double *d, void *feat,
+                                float *scales) {
+  if (!ctx || !ctx->have_op || !eta1 || !eta2 || !b || !e || !m || !d || !feat || !scales)
+    return SEVP_BAD_ARG;
+  int s = form_guess(ctx, eta1, eta2, e, 2);  // e = 2 eta1 - eta2
+  if (s) return s;
+  k_guess<<<grid_for(ctx->n), 256, 0, ctx->stream>>>(eta1, eta2, d, ctx->n, 3);
+  ctx->launches++;
+  s = launch_residual<double>(ctx, e, nullptr, nullptr, b, ctx->r64, 0, 0.0);
+  if (s) return s;
+  s = launch_tile<double, false, false>(ctx, nullptr, nullptr, ctx->r64, nullptr, m, 1);
+  if (s) return s;
+  k_rms3<<<grid_for(ctx->n), 256, 0, ctx->stream>>>(ctx->r64, m, d, ctx->n, ctx->partials,
+                                                   ctx->tickets + 5, scales);
+  k_pack_features<<<grid_for(ctx->n), 256, 0, ctx->stream>>>(ctx->r64, m, d, scales,
+                                                            (__nv_bfloat16 *)feat, ctx->n);
+  ctx->launches += 2;
+  SEVP_CUDA_TRY(cudaGetLastError());
+  return SEVP_OK;
+}
+
+extern "C" int sevp_nn_target(sevp_ctx *ctx, const double *eta, const double *e, const double *m,
+                              const float *scales, float *t) {
+  if (!ctx || !eta || !e || !m || !scales || !t) return SEVP_BAD_ARG;
+  k_nn_target<<<grid_for(ctx->n), 256, 0, ctx->stream>>>(eta, e, m, scales, t, ctx->n);
+  ctx->launches++;
+  SEVP_CUDA_TRY(cudaGetLastError());
+  return SEVP_OK;
+}
+
+extern "C" int sevp_nn_combine(sevp_ctx *ctx, const double *e, const double *m, const float *y,
+                               const float *scales, double *x) {
+  if (!ctx || !e || !m || !y || !scales || !x) return SEVP_BAD_ARG;
+  k_nn_combine<<<grid_for(ctx->n), 256, 0, ctx->stream>>>(e, m, y, scales, x, ctx->n);
+  ctx->launches++;
+  SEVP_CUDA_TRY(cudaGetLastError());
+  return SEVP_OK;
+}
+
+extern "C" void *sevp_stream(const sevp_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+extern "C" int sevp_add_launches(sevp_ctx *ctx, int n) {
+  if (!ctx) return SEVP_BAD_ARG;
+  ctx->launches += n;
+  return SEVP_OK;
 }
 
 extern "C" int sevp_relative_residual(sevp_ctx *ctx, const double *b, const double *x,

@@ -1,0 +1,169 @@
+"""The BF16 U-Net kernels (forward, backward, Adam) against a PyTorch-CPU FP64
+restatement of the same network that rounds stored activations to BF16.
+
+Single layers are checked on identical BF16 inputs against FP64 (forward
+and data gradient to one BF16 rounding, weight gradient to FP32
+accumulation).  The whole network is an integration check: its forward
+output agrees to 2e-2 and its parameter gradients to about 6e-2 (the GPU
+accumulates in FP32 and stores BF16; small differences in the forward
+activations flip BF16 roundings and reach every gradient through the loss);
+a wrong index or layout gives O(1) errors.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from musoc_solver_b200 import build
+
+    build.build()
+    return torch
+
+
+def _rel(a, b):
+    a = np.asarray(a, np.float64).ravel()
+    b = np.asarray(b, np.float64).ravel()
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)
+
+
+@pytest.mark.parametrize("H,W", [(16, 24), (32, 32)])
+def test_unet_forward_backward_matches_reference(torch_cuda, H, W):
+    torch = torch_cuda
+    import unet_ref
+
+    from musoc_solver_b200.unet import UNet
+
+    net = UNet(H, W, seed=3)
+    # give the biases and the head some weight so every path matters
+    rng = np.random.default_rng(1)
+    for name, v in net.params.items():
+        v[1].copy_(torch.from_numpy(rng.normal(0, 0.05, v[1].shape).astype(np.float32)))
+    net.params["head"][0].copy_(torch.from_numpy(rng.normal(0, 0.2, 32).astype(np.float32)))
+    net.sync_weights()
+    x = np.zeros((1, H, W, 16), np.float32)
+    x[..., :3] = rng.standard_normal((1, H, W, 3))
+    net.A["x"].copy_(torch.from_numpy(x.reshape(-1, 16)).to(torch.bfloat16))
+    t = rng.standard_normal(H * W).astype(np.float32)
+    tt = torch.from_numpy(t).cuda()
+    y = net.forward().cpu().numpy()
+    net.backward(tt)
+    torch.cuda.synchronize()
+    st = net.state()
+    xr = net.A["x"].float().cpu().numpy().reshape(1, H, W, 16)
+    yr, lr, gr = unet_ref.forward_backward(st, xr, t)
+    assert _rel(y, yr) < 2e-2
+    assert abs(float(net.loss.item()) - lr) <= 2e-2 * lr
+    errs = {}
+    for name, (gw, gb) in net.gw.items():
+        errs[name] = _rel(gw.cpu().numpy(), gr[f"{name}.0"])
+        if np.linalg.norm(gr[f"{name}.1"]) > 1e-8:
+            errs[name + ".bias"] = _rel(gb.cpu().numpy(), gr[f"{name}.1"])
+    print("relative gradient errors:", {k: round(v, 4) for k, v in errs.items()})
+    assert max(errs.values()) < 1.2e-1, errs
+    assert np.median(list(errs.values())) < 8e-2, errs
+
+
+def test_unet_adam_reduces_loss(torch_cuda):
+    torch = torch_cuda
+    from musoc_solver_b200.unet import UNet
+
+    H, W = 32, 48
+    net = UNet(H, W, seed=4)
+    rng = np.random.default_rng(2)
+    x = np.zeros((H * W, 16), np.float32)
+    x[:, :3] = rng.standard_normal((H * W, 3))
+    net.A["x"].copy_(torch.from_numpy(x).to(torch.bfloat16))
+    # a smooth target that depends on the inputs: a learnable map
+    t = torch.from_numpy((0.5 * x[:, 0] - 0.3 * x[:, 1]).astype(np.float32)).cuda()
+    losses = []
+    for k in range(60):
+        net.forward()
+        net.backward(t)
+        net.adam_step(lr=2e-3)
+        losses.append(float(net.loss.item()))
+    assert losses[-1] < 0.3 * losses[0]
+
+
+def _bf(torch, a):
+    return torch.from_numpy(np.asarray(a, np.float32)).to(torch.bfloat16)
+
+
+@pytest.mark.parametrize("cin,cout,H,W", [(16, 32, 8, 16), (64, 128, 16, 8), (256, 128, 8, 8)])
+def test_conv_layer_forward_dgrad_wgrad(torch_cuda, cin, cout, H, W):
+    """One 3x3 layer: forward (+bias, ReLU), masked data gradient and weight
+    gradient against torch FP64 on the same BF16 values."""
+    torch = torch_cuda
+    import ctypes as C
+
+    import torch.nn.functional as F
+
+    from musoc_solver_b200.unet import lib
+
+    L = lib()
+    rng = np.random.default_rng(cin + cout)
+    x = _bf(torch, rng.standard_normal((H * W, cin)))
+    w = _bf(torch, rng.normal(0, (2.0 / (9 * cin)) ** 0.5, (9, cin, cout)))
+    b = torch.from_numpy(rng.normal(0, 0.1, cout).astype(np.float32))
+    dy = _bf(torch, rng.standard_normal((H * W, cout)))
+    xd, wd, bd, dyd = x.cuda(), w.cuda(), b.cuda(), dy.cuda()
+    y = torch.zeros((H * W, cout), dtype=torch.bfloat16, device="cuda")
+    p = lambda t: C.c_void_p(t.data_ptr())
+    assert L.sevp_nn_conv3x3(p(xd), cin, 0, cin, p(wd), p(bd), p(y), cout, 0, cout, 1, H, W, 1, None,
+                             0, 0, 0, None) == 0
+    # reference in FP64 from the same BF16 values
+    xr = x.double().reshape(1, H, W, cin).permute(0, 3, 1, 2)
+    wr = w.double().reshape(3, 3, cin, cout).permute(3, 2, 0, 1)
+    yr = F.relu(F.conv2d(xr, wr, bias=b.double(), padding=1)).permute(0, 2, 3, 1).reshape(H * W, cout)
+    yg = y.double().cpu()
+    assert (torch.norm(yg - yr) / torch.norm(yr)).item() < 4e-3
+    # masked data gradient: dX = conv^T(dY * (y > 0))
+    wt = torch.zeros((9, cout, cin), dtype=torch.bfloat16, device="cuda")
+    assert L.sevp_nn_weight_transpose(p(wd), p(wt), cin, cout, None) == 0
+    dx = torch.zeros((H * W, cin), dtype=torch.bfloat16, device="cuda")
+    assert L.sevp_nn_conv3x3(p(dyd), cout, 0, cout, p(wt), None, p(dx), cin, 0, cin, 1, H, W, 0, p(y),
+                             cout, 0, 1, None) == 0
+    gm = (dy.double() * (yg > 0)).reshape(1, H, W, cout).permute(0, 3, 1, 2)
+    dxr = torch.nn.grad.conv2d_input((1, cin, H, W), wr, gm, padding=1)
+    dxr = dxr.permute(0, 2, 3, 1).reshape(H * W, cin)
+    assert (torch.norm(dx.double().cpu() - dxr) / torch.norm(dxr)).item() < 4e-3
+    # weight and bias gradients (FP32 accumulation)
+    dw = torch.zeros((9, cin, cout), dtype=torch.float32, device="cuda")
+    db = torch.zeros(cout, dtype=torch.float32, device="cuda")
+    assert L.sevp_nn_conv3x3_wgrad(p(xd), cin, 0, cin, p(dyd), cout, 0, cout, p(y), cout, 0, p(dw),
+                                   p(db), 1, H, W, None) == 0
+    dwr = torch.nn.grad.conv2d_weight(xr, (cout, cin, 3, 3), gm, padding=1)  # co, ci, ky, kx
+    dwr = dwr.permute(2, 3, 1, 0).reshape(9, cin, cout)
+    assert (torch.norm(dw.double().cpu() - dwr) / torch.norm(dwr)).item() < 1e-5
+    dbr = gm.sum(dim=(0, 2, 3))
+    assert (torch.norm(db.double().cpu() - dbr) / torch.norm(dbr)).item() < 1e-5
+
+
+def test_pool_upsample_exact(torch_cuda):
+    torch = torch_cuda
+    import ctypes as C
+
+    import torch.nn.functional as F
+
+    from musoc_solver_b200.unet import lib
+
+    L = lib()
+    H, W, Cc = 8, 12, 16
+    rng = np.random.default_rng(9)
+    x = _bf(torch, rng.standard_normal((H * W, Cc))).cuda()
+    p = lambda t: C.c_void_p(t.data_ptr())
+    pooled = torch.zeros((H * W // 4, Cc), dtype=torch.bfloat16, device="cuda")
+    assert L.sevp_nn_pool(p(x), Cc, 0, p(pooled), Cc, 0, Cc, 1, H, W, 0, 0, None) == 0
+    xr = x.double().cpu().reshape(1, H, W, Cc).permute(0, 3, 1, 2)
+    pr = F.avg_pool2d(xr, 2).permute(0, 2, 3, 1).reshape(-1, Cc).to(torch.bfloat16)
+    assert torch.equal(pooled.cpu(), pr)
+    up = torch.zeros((H * W, Cc), dtype=torch.bfloat16, device="cuda")
+    assert L.sevp_nn_upsample(p(pooled), Cc, 0, p(up), Cc, 0, Cc, 1, H, W, 0, None) == 0
+    ur = F.interpolate(pooled.double().cpu().reshape(1, H // 2, W // 2, Cc).permute(0, 3, 1, 2),
+                       scale_factor=2, mode="nearest").permute(0, 2, 3, 1).reshape(-1, Cc)
+    assert torch.equal(up.double().cpu(), ur)
