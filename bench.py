@@ -11,11 +11,17 @@ Workload (one "step" = one time step of a sequence of barotropic solves):
   * a step solves A eta_n = b_n to ||b - A eta|| / ||b|| <= 1e-12 (FP64
     residual) on the GPU.
 
+The first --train-steps steps of the sequence are solved in FP64 (untimed);
+they are the history of the timed steps and the training set of the
+warm-start U-Net, which is trained on them at start-up by the library's own
+BF16 forward/backward kernels (untimed).
+
 Arms reported in one JSON line:
-  value        mixed precision (FP32 PCG + FP64 refinement) from the best
-               warm start available (learned network when trained weights
-               are given, else linear extrapolation of the two previous
-               solutions); inputs resident in HBM, device-timed
+  value        mixed precision (FP32 PCG + FP64 refinement) from the learned
+               warm start (network inference inside the timing); inputs
+               resident in HBM, device-timed
+  linear_mixed the same steps from linear extrapolation 2 eta[n-1] - eta[n-2]
+               (no network)
   fp64_plain   the plain FP64 SEVP-PCG from a zero guess on the same steps
   e2e          the value arm through the C ABI with host buffers (b_n,
                eta_{n-1}, eta_{n-2} in, eta_n out, copies inside the timing)
@@ -61,8 +67,14 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precond-fp32", type=int, default=0,
                     help="FP32 influence matrices in the inner FP32 solve of the mixed arms")
-    ap.add_argument("--weights", default=os.path.join(ROOT, "musoc_solver_b200", "weights",
-                                                      "unet_eddy.npz"))
+    ap.add_argument("--train-steps", type=int, default=40,
+                    help="leading steps of the sequence solved in FP64 and used to train the "
+                         "warm-start network (untimed)")
+    ap.add_argument("--epochs", type=int, default=3)
+    ap.add_argument("--coarse", type=int, default=4, choices=[1, 2, 4],
+                    help="the network runs on the grid averaged over coarse x coarse cells")
+    ap.add_argument("--no-learned", action="store_true",
+                    help="value arm from linear extrapolation instead of the network")
     return ap.parse_args()
 
 
@@ -231,7 +243,9 @@ def run_native(args, world, rank, local, dist):
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     K, W = args.steps, args.warmup
-    nsteps = W + K + 2
+
+    T = max(args.train_steps, 4)
+    nsteps = T + W + K
     p, rhs = make_sequence(args.nx, args.ny, nsteps)
     n = p.nx * p.ny
     solver = SevpSolver(p, tile_m=TILE_M, tile_h=TILE_H, growth_limit=GROWTH,
@@ -240,23 +254,30 @@ def run_native(args, world, rank, local, dist):
     b_dev = [torch.from_numpy(b).to(dev) for b in rhs]
     torch.cuda.synchronize()
 
-    # learned warm start if trained weights exist, else linear extrapolation
+    # the leading T steps: FP64 solves from linear extrapolation (untimed);
+    # they are the history of the timed steps and the network's training set
+    from musoc_solver_b200.warmstart import LearnedWarmStart, solve_sequence, train
+
+    eta = solve_sequence(solver, b_dev[:T])
+    eta += [torch.zeros_like(eta[0]) for _ in range(W + K)]
     guess_mode, guess_name = N.GUESS_LINEAR, "linear extrapolation 2*eta[n-1]-eta[n-2]"
-    warm = None
-    if os.path.exists(args.weights):
-        try:
-            from musoc_solver_b200.warmstart import LearnedWarmStart
-
-            warm = LearnedWarmStart.load(args.weights, p, device=dev)
-            warm.attach(solver)
-            guess_mode, guess_name = N.GUESS_LEARNED, "learned U-Net (BF16)"
-        except Exception as e:  # report and fall back to the physics guess
-            print(f"# warm start network unavailable: {e}", file=sys.stderr)
-
-    # history: the first two steps solved in FP64 from zero (untimed)
-    eta = [torch.zeros(p.ny, p.nx, dtype=torch.float64, device=dev) for _ in range(nsteps)]
-    for k in range(2):
-        eta[k].copy_(solver.solve(b_dev[k], precision=0)[0])
+    warm, train_info = None, None
+    if not args.no_learned:
+        t0 = time.perf_counter()
+        trainer = LearnedWarmStart.create(solver, seed=0, train=True, coarse=args.coarse)
+        losses = train(trainer, eta, b_dev, list(range(2, T)), epochs=args.epochs, lr=2e-3,
+                       lr_final=2e-4)
+        warm = trainer.inference_copy()
+        del trainer
+        torch.cuda.synchronize()
+        warm.attach(solver)
+        guess_mode = N.GUESS_LEARNED
+        guess_name = (f"learned: U-Net (4 levels, 32 base channels, BF16) on the "
+                      f"{warm.net.H}x{warm.net.W} grid ({args.coarse}x{args.coarse} averages), "
+                      "correction added to 2*eta[n-1]-eta[n-2] + one tile-SEVP solve")
+        train_info = {"steps": T - 2, "epochs": args.epochs, "seconds": time.perf_counter() - t0,
+                      "loss_first": losses[0][1], "loss_last": losses[-1][1],
+                      "network_grid": [warm.net.W, warm.net.H]}
 
     def barrier():
         if dist is not None:
@@ -271,45 +292,54 @@ def run_native(args, world, rank, local, dist):
         return float(t.item())
 
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    timed = range(T + W, T + W + K)
 
-    # ---- value arm: mixed precision + warm start, device-resident inputs
-    for k in range(2, 2 + W):
-        solver.solve_step(b_dev[k], eta[k - 1], eta[k - 2], eta[k], guess=guess_mode, precision=1)
-    barrier()
-    solver.profile(True)
-    l_value0 = solver.launches()
-    reps = []
-    with ClockSampler(local) as clk:
+    def run_arm(mode, hist):
+        """Warm-up and timed steps of a sequence arm; hist holds the solutions."""
+        for k in range(T, T + W):
+            solver.solve_step(b_dev[k], hist[k - 1], hist[k - 2], hist[k], guess=mode, precision=1)
+        barrier()
+        reps = []
         ev0.record(stream)
-        for k in range(2 + W, 2 + W + K):
-            _, r = solver.solve_step(b_dev[k], eta[k - 1], eta[k - 2], eta[k], guess=guess_mode,
+        for k in timed:
+            _, r = solver.solve_step(b_dev[k], hist[k - 1], hist[k - 2], hist[k], guess=mode,
                                      precision=1)
             reps.append(r)
         ev1.record(stream)
         torch.cuda.synchronize()
-    t_value = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
+        return max_over_ranks(ev0.elapsed_time(ev1) / 1e3), reps
+
+    # ---- value arm: mixed precision + warm start, device-resident inputs
+    solver.profile(True)
+    l_value0 = solver.launches()
+    with ClockSampler(local) as clk:
+        t_value, reps = run_arm(guess_mode, eta)
     prof = solver.profile_read()
     solver.profile(False)
     launches_value = solver.launches() - l_value0
     relres = [r.rel_residual for r in reps]
     status = [r.status for r in reps]
 
+    # ---- the same sequence from linear extrapolation (no network)
+    eta_lin = eta[:T] + [torch.zeros_like(eta[0]) for _ in range(W + K)]
+    t_lin, reps_lin = run_arm(N.GUESS_LINEAR, eta_lin)
+    del eta_lin
+
     # error of the value arm against an FP64 solve of the same steps
     ref_x = torch.zeros_like(eta[0])
     errs = []
-    for k in (2 + W, 2 + W + K - 1):
+    for k in (timed[0], timed[-1]):
         solver.solve(b_dev[k], x=ref_x.zero_(), precision=0)
         errs.append(float((eta[k] - ref_x).abs().max() / ref_x.abs().max()))
 
     # ---- plain FP64 SEVP-PCG from a zero guess
     xz = torch.zeros_like(eta[0])
-    for k in range(2, 2 + min(W, 2)):
+    for k in range(T, T + W):
         solver.solve(b_dev[k], x=xz.zero_(), precision=0)
     barrier()
-    l0 = solver.launches()
     ev0.record(stream)
     it64 = []
-    for k in range(2 + W, 2 + W + K):
+    for k in timed:
         _, r = solver.solve(b_dev[k], x=xz.zero_(), precision=0)
         it64.append(r.iterations)
     ev1.record(stream)
@@ -320,7 +350,7 @@ def run_native(args, world, rank, local, dist):
     barrier()
     ev0.record(stream)
     itmz = []
-    for k in range(2 + W, 2 + W + K):
+    for k in timed:
         _, r = solver.solve(b_dev[k], x=xz.zero_(), precision=1)
         itmz.append(r.iterations)
     ev1.record(stream)
@@ -329,17 +359,17 @@ def run_native(args, world, rank, local, dist):
 
     # ---- e2e: the same value arm through the C ABI with host buffers
     pin = lambda a: torch.from_numpy(a).pin_memory().numpy()
-    b_host = [pin(b) for b in rhs]
-    eta_host = [pin(np.zeros((p.ny, p.nx))) for _ in range(nsteps)]
-    for k in range(2):
+    b_host = {k: pin(rhs[k]) for k in range(T, T + W + K)}
+    eta_host = {k: pin(np.zeros((p.ny, p.nx))) for k in range(T - 2, T + W + K)}
+    for k in (T - 2, T - 1):
         eta_host[k][:] = eta[k].cpu().numpy()
-    for k in range(2, 2 + W):
+    for k in range(T, T + W):
         solver.solve_step_host(b_host[k], eta_host[k - 1], eta_host[k - 2], eta_host[k],
                                guess=guess_mode, precision=1)
     barrier()
     t0 = time.perf_counter()
     l1 = solver.launches()
-    for k in range(2 + W, 2 + W + K):
+    for k in timed:
         solver.solve_step_host(b_host[k], eta_host[k - 1], eta_host[k - 2], eta_host[k],
                                guess=guess_mode, precision=1)
     torch.cuda.synchronize()
@@ -364,9 +394,9 @@ def run_native(args, world, rank, local, dist):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cores = os.cpu_count() or 1
-        dt, itc, relc = cpu_solve_seconds(p, rhs[2 + W], cores, solver.tile_nb)
+        dt, itc, relc = cpu_solve_seconds(p, rhs[timed[0]], cores, solver.tile_nb)
         cpu = {"value": 1.0 / dt, "unit": "solves/s", "cores": cores, "kind": "port",
-               "sample": f"one full FP64 tile-SEVP PCG solve of step {2 + W} with the C oracle "
+               "sample": f"one full FP64 tile-SEVP PCG solve of step {timed[0]} with the C oracle "
                          f"(OpenMP, {cores} threads, {itc} iterations, rel. residual {relc:.2e}), "
                          "setup excluded"}
 
@@ -399,6 +429,10 @@ def run_native(args, world, rank, local, dist):
                        "mean_iterations": float(np.mean(it64))},
         "mixed_zero_guess": {"value": world * K / t_mixed0, "unit": "solves/s",
                              "mean_iterations": float(np.mean(itmz))},
+        "linear_mixed": {"value": world * K / t_lin, "unit": "solves/s",
+                         "ms_per_step": 1e3 * t_lin / K,
+                         "mean_iterations": float(np.mean([r.iterations for r in reps_lin]))},
+        "warm_start_training": train_info,
         "value_arm": {"mean_iterations": float(np.mean([r.iterations for r in reps])),
                       "mean_refinements": float(np.mean([r.refinements for r in reps])),
                       "max_rel_residual": float(max(relres)), "status": sorted(set(status)),

@@ -285,6 +285,7 @@ struct OpResidual {
   R *r;
   SolveState *st;
   double tol2;
+  double outer2;  // (safety * outer tolerance)^2: the inner solve need not go below it
   int set_inner;  // 1: also initialise the inner FP32 solve state
   __device__ void prepare(SolveState *) {}
   __device__ double value(size_t idx) const {
@@ -307,7 +308,8 @@ struct OpResidual {
       // inner solve starts from zero: its reference norm is ||r||^2
       st->bb = s[0];
       st->rr = s[0];
-      st->tol2 = tol2;
+      // reduce ||r|| by inner_tol, or only as far as the outer test needs
+      st->tol2 = s[0] > 0.0 ? fmax(tol2, fmin(outer2 * s[1] / s[0], 0.25)) : tol2;
       st->iter = 0;
       st->done = 0;
       st->beta = 0.0;
@@ -1213,8 +1215,9 @@ static int read_state(sevp_ctx *ctx) {
 // Residual pass: xout = x + d; r = b - A xout; ||r||^2, ||b||^2 into state.
 template <typename R>
 static int launch_residual(sevp_ctx *ctx, const double *x, const float *d, double *xout,
-                           const double *b, R *r, int set_inner, double tol2) {
-  OpResidual<R> op{x, d, xout, b, r, ctx->st, tol2, set_inner};
+                           const double *b, R *r, int set_inner, double tol2,
+                           double outer2 = 0.0) {
+  OpResidual<R> op{x, d, xout, b, r, ctx->st, tol2, outer2, set_inner};
   return launch_stencil(ctx, op, 2);
 }
 
@@ -1327,6 +1330,9 @@ static int solve_mixed(sevp_ctx *ctx, const double *b, double *x, const sevp_sol
   } flag{ctx};
   ctx->infl32_active = o->precond_fp32 != 0;
   const double inner2 = o->inner_tol * o->inner_tol;
+  // the last inner solve stops at half the outer tolerance instead of
+  // overshooting it by up to a factor inner_tol
+  const double outer2 = 0.25 * o->tol * o->tol;
   int total = 0, status = SEVP_MAXITER;
   double *xa = x, *xb = ctx->x64s;  // ping-pong: the residual kernel reads xa, writes xb
   bool have_d = false;
@@ -1335,9 +1341,9 @@ static int solve_mixed(sevp_ctx *ctx, const double *b, double *x, const sevp_sol
     ctx->launches++;
     int s;
     if (have_d)
-      s = launch_residual<float>(ctx, xa, ctx->d32, xb, b, ctx->r32, 1, inner2);
+      s = launch_residual<float>(ctx, xa, ctx->d32, xb, b, ctx->r32, 1, inner2, outer2);
     else
-      s = launch_residual<float>(ctx, xa, nullptr, nullptr, b, ctx->r32, 1, inner2);
+      s = launch_residual<float>(ctx, xa, nullptr, nullptr, b, ctx->r32, 1, inner2, outer2);
     if (s) return s;
     if (have_d) std::swap(xa, xb);
     s = read_state(ctx);
@@ -1516,14 +1522,40 @@ __global__ void k_rms3(const double *a, const double *b, const double *c, size_t
   reduce_and_finish<3>(s, partials, ticket, fin);
 }
 
+// The network grid is the solver grid averaged over coarse x coarse cells
+// (coarse = 1, 2 or 4), padded with zeros to wn x hn (multiples of 8).
+// feat holds 16 BF16 channels per network pixel.
+__device__ __forceinline__ bool net_cell(size_t k, int wn, int cx, int cy, int coarse, int &i,
+                                         int &j) {
+  const int ci = (int)(k % wn), cj = (int)(k / wn);
+  i = ci * coarse;
+  j = cj * coarse;
+  return ci < cx && cj < cy;
+}
+
 __global__ void k_pack_features(const double *r, const double *m, const double *d,
-                                const float *scales, __nv_bfloat16 *feat, size_t n) {
+                                const float *scales, __nv_bfloat16 *feat, int nx, int ny,
+                                int coarse, int wn, int hn) {
+  const int cx = nx / coarse, cy = ny / coarse;
+  const size_t n = (size_t)wn * hn;
   for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
        k += (size_t)gridDim.x * blockDim.x) {
+    int i, j;
+    double a = 0.0, bm = 0.0, c = 0.0;
+    if (net_cell(k, wn, cx, cy, coarse, i, j)) {
+      for (int dj = 0; dj < coarse; ++dj)
+        for (int di = 0; di < coarse; ++di) {
+          const size_t q = (size_t)(j + dj) * nx + i + di;
+          a += r[q];
+          bm += m[q];
+          c += d[q];
+        }
+    }
+    const double inv = 1.0 / (coarse * coarse);
     __nv_bfloat16 v[16];
-    v[0] = __float2bfloat16((float)(r[k] / scales[0]));
-    v[1] = __float2bfloat16((float)(m[k] / scales[1]));
-    v[2] = __float2bfloat16((float)(d[k] / scales[2]));
+    v[0] = __float2bfloat16((float)(a * inv / scales[0]));
+    v[1] = __float2bfloat16((float)(bm * inv / scales[1]));
+    v[2] = __float2bfloat16((float)(c * inv / scales[2]));
 #pragma unroll
     for (int q = 3; q < 16; ++q) v[q] = __float2bfloat16(0.f);
     uint4 *dst = reinterpret_cast<uint4 *>(feat + k * 16);
@@ -1532,26 +1564,67 @@ __global__ void k_pack_features(const double *r, const double *m, const double *
   }
 }
 
-// target of training: (eta - e - m) / scale_m ; combine: x = e + m + scale_m * y
+// training target (eta - e - m) / scale_m averaged like the features (0 on
+// the padding); combine x = e + m + scale_m * y with y taken from the
+// network cell that contains the point
 __global__ void k_nn_target(const double *eta, const double *e, const double *m,
-                            const float *scales, float *t, size_t n) {
+                            const float *scales, float *t, int nx, int ny, int coarse, int wn,
+                            int hn) {
+  const int cx = nx / coarse, cy = ny / coarse;
+  const size_t n = (size_t)wn * hn;
   for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
-       k += (size_t)gridDim.x * blockDim.x)
-    t[k] = (float)((eta[k] - e[k] - m[k]) / scales[1]);
+       k += (size_t)gridDim.x * blockDim.x) {
+    int i, j;
+    double a = 0.0;
+    if (net_cell(k, wn, cx, cy, coarse, i, j)) {
+      for (int dj = 0; dj < coarse; ++dj)
+        for (int di = 0; di < coarse; ++di) {
+          const size_t q = (size_t)(j + dj) * nx + i + di;
+          a += eta[q] - e[q] - m[q];
+        }
+    }
+    t[k] = (float)(a / (coarse * coarse) / scales[1]);
+  }
 }
 __global__ void k_nn_combine(const double *e, const double *m, const float *y, const float *scales,
-                             double *x, size_t n) {
+                             double *x, int nx, int ny, int coarse, int wn) {
+  const size_t n = (size_t)nx * ny;
+  const int cx = nx / coarse, cy = ny / coarse;
+  const float inv = 1.f / coarse;
   for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
-       k += (size_t)gridDim.x * blockDim.x)
-    x[k] = e[k] + m[k] + (double)scales[1] * (double)y[k];
+       k += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(k % nx), j = (int)(k / nx);
+    double c;
+    if (coarse == 1) {
+      c = y[(size_t)j * wn + i];
+    } else {
+      // bilinear between network cell centres (clamped at the edges), so
+      // the correction adds no steps at cell boundaries
+      const float u = (i + 0.5f) * inv - 0.5f, v = (j + 0.5f) * inv - 0.5f;
+      const int i0 = max(0, min(cx - 1, (int)floorf(u))), j0 = max(0, min(cy - 1, (int)floorf(v)));
+      const int i1 = min(cx - 1, i0 + 1), j1 = min(cy - 1, j0 + 1);
+      const float wx = fminf(fmaxf(u - i0, 0.f), 1.f), wy = fminf(fmaxf(v - j0, 0.f), 1.f);
+      const float y00 = y[(size_t)j0 * wn + i0], y01 = y[(size_t)j0 * wn + i1];
+      const float y10 = y[(size_t)j1 * wn + i0], y11 = y[(size_t)j1 * wn + i1];
+      c = (1.f - wy) * ((1.f - wx) * y00 + wx * y01) + wy * ((1.f - wx) * y10 + wx * y11);
+    }
+    x[k] = e[k] + m[k] + (double)scales[1] * c;
+  }
 }
 
 static unsigned grid_for(size_t n) { return (unsigned)std::min<size_t>((n + 255) / 256, 148 * 16); }
 
+static bool net_grid_ok(const sevp_ctx *ctx, int coarse, int wn, int hn) {
+  if (coarse != 1 && coarse != 2 && coarse != 4) return false;
+  if (ctx->nx % coarse || ctx->ny % coarse) return false;
+  return wn % 8 == 0 && hn % 8 == 0 && wn >= ctx->nx / coarse && hn >= ctx->ny / coarse;
+}
+
 extern "C" int sevp_nn_features(sevp_ctx *ctx, const double *eta1, const double *eta2,
                                 const double *b, double *e, double *m, double *d, void *feat,
-                                float *scales) {
-  if (!ctx || !ctx->have_op || !eta1 || !eta2 || !b || !e || !m || !d || !feat || !scales)
+                                float *scales, int coarse, int wn, int hn) {
+  if (!ctx || !ctx->have_op || !eta1 || !eta2 || !b || !e || !m || !d || !feat || !scales ||
+      !net_grid_ok(ctx, coarse, wn, hn))
     return SEVP_BAD_ARG;
   int s = form_guess(ctx, eta1, eta2, e, 2);  // e = 2 eta1 - eta2
   if (s) return s;
@@ -1563,26 +1636,30 @@ extern "C" int sevp_nn_features(sevp_ctx *ctx, const double *eta1, const double 
   if (s) return s;
   k_rms3<<<grid_for(ctx->n), 256, 0, ctx->stream>>>(ctx->r64, m, d, ctx->n, ctx->partials,
                                                    ctx->tickets + 5, scales);
-  k_pack_features<<<grid_for(ctx->n), 256, 0, ctx->stream>>>(ctx->r64, m, d, scales,
-                                                            (__nv_bfloat16 *)feat, ctx->n);
+  k_pack_features<<<grid_for((size_t)wn * hn), 256, 0, ctx->stream>>>(
+      ctx->r64, m, d, scales, (__nv_bfloat16 *)feat, ctx->nx, ctx->ny, coarse, wn, hn);
   ctx->launches += 2;
   SEVP_CUDA_TRY(cudaGetLastError());
   return SEVP_OK;
 }
 
 extern "C" int sevp_nn_target(sevp_ctx *ctx, const double *eta, const double *e, const double *m,
-                              const float *scales, float *t) {
-  if (!ctx || !eta || !e || !m || !scales || !t) return SEVP_BAD_ARG;
-  k_nn_target<<<grid_for(ctx->n), 256, 0, ctx->stream>>>(eta, e, m, scales, t, ctx->n);
+                              const float *scales, float *t, int coarse, int wn, int hn) {
+  if (!ctx || !eta || !e || !m || !scales || !t || !net_grid_ok(ctx, coarse, wn, hn))
+    return SEVP_BAD_ARG;
+  k_nn_target<<<grid_for((size_t)wn * hn), 256, 0, ctx->stream>>>(eta, e, m, scales, t, ctx->nx,
+                                                                 ctx->ny, coarse, wn, hn);
   ctx->launches++;
   SEVP_CUDA_TRY(cudaGetLastError());
   return SEVP_OK;
 }
 
 extern "C" int sevp_nn_combine(sevp_ctx *ctx, const double *e, const double *m, const float *y,
-                               const float *scales, double *x) {
-  if (!ctx || !e || !m || !y || !scales || !x) return SEVP_BAD_ARG;
-  k_nn_combine<<<grid_for(ctx->n), 256, 0, ctx->stream>>>(e, m, y, scales, x, ctx->n);
+                               const float *scales, double *x, int coarse, int wn, int hn) {
+  if (!ctx || !e || !m || !y || !scales || !x || !net_grid_ok(ctx, coarse, wn, hn))
+    return SEVP_BAD_ARG;
+  k_nn_combine<<<grid_for(ctx->n), 256, 0, ctx->stream>>>(e, m, y, scales, x, ctx->nx, ctx->ny,
+                                                         coarse, wn);
   ctx->launches++;
   SEVP_CUDA_TRY(cudaGetLastError());
   return SEVP_OK;

@@ -59,9 +59,9 @@ _SIGS = {
                       C.c_longlong, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int, C.c_float,
                       C.c_void_p], C.c_int),
     "sevp_nn_to_bf16": ([C.c_void_p, C.c_void_p, C.c_longlong, C.c_void_p], C.c_int),
-    "sevp_nn_features": ([C.c_void_p] * 9, C.c_int),
-    "sevp_nn_target": ([C.c_void_p] * 6, C.c_int),
-    "sevp_nn_combine": ([C.c_void_p] * 6, C.c_int),
+    "sevp_nn_features": ([C.c_void_p] * 9 + [C.c_int] * 3, C.c_int),
+    "sevp_nn_target": ([C.c_void_p] * 6 + [C.c_int] * 3, C.c_int),
+    "sevp_nn_combine": ([C.c_void_p] * 6 + [C.c_int] * 3, C.c_int),
     "sevp_stream": ([C.c_void_p], C.c_void_p),
     "sevp_add_launches": ([C.c_void_p, C.c_int], C.c_int),
 }

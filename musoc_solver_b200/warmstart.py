@@ -26,6 +26,15 @@ import numpy as np
 from . import native as N
 from .unet import UNet, lib as nnlib
 
+def net_grid(nx: int, ny: int, coarse: int):
+    """(H, W) of the network for a solver grid averaged over coarse x coarse
+    cells, rounded up to multiples of 8."""
+    if coarse not in (1, 2, 4) or nx % coarse or ny % coarse:
+        raise ValueError("coarse must be 1, 2 or 4 and divide the grid")
+    r8 = lambda v: (v + 7) // 8 * 8
+    return r8(ny // coarse), r8(nx // coarse)
+
+
 WARMSTART_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                            C.c_int, C.c_int, C.c_void_p)
 
@@ -39,7 +48,14 @@ class LearnedWarmStart:
         self.torch = torch
         self.solver = solver
         self.net = unet
-        n = solver.nx * solver.ny
+        # the network grid: the solver grid averaged over coarse x coarse
+        # cells, padded to multiples of 8
+        self.coarse = next((c for c in (1, 2, 4) if net_grid(solver.nx, solver.ny, c) ==
+                            (unet.H, unet.W)), None)
+        if self.coarse is None:
+            raise ValueError("network grid does not match the solver grid at coarse 1, 2 or 4")
+        self._g = (self.coarse, unet.W, unet.H)
+        n = unet.H * unet.W
         dev = solver.device
         self.e = torch.zeros((solver.ny, solver.nx), dtype=torch.float64, device=dev)
         self.m = torch.zeros_like(self.e)
@@ -57,7 +73,7 @@ class LearnedWarmStart:
                                      C.c_void_p(int(b)), C.c_void_p(self.e.data_ptr()),
                                      C.c_void_p(self.m.data_ptr()), C.c_void_p(self.d.data_ptr()),
                                      C.c_void_p(self.net.A["x"].data_ptr()),
-                                     C.c_void_p(self.scales.data_ptr()))
+                                     C.c_void_p(self.scales.data_ptr()), *self._g)
         N.check(s, "sevp_nn_features")
 
     def _forward(self):
@@ -91,7 +107,8 @@ class LearnedWarmStart:
         s = nnlib().sevp_nn_combine(self.solver.h, C.c_void_p(self.e.data_ptr()),
                                     C.c_void_p(self.m.data_ptr()),
                                     C.c_void_p(self.net.A["y"].data_ptr()),
-                                    C.c_void_p(self.scales.data_ptr()), C.c_void_p(ptr(x)))
+                                    C.c_void_p(self.scales.data_ptr()), C.c_void_p(ptr(x)),
+                                    *self._g)
         N.check(s, "sevp_nn_combine")
 
     def attach(self, solver=None):
@@ -124,7 +141,7 @@ class LearnedWarmStart:
         s = nnlib().sevp_nn_target(self.solver.h, C.c_void_p(eta.data_ptr()),
                                    C.c_void_p(self.e.data_ptr()), C.c_void_p(self.m.data_ptr()),
                                    C.c_void_p(self.scales.data_ptr()),
-                                   C.c_void_p(self.target.data_ptr()))
+                                   C.c_void_p(self.target.data_ptr()), *self._g)
         N.check(s, "sevp_nn_target")
         self.net.forward()
         self.net.backward(self.target)
@@ -136,18 +153,28 @@ class LearnedWarmStart:
         np.savez(path, **st)
 
     @classmethod
-    def load(cls, path, solver):
+    def load(cls, path, solver, coarse=1):
         """Inference-only network for the solver's grid from saved weights."""
         st = dict(np.load(path))
-        net = UNet(solver.ny, solver.nx, device=solver.device, train=False, stream=solver.stream)
+        H, W = net_grid(solver.nx, solver.ny, coarse)
+        net = UNet(H, W, device=solver.device, train=False, stream=solver.stream)
         net.load_state(st)
         return cls(solver, net)
 
     @classmethod
-    def create(cls, solver, seed=0, train=True):
-        net = UNet(solver.ny, solver.nx, device=solver.device, train=train, seed=seed,
-                   stream=solver.stream)
+    def create(cls, solver, seed=0, train=True, coarse=1):
+        """A fresh network on the solver grid averaged over coarse x coarse
+        cells (coarse = 1, 2 or 4)."""
+        H, W = net_grid(solver.nx, solver.ny, coarse)
+        net = UNet(H, W, device=solver.device, train=train, seed=seed, stream=solver.stream)
         return cls(solver, net, use_graph=not train)
+
+    def inference_copy(self):
+        """A graph-captured inference-only warm start with the trained weights."""
+        net = UNet(self.net.H, self.net.W, device=self.solver.device, train=False,
+                   stream=self.solver.stream)
+        net.load_state(self.net.state())
+        return LearnedWarmStart(self.solver, net, use_graph=True)
 
 
 def solve_sequence(solver, rhs, tol=1e-12):

@@ -15,7 +15,8 @@ from musoc_solver_b200 import problems as P
 pytestmark = pytest.mark.gpu
 
 
-def test_learned_warm_start_beats_no_network(torch_cuda_ws):
+@pytest.mark.parametrize("coarse", [1, 2, 4])
+def test_learned_warm_start_beats_no_network(torch_cuda_ws, coarse):
     torch = torch_cuda_ws
     from musoc_solver_b200 import native as N
     from musoc_solver_b200.solver import SevpSolver
@@ -28,7 +29,7 @@ def test_learned_warm_start_beats_no_network(torch_cuda_ws):
            for _, b in P.eddy_rhs(nx, ny, range(nsteps), seed=4)]
     s = SevpSolver(p, tile_m=16, tile_h=16)
     etas = solve_sequence(s, rhs)
-    warm = LearnedWarmStart.create(s, seed=0, train=True)
+    warm = LearnedWarmStart.create(s, seed=0, train=True, coarse=coarse)
     train_idx = list(range(2, 36))
     test_idx = list(range(38, nsteps))
     losses = train(warm, etas, rhs, train_idx, epochs=6, lr=2e-3, lr_final=2e-4)
@@ -36,6 +37,7 @@ def test_learned_warm_start_beats_no_network(torch_cuda_ws):
     # guess error with and without the network on held-out steps
     x = torch.zeros_like(etas[0])
     gain = []
+    warm = warm.inference_copy()
     for n in test_idx:
         warm.predict(etas[n - 1], etas[n - 2], rhs[n], x)
         err_net = float((x - etas[n]).norm())
@@ -43,7 +45,7 @@ def test_learned_warm_start_beats_no_network(torch_cuda_ws):
         gain.append(err_base / err_net)
     warm.attach()
     res = evaluate(s, warm, etas, rhs, test_idx)
-    print("warm start (mean iterations, ms):",
+    print(f"coarse={coarse} warm start (mean iterations, ms):",
           {k: (v["mean_iterations"], round(v["mean_ms"], 3)) for k, v in res.items()},
           "guess-error ratio (no network / network):", np.round(gain, 2))
     assert np.median(gain) > 1.0
