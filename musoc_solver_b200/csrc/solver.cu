@@ -97,6 +97,7 @@ __device__ __forceinline__ void reduce_and_finish(double (&v)[NV], double *parti
 // east/west neighbours come from warp shuffles, except at the warp's edge
 // lanes, which evaluate the neighbour column directly (periodic wrap in x).
 constexpr int kStencilThreads = 256;
+constexpr int kStencilCols = 30;  // output columns per warp (32 loaded)
 // Launch shape, chosen by measurement at 3600x2400 on a B200: the minimum
 // resident CTAs cap the registers (64 for the stencil, 85 for the tile
 // kernel) so that enough warps keep memory requests in flight; FP32 fields
@@ -105,7 +106,7 @@ constexpr int kStencilThreads = 256;
 #define SEVP_STENCIL_UNROLL 0
 #endif
 #ifndef SEVP_STENCIL_MINB
-#define SEVP_STENCIL_MINB 4
+#define SEVP_STENCIL_MINB 6
 #endif
 #ifndef SEVP_TILE_MINB
 #define SEVP_TILE_MINB 3
@@ -128,43 +129,40 @@ __global__ void __launch_bounds__(kStencilThreads, SEVP_STENCIL_MINB)
   op.prepare(st);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int nx = g.nx, ny = g.ny;
-  // the CTA's warps sit side by side: each row is read as one contiguous
-  // span of 256 columns, which keeps DRAM pages open across the warps
-  const int i = (blockIdx.x * (kStencilThreads / 32) + w) * 32 + lane;
+  // Overlapping warps: a warp loads 32 consecutive columns and writes the
+  // inner kStencilCols; lanes 0 and 31 only supply the west and east
+  // neighbours, so every neighbour value arrives by shuffle from the same
+  // coalesced row load.  The warps of a CTA sit side by side.
+  const int raw = (blockIdx.x * (kStencilThreads / 32) + w) * kStencilCols + lane - 1;
+  const bool out = lane >= 1 && lane <= kStencilCols && raw >= 0 && raw < nx;
+  int i = raw;
+  bool col_ok = raw >= 0 && raw < nx;
+  if (g.periodic && raw == -1) i = nx - 1, col_ok = true;
+  if (g.periodic && raw == nx) i = 0, col_ok = true;
   const int j0 = blockIdx.y * rpw;
   const int j1 = min(j0 + rpw, ny);
-  const bool col_ok = i < nx;
   double acc[Op::NV];
 #pragma unroll
   for (int k = 0; k < Op::NV; ++k) acc[k] = 0.0;
   if (j0 < ny) {
-    int iw = i - 1;
-    if (iw < 0) iw = g.periodic ? nx - 1 : -1;
-    int ie = i + 1;
-    if (ie >= nx) ie = g.periodic ? ie - nx : -1;
-    const bool own_w = (lane == 0);
-    const bool own_e = (lane == 31) || (i + 1 >= nx);
     T vb = (j0 > 0 && col_ok) ? op.value((size_t)(j0 - 1) * nx + i) : T(0);
     T vc = col_ok ? op.value((size_t)j0 * nx + i) : T(0);
     float at_prev = (SYM && j0 > 0 && col_ok) ? __ldg(c.at + (size_t)(j0 - 1) * nx + i) : 0.f;
     for (int jb = j0; jb < j1; jb += U) {
-      // loads: the next U rows of the field, U rows of coefficients, edge columns
-      T va[U], vwe[U], vee[U];
+      // loads: the next U rows of the field and U rows of coefficients
+      T va[U];
       float cb[U], cw[U], ccn[U], ce[U], cn[U];
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         const int j = jb + u;
-        const size_t row = (size_t)j * nx;
+        const size_t idx = (size_t)j * nx + i;
         const bool rok = (j < j1) && col_ok;
-        va[u] = (rok && j + 1 < ny) ? op.value(row + nx + i) : T(0);
-        vwe[u] = (rok && own_w && iw >= 0) ? op.value(row + iw) : T(0);
-        vee[u] = (rok && own_e && ie >= 0) ? op.value(row + ie) : T(0);
-        const size_t idx = row + i;
+        va[u] = (rok && j + 1 < ny) ? op.value(idx + nx) : T(0);
         ccn[u] = rok ? __ldg(c.ac + idx) : 0.f;
         ce[u] = rok ? __ldg(c.ar + idx) : 0.f;
         cn[u] = rok ? __ldg(c.at + idx) : 0.f;
         if (SYM) {
-          cw[u] = (rok && own_w && iw >= 0) ? __ldg(c.ar + row + iw) : 0.f;  // edge lanes only
+          cw[u] = 0.f;
           cb[u] = 0.f;
         } else {
           cb[u] = rok ? __ldg(c.ab + idx) : 0.f;
@@ -175,17 +173,14 @@ __global__ void __launch_bounds__(kStencilThreads, SEVP_STENCIL_MINB)
       for (int u = 0; u < U; ++u) {
         const int j = jb + u;
         if (j >= j1) break;
-        T vw = __shfl_up_sync(0xffffffffu, vc, 1);
-        T ve = __shfl_down_sync(0xffffffffu, vc, 1);
-        if (own_w) vw = vwe[u];
-        if (own_e) ve = vee[u];
+        const T vw = __shfl_up_sync(0xffffffffu, vc, 1);
+        const T ve = __shfl_down_sync(0xffffffffu, vc, 1);
         float cwu = cw[u], cbu = cb[u];
         if (SYM) {
-          const float arw = __shfl_up_sync(0xffffffffu, ce[u], 1);
-          if (!own_w) cwu = arw;
-          cbu = (u == 0) ? at_prev : cn[u - 1];
+          cwu = __shfl_up_sync(0xffffffffu, ce[u], 1);  // AL = AR of the west point
+          cbu = (u == 0) ? at_prev : cn[u - 1];          // AB = AT of the south point
         }
-        if (col_ok) {
+        if (out) {
           T av = T(cbu) * vb;
           av += T(cwu) * vw;
           av += T(ccn[u]) * vc;
@@ -322,6 +317,7 @@ struct OpResidual {
 // --------------------------------------------------- tile apply kernel
 constexpr int kTileWarps = 8;
 
+
 // Shared memory per warp: the tile's rows of z (FP64 marching state, 32
 // lanes per row), the last-equation residual of each sub-block (stored at
 // the sub-block's last row), and the mat-vec broadcast vector.
@@ -385,6 +381,53 @@ __device__ __forceinline__ void load_row(RowIn<V> &in, const Coeffs &c, const V 
   in.cn = __ldg(c.at + idx);
 }
 
+// 1/a for the marching rows: the hardware's approximate FP64 reciprocal
+// refined by two Newton-Raphson steps r <- r + r (1 - a r), each of which
+// squares the relative error (a few ulp at most from the rounded quotient).
+// It is formed off the row recurrence's dependency chain.
+__device__ __forceinline__ double march_rcp(double a) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(a));
+  double e = fma(-a, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-a, r, 1.0);
+  return fma(r, e, r);
+}
+
+// Finishes a PCG iteration after pass B: r.z and r.r are complete.
+struct TileFin {
+  SolveState *st;
+  __device__ void operator()(double (&s)[2]) {
+    double rz = s[0], rr = s[1];
+    int first = (st->beta == 0.0 && st->iter == 0);
+    st->rr = rr;
+    if (!isfinite(rz) || !isfinite(rr)) {
+      st->status = SEVP_NONFINITE;
+      st->done = 1;
+      return;
+    }
+    if (rr <= st->tol2 * st->bb) {
+      st->done = 1;
+      st->status = SEVP_OK;
+      st->rz = rz;
+      return;
+    }
+    if (st->iter >= st->max_iter) {
+      st->done = 1;
+      st->status = SEVP_MAXITER;
+      st->rz = rz;
+      return;
+    }
+    if (rz == 0.0) {
+      st->status = SEVP_BREAKDOWN;
+      st->done = 1;
+      return;
+    }
+    st->beta = first ? 0.0 : rz / st->rz;
+    st->rz = rz;
+  }
+};
+
 // UPDATE: fused x += alpha p, r -= alpha q before preconditioning (pass B).
 // DOTS:   accumulate r.z and r.r and finish the iteration on the device.
 // SYM:    symmetric operator: AL and AB are taken from the west lane's AR and
@@ -397,6 +440,7 @@ __global__ void __launch_bounds__(kTileWarps * 32, SEVP_TILE_MINB)
     k_tile_apply(TileGeom tg, Coeffs c, const MT *__restrict__ mats, V *x, const V *p, V *r,
                  const V *q, V *z, SolveState *st, double *partials, unsigned *ticket) {
   if (DOTS && st->done) return;
+  constexpr bool kChain = sizeof(V) == 4;
   extern __shared__ __align__(16) unsigned char tsm[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   unsigned char *base = tsm + tile_smem_per_warp(tg.hmax) * wib;
@@ -446,6 +490,11 @@ __global__ void __launch_bounds__(kTileWarps * 32, SEVP_TILE_MINB)
       }
       const double cc = cur.cc, ce = cur.ce;
       const double cn = active ? (double)cur.cn : 1.0;
+      // FP32 vectors (the inner solve): the row equation is evaluated as
+      // ((r - AB z_s - AC z_c) - AL z_w - AR z_e) * (1 / AT), so only two
+      // multiply-adds and a multiply wait on the neighbour shuffles; FP64
+      // vectors keep the reference's order and division (faster there)
+      const double rcp_k = kChain ? march_rcp(cn) : 0.0;
       if (active) {
         if (UPDATE) {
           V xn = cur.x + (V)alpha * cur.p;
@@ -459,17 +508,27 @@ __global__ void __launch_bounds__(kTileWarps * 32, SEVP_TILE_MINB)
         acc_rr += rv * rv;
       }
       if (k == kb) zc = 0.0;
+      const double part = (kChain && active) ? (rv - cs * zb) - cc * zc : 0.0;
       double zw = __shfl_up_sync(0xffffffffu, zc, 1);
       double ze = __shfl_down_sync(0xffffffffu, zc, 1);
       if (n == 0) zw = 0.0;
       if (n >= mw - 1) ze = 0.0;
       zs[k * 32 + lane] = zc;
+      const double res = (kChain && active) ? (part - cw * zw) - ce * ze : 0.0;
       if (k < ke) {
-        double zn = active ? ((((rv - cw * zw) - cs * zb) - cc * zc) - ce * ze) / cn : 0.0;
+        double zn;
+        if constexpr (kChain)
+          zn = res * rcp_k;
+        else
+          zn = active ? ((((rv - cw * zw) - cs * zb) - cc * zc) - ce * ze) / cn : 0.0;
         zb = zc;
         zc = zn;
       } else {
-        double rho = active ? (((rv - cw * zw) - cs * zb) - cc * zc) - ce * ze : 0.0;
+        double rho;
+        if constexpr (kChain)
+          rho = res;
+        else
+          rho = active ? (((rv - cw * zw) - cs * zb) - cc * zc) - ce * ze : 0.0;
         rho_s[k * 32 + lane] = rho;
         if (t < nb - 1) {
           dv[lane] = rho;
@@ -529,11 +588,17 @@ __global__ void __launch_bounds__(kTileWarps * 32, SEVP_TILE_MINB)
           if (!SYM) ncw = __ldg(c.al + id), ncs = __ldg(c.ab + id);
           ncc = __ldg(c.ac + id), nce = __ldg(c.ar + id), ncn = __ldg(c.at + id);
         }
+        const double rcp_k = kChain ? march_rcp(cn) : 0.0;
+        const double part = kChain ? -(cs * hb) - cc * hc : 0.0;
         double hw = __shfl_up_sync(0xffffffffu, hc, 1);
         double he = __shfl_down_sync(0xffffffffu, hc, 1);
         if (n == 0) hw = 0.0;
         if (n >= mw - 1) he = 0.0;
-        double hn = active ? ((((-(cw * hw)) - cs * hb) - cc * hc) - ce * he) / cn : 0.0;
+        double hn;
+        if constexpr (kChain)
+          hn = active ? ((part - cw * hw) - ce * he) * rcp_k : 0.0;
+        else
+          hn = active ? ((((-(cw * hw)) - cs * hb) - cc * hc) - ce * he) / cn : 0.0;
         zs[(k + 1) * 32 + lane] += hn;
         hb = hc;
         hc = hn;
@@ -552,38 +617,7 @@ __global__ void __launch_bounds__(kTileWarps * 32, SEVP_TILE_MINB)
   }
   if (DOTS) {
     double v2[2] = {acc_rz, acc_rr};
-    struct Fin {
-      SolveState *st;
-      __device__ void operator()(double (&s)[2]) {
-        double rz = s[0], rr = s[1];
-        int first = (st->beta == 0.0 && st->iter == 0);
-        st->rr = rr;
-        if (!isfinite(rz) || !isfinite(rr)) {
-          st->status = SEVP_NONFINITE;
-          st->done = 1;
-          return;
-        }
-        if (rr <= st->tol2 * st->bb) {
-          st->done = 1;
-          st->status = SEVP_OK;
-          st->rz = rz;
-          return;
-        }
-        if (st->iter >= st->max_iter) {
-          st->done = 1;
-          st->status = SEVP_MAXITER;
-          st->rz = rz;
-          return;
-        }
-        if (rz == 0.0) {
-          st->status = SEVP_BREAKDOWN;
-          st->done = 1;
-          return;
-        }
-        st->beta = first ? 0.0 : rz / st->rz;
-        st->rz = rz;
-      }
-    } fin{st};
+    TileFin fin{st};
     reduce_and_finish<2>(v2, partials, ticket, fin);
   }
 }
@@ -881,7 +915,8 @@ extern "C" const char *sevp_status_string(int s) {
 static int stencil_rpw(int ny) { return ny >= 1024 ? SEVP_STENCIL_RPW : 8; }
 
 static dim3 stencil_grid(const sevp_ctx *ctx, int rpw) {
-  return dim3((unsigned)ceil_div(ctx->nx, kStencilThreads), (unsigned)ceil_div(ctx->ny, rpw));
+  const int groups = ceil_div(ctx->nx, kStencilCols);
+  return dim3((unsigned)ceil_div(groups, kStencilThreads / 32), (unsigned)ceil_div(ctx->ny, rpw));
 }
 
 static size_t tile_warps(const TileGeom &tg) { return (size_t)tg.ty * tg.txg; }
@@ -1019,7 +1054,7 @@ extern "C" int sevp_create(sevp_ctx **out, int nx, int ny, int periodic, void *s
   ALLOC(ctx->tickets, 16 * sizeof(unsigned));
   // partial sums: enough for the larger of the stencil and tile grids
   // stencil grid: ceil(nx / 256) x ceil(ny / rpw), rpw >= 8
-  size_t sgrid = (size_t)ceil_div(nx, kStencilThreads) * ceil_div(ny, 8);
+  size_t sgrid = (size_t)ceil_div(ceil_div(nx, kStencilCols), kStencilThreads / 32) * ceil_div(ny, 8);
   size_t tgrid = (size_t)ceil_div(nx, 1) * ceil_div(ny, 1) / (kTileWarps) + 1024;
   ctx->partials_n = std::max(sgrid, tgrid) * 2 + 64;
   ALLOC(ctx->partials, ctx->partials_n * 8);
