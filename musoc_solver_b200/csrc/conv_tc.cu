@@ -1,0 +1,302 @@
+// 3x3 convolution (forward) of the warm-start U-Net on the fifth-generation
+// tensor cores of sm_100a: tcgen05.mma with the FP32 accumulator in tensor
+// memory (TMEM), operands staged in shared memory by cp.async.
+//
+// Implicit GEMM: D[p][n] = sum_{tap, k} In[p + shift(tap)][k] * Wk[tap][n][k]
+// over a CTA tile of 128 consecutive output pixels (UMMA M = 128) and all
+// output channels (UMMA N = cout <= 256), K = 16 per instruction.  Each
+// pipeline step stages one tap and one chunk of kc input channels:
+//   A: 128 pixels x kc channels, gathered at the tap's shifted positions
+//      (zero outside the image),
+//   B: cout x kc weights,
+// both K-major in the no-swizzle core-matrix layout: an 8-row x 16-byte
+// core matrix is 128 contiguous bytes; core matrices adjacent in K are 128 B
+// apart (leading byte offset), adjacent in M/N kc*16 B apart (stride byte
+// offset).  One thread issues the MMAs of a step and commits them to the
+// stage's mbarrier; a stage is refilled only after that barrier completes.
+// Loads run two steps ahead of the MMAs (four stages).
+//
+// Every wait on an mbarrier is bounded: on timeout the kernel records
+// SEVP_TIMEOUT in a device flag (read by sevp_nn_tc_status), skips its
+// stores, drains its copies, frees its TMEM and returns.
+#include <cuda_bf16.h>
+#include <cstdint>
+
+#include "common.cuh"
+
+typedef __nv_bfloat16 bf16;
+
+namespace {
+
+constexpr int kTcM = 128;        // pixels per CTA (UMMA M)
+constexpr int kTcThreads = 128;  // 4 warps: warp w reads TMEM lanes 32w..32w+31
+constexpr int kTcStages = 4;
+constexpr int kTcAhead = kTcStages - 2;  // steps of loads in flight ahead of the MMAs
+constexpr unsigned kSpinLimit = 1u << 22;
+
+__device__ int g_tc_error;  // first error recorded by a tensor-core kernel
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, bool valid) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src),
+               "r"(valid ? 16 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, unsigned parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait for the completion of the phase with the given parity.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, unsigned parity) {
+  for (unsigned k = 0; k < kSpinLimit; ++k)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+}
+
+// Shared-memory matrix descriptor: no swizzle, K-major.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;  // descriptor version of sm_100
+  return d;                // base offset 0, layout type 0 (no swizzle)
+}
+// Instruction descriptor of kind::f16: BF16 A and B, FP32 D, both K-major.
+__host__ __device__ constexpr uint32_t instr_desc_bf16(int m, int n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) |
+         ((uint32_t)(m >> 4) << 24);
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                       uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+__device__ __forceinline__ void tc_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(bar)
+               : "memory");
+}
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+      "[%16];\n"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+        "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+        "=r"(v[14]), "=r"(v[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+}
+
+__global__ void __launch_bounds__(kTcThreads)
+    k_conv3x3_tc(const bf16 *__restrict__ in, int in_ld, int in_off, int cin,
+                 const bf16 *__restrict__ wk, const float *__restrict__ bias, bf16 *__restrict__ out,
+                 int out_ld, int out_off, int cout, int B, int H, int W, int relu, int kc,
+                 uint32_t tmem_cols) {
+  extern __shared__ __align__(1024) unsigned char sm[];
+  __shared__ __align__(8) uint64_t bars[kTcStages];
+  __shared__ uint32_t s_tmem;
+  __shared__ int s_py[kTcM], s_px[kTcM];
+  __shared__ long long s_pimg[kTcM];  // first pixel of the row's image, -1 past the end
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const long long P = (long long)B * H * W;
+  const long long p0 = (long long)blockIdx.x * kTcM;
+  const int kc8 = kc >> 3;
+  const uint32_t a_bytes = (uint32_t)kTcM * kc * 2, b_bytes = (uint32_t)cout * kc * 2;
+  const uint32_t stage_bytes = a_bytes + b_bytes;
+  const uint32_t sbase = smem_u32(sm);
+  const int nkc = cin / kc;
+  const int T = 9 * nkc;
+  const uint32_t core_sbo = (uint32_t)kc8 * 128;  // next 8 rows (M or N)
+
+  {  // pixel coordinates of the tile's rows
+    const long long p = p0 + tid;
+    if (p < P) {
+      const long long img = p / ((long long)H * W);
+      const int rem = (int)(p - img * H * W);
+      s_py[tid] = rem / W;
+      s_px[tid] = rem - (rem / W) * W;
+      s_pimg[tid] = img * H * W;
+    } else {
+      s_py[tid] = 0, s_px[tid] = 0, s_pimg[tid] = -1;
+    }
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                     smem_u32(&s_tmem)),
+                 "r"(tmem_cols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+  }
+  if (tid == 0) {
+    for (int s = 0; s < kTcStages; ++s) mbar_init(smem_u32(&bars[s]), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = s_tmem;
+
+  auto issue = [&](int s) {
+    const int st = s % kTcStages;
+    const int tap = s / nkc, c0 = (s - tap * nkc) * kc;
+    const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+    const uint32_t a_s = sbase + st * stage_bytes, b_s = a_s + a_bytes;
+    for (int e = tid; e < kTcM * kc8; e += kTcThreads) {
+      const int r = e / kc8, c = e - r * kc8;
+      const int y = s_py[r] + dy, x = s_px[r] + dx;
+      const bool ok = s_pimg[r] >= 0 && y >= 0 && y < H && x >= 0 && x < W;
+      const bf16 *src =
+          ok ? in + ((s_pimg[r] + (long long)y * W + x) * in_ld + in_off + c0 + c * 8) : in;
+      cp_async16(a_s + (r >> 3) * core_sbo + c * 128 + (r & 7) * 16, src, ok);
+    }
+    for (int e = tid; e < cout * kc8; e += kTcThreads) {
+      const int n = e / kc8, c = e - n * kc8;
+      const bf16 *src = wk + ((size_t)tap * cout + n) * cin + c0 + c * 8;
+      cp_async16(b_s + (n >> 3) * core_sbo + c * 128 + (n & 7) * 16, src, true);
+    }
+  };
+
+  const uint32_t idesc = instr_desc_bf16(kTcM, cout);
+  bool failed = false;
+  for (int s = 0; s < kTcAhead && s < T; ++s) {
+    issue(s);
+    cp_async_commit();
+  }
+  for (int s = 0; s < T; ++s) {
+    const int sn = s + kTcAhead;
+    if (sn < T) {
+      if (sn >= kTcStages) {  // the stage was last read by the MMAs of step sn - kTcStages
+        const int sp = sn - kTcStages;
+        if (!mbar_wait(smem_u32(&bars[sp % kTcStages]), (unsigned)(sp / kTcStages) & 1u))
+          failed = true;
+      }
+      if (!failed) issue(sn);
+    }
+    cp_async_commit();
+    cp_async_wait<kTcAhead>();  // this thread's copies of step s have landed
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      tc_fence_after();
+      const int st = s % kTcStages;
+      const uint32_t a_s = sbase + st * stage_bytes, b_s = a_s + a_bytes;
+      for (int k16 = 0; k16 < (kc >> 4); ++k16) {
+        const uint64_t ad = smem_desc(a_s + k16 * 256, 128, core_sbo);
+        const uint64_t bd = smem_desc(b_s + k16 * 256, 128, core_sbo);
+        tc_mma(tmem, ad, bd, idesc, (s > 0 || k16 > 0) ? 1u : 0u);
+      }
+      tc_commit(smem_u32(&bars[st]));
+    }
+  }
+  // all MMAs have completed once the last step's commit has arrived
+  if (!mbar_wait(smem_u32(&bars[(T - 1) % kTcStages]), (unsigned)((T - 1) / kTcStages) & 1u))
+    failed = true;
+  cp_async_wait<0>();
+  failed = __syncthreads_or(failed) != 0;  // a timeout anywhere voids the whole tile
+  tc_fence_after();
+  const long long p = p0 + warp * 32 + lane;
+  const uint32_t tl = tmem + ((uint32_t)(warp * 32) << 16);
+  for (int n0 = 0; n0 < cout; n0 += 16) {
+    uint32_t v[16];
+    tmem_ld16(tl + (uint32_t)n0, v);
+    if (p < P && !failed) {
+      __align__(16) bf16 o[16];
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        float f = __uint_as_float(v[q]);
+        if (bias) f += bias[n0 + q];
+        if (relu) f = fmaxf(f, 0.f);
+        o[q] = __float2bfloat16(f);
+      }
+      uint4 *dst = reinterpret_cast<uint4 *>(out + p * out_ld + out_off + n0);
+      dst[0] = *reinterpret_cast<const uint4 *>(&o[0]);
+      dst[1] = *reinterpret_cast<const uint4 *>(&o[8]);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(tmem_cols)
+                 : "memory");
+  if (failed) atomicCAS(&g_tc_error, 0, SEVP_TIMEOUT);
+}
+
+bool aligned16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
+
+}  // namespace
+
+extern "C" {
+
+// out[p][out_off + n] = act(bias[n] + sum_{tap, k} in[p + shift(tap)][in_off + k] * wk[tap][n][k])
+// with wk the K-major ([9][cout][cin]) weights.  cin in {16, 32, 64, 128, 256},
+// cout a multiple of 16 up to 256, leading dimensions and offsets multiples
+// of 8 channels, pointers 16-byte aligned.
+int sevp_nn_conv3x3_tc(const void *in, int in_ld, int in_off, int cin, const void *wk,
+                       const float *bias, void *out, int out_ld, int out_off, int cout, int B, int H,
+                       int W, int relu, void *stream) {
+  if (!in || !wk || !out || B < 1 || H < 1 || W < 1) return SEVP_BAD_ARG;
+  if (!(cin == 16 || cin == 32 || cin == 64 || cin == 128 || cin == 256)) return SEVP_BAD_ARG;
+  if (cout < 16 || cout > 256 || cout % 16) return SEVP_BAD_ARG;
+  if ((in_ld % 8) || (in_off % 8) || (out_ld % 8) || (out_off % 8) || in_off + cin > in_ld ||
+      out_off + cout > out_ld)
+    return SEVP_BAD_ARG;
+  if (!aligned16(in) || !aligned16(wk) || !aligned16(out)) return SEVP_BAD_ARG;
+  const int kc = cin < 64 ? cin : 64;
+  uint32_t cols = 32;
+  while (cols < (uint32_t)cout) cols <<= 1;
+  const size_t smem = (size_t)kTcStages * ((size_t)kTcM * kc * 2 + (size_t)cout * kc * 2);
+  static size_t set_smem = 0;
+  if (smem > set_smem) {
+    SEVP_CUDA_TRY(cudaFuncSetAttribute(k_conv3x3_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
+    set_smem = smem;
+  }
+  const long long P = (long long)B * H * W;
+  const unsigned grid = (unsigned)((P + kTcM - 1) / kTcM);
+  k_conv3x3_tc<<<grid, kTcThreads, smem, (cudaStream_t)stream>>>(
+      (const bf16 *)in, in_ld, in_off, cin, (const bf16 *)wk, bias, (bf16 *)out, out_ld, out_off,
+      cout, B, H, W, relu, kc, cols);
+  SEVP_CUDA_TRY(cudaGetLastError());
+  return SEVP_OK;
+}
+
+// First error a tensor-core kernel recorded since the last call (0 if none);
+// resets the flag.  Synchronises the device.
+int sevp_nn_tc_status(int *code) {
+  if (!code) return SEVP_BAD_ARG;
+  int v = 0, zero = 0;
+  SEVP_CUDA_TRY(cudaMemcpyFromSymbol(&v, g_tc_error, sizeof(int)));
+  SEVP_CUDA_TRY(cudaMemcpyToSymbol(g_tc_error, &zero, sizeof(int)));
+  *code = v;
+  return SEVP_OK;
+}
+
+}  // extern "C"

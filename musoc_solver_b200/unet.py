@@ -13,8 +13,9 @@ The network predicts a correction for the warm start of the barotropic solve
     head: conv1x1 32->1 (FP32)
 
 Every convolution is followed by ReLU.  Activations and weights are BF16
-(NHWC), products accumulate in FP32 on the tensor cores, the master weights
-and Adam state are FP32.  Every arithmetic step is a kernel of
+(NHWC), products accumulate in FP32 on the tensor cores (the forward
+convolutions on tcgen05 with the accumulator in tensor memory, the backward
+ones on warp-level MMA), the master weights and Adam state are FP32.  Every arithmetic step is a kernel of
 ``libsevp_b200.so``; PyTorch only allocates the buffers.
 """
 from __future__ import annotations
@@ -42,6 +43,10 @@ _SIGS = {
     "sevp_nn_conv3x3": ([C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                          C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
                          C.c_int, C.c_int, C.c_int, C.c_void_p], C.c_int),
+    "sevp_nn_conv3x3_tc": ([C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                            C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                            C.c_int, C.c_void_p], C.c_int),
+    "sevp_nn_tc_status": ([C.c_void_p], C.c_int),
     "sevp_nn_conv3x3_wgrad": ([C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int,
                                C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
                                C.c_int, C.c_int, C.c_int, C.c_void_p], C.c_int),
@@ -148,6 +153,9 @@ class UNet:
         A["y"] = torch.zeros(P[0], dtype=torch.float32, device=self.dev)
         self.A = A
         self.w16 = {n: torch.zeros((9, ci, co), dtype=bf, device=self.dev) for n, ci, co in CONVS}
+        # K-major ([9][co][ci]) copies: the tensor-core forward's B operand and
+        # the data gradient's transposed weights
+        self.wt16 = {n: torch.zeros((9, co, ci), dtype=bf, device=self.dev) for n, ci, co in CONVS}
         if self.train:
             G = {}
             for k in ("d0b", "d0a", "d1b", "d1a", "d2b", "d2a", "b1", "b0", "e2a", "e1a", "e0a"):
@@ -156,7 +164,6 @@ class UNet:
                 G[k] = torch.zeros_like(A[k])
             G["y"] = torch.zeros_like(A["y"])
             self.G = G
-            self.wt16 = {n: torch.zeros((9, co, ci), dtype=bf, device=self.dev) for n, ci, co in CONVS}
             self.gw = {n: [torch.zeros_like(v[0]), torch.zeros_like(v[1])] for n, v in self.params.items()}
             self.m = {n: [torch.zeros_like(v[0]), torch.zeros_like(v[1])] for n, v in self.params.items()}
             self.v = {n: [torch.zeros_like(v[0]), torch.zeros_like(v[1])] for n, v in self.params.items()}
@@ -172,21 +179,21 @@ class UNet:
         self.launches += 1
 
     def sync_weights(self):
-        """BF16 working copies (and transposes for the data gradient)."""
+        """BF16 working copies and their K-major transposes."""
         L = lib()
         for name, ci, co in CONVS:
             w = self.params[name][0]
             self._ck(L.sevp_nn_to_bf16(_p(w), _p(self.w16[name]), w.numel(), self.sp), "to_bf16")
-            if self.train:
-                self._ck(L.sevp_nn_weight_transpose(_p(self.w16[name]), _p(self.wt16[name]), ci, co,
-                                                    self.sp), "transpose")
+            self._ck(L.sevp_nn_weight_transpose(_p(self.w16[name]), _p(self.wt16[name]), ci, co,
+                                                self.sp), "transpose")
 
     def _conv(self, name, src, src_off, src_ld, dst, dst_off, dst_ld, lvl):
+        """Forward 3x3 conv + bias + ReLU on the tcgen05 tensor-core kernel."""
         _, ci, co = next(c for c in CONVS if c[0] == name)
         H, W = self.H >> lvl, self.W >> lvl
-        self._ck(lib().sevp_nn_conv3x3(_p(src), src_ld, src_off, ci, _p(self.w16[name]),
-                                       _p(self.params[name][1]), _p(dst), dst_ld, dst_off, co,
-                                       self.B, H, W, 1, None, 0, 0, 0, self.sp), name)
+        self._ck(lib().sevp_nn_conv3x3_tc(_p(src), src_ld, src_off, ci, _p(self.wt16[name]),
+                                          _p(self.params[name][1]), _p(dst), dst_ld, dst_off, co,
+                                          self.B, H, W, 1, self.sp), name)
 
     def forward(self):
         """x (features) -> y (FP32 correction).  Returns y."""

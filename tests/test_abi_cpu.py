@@ -11,9 +11,9 @@ from musoc_solver_b200.solver import default_sub_rows, tile_sub_blocks
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-def _declared():
+def _declared(headers=("sevp_b200.h", "sevp_nn.h")):
     names = []
-    for h in ("sevp_b200.h",):
+    for h in headers:
         txt = open(os.path.join(ROOT, "include", h)).read()
         txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
         txt = re.sub(r"typedef[^;]*;", "", txt, flags=re.S)
@@ -27,11 +27,14 @@ def test_library_builds_and_exports_header_symbols():
     assert os.path.exists(lib_path)
     L = native.lib()
     declared = _declared()
-    assert len(declared) >= 30
+    assert len(declared) >= 50
     missing = [n for n in declared if not hasattr(L, n)]
     assert not missing, missing
-    # the Python binding covers the same set
+    # the Python bindings cover the same set
+    from musoc_solver_b200 import unet
+
     assert set(native.exported_symbols()) <= set(declared) | {"sevp_bir_sweeps_", "sevp_pre_strips_"}
+    assert set(unet._SIGS) <= set(_declared(("sevp_nn.h",)))
 
 
 def test_status_strings():

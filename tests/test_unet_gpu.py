@@ -144,6 +144,68 @@ def test_conv_layer_forward_dgrad_wgrad(torch_cuda, cin, cout, H, W):
     assert (torch.norm(db.double().cpu() - dbr) / torch.norm(dbr)).item() < 1e-5
 
 
+@pytest.mark.parametrize("cin,cout,H,W,in_ld,in_off,out_ld,out_off",
+                         [(16, 32, 8, 16, 16, 0, 32, 0), (32, 32, 24, 40, 32, 0, 64, 32),
+                          (32, 64, 5, 31, 32, 0, 64, 0), (64, 64, 12, 20, 128, 64, 64, 0),
+                          (64, 128, 16, 8, 64, 0, 256, 128), (128, 256, 8, 8, 128, 0, 256, 0),
+                          (256, 256, 6, 10, 256, 0, 256, 0), (256, 128, 8, 8, 256, 0, 128, 0)])
+def test_conv_tcgen05_forward(torch_cuda, cin, cout, H, W, in_ld, in_off, out_ld, out_off):
+    """The tcgen05 forward conv (K-major weights, channel offsets of
+    concatenated buffers, ragged last tile) against torch FP64 on the same
+    BF16 values, and against the warp-MMA kernel; no timeout recorded."""
+    torch = torch_cuda
+    import ctypes as C
+
+    import torch.nn.functional as F
+
+    from musoc_solver_b200.unet import lib
+
+    L = lib()
+    rng = np.random.default_rng(cin * 7 + cout)
+    P = H * W
+    x = _bf(torch, rng.standard_normal((P, in_ld)))
+    w = _bf(torch, rng.normal(0, (2.0 / (9 * cin)) ** 0.5, (9, cin, cout)))
+    b = torch.from_numpy(rng.normal(0, 0.1, cout).astype(np.float32))
+    xd, wd, bd = x.cuda(), w.cuda(), b.cuda()
+    wk = wd.permute(0, 2, 1).contiguous()
+    y = torch.full((P, out_ld), 7.0, dtype=torch.bfloat16, device="cuda")
+    y2 = torch.zeros((P, cout), dtype=torch.bfloat16, device="cuda")
+    p = lambda t: C.c_void_p(t.data_ptr())
+    assert L.sevp_nn_conv3x3_tc(p(xd), in_ld, in_off, cin, p(wk), p(bd), p(y), out_ld, out_off, cout,
+                                1, H, W, 1, None) == 0
+    assert L.sevp_nn_conv3x3(p(xd), in_ld, in_off, cin, p(wd), p(bd), p(y2), cout, 0, cout, 1, H, W,
+                             1, None, 0, 0, 0, None) == 0
+    code = C.c_int(-1)
+    assert L.sevp_nn_tc_status(C.byref(code)) == 0 and code.value == 0
+    xr = x[:, in_off:in_off + cin].double().reshape(1, H, W, cin).permute(0, 3, 1, 2)
+    wr = w.double().reshape(3, 3, cin, cout).permute(3, 2, 0, 1)
+    yr = F.relu(F.conv2d(xr, wr, bias=b.double(), padding=1)).permute(0, 2, 3, 1).reshape(P, cout)
+    yg = y.double().cpu()
+    assert (torch.norm(yg[:, out_off:out_off + cout] - yr) / torch.norm(yr)).item() < 4e-3
+    # channels outside [out_off, out_off + cout) are untouched
+    rest = torch.cat([yg[:, :out_off], yg[:, out_off + cout:]], dim=1)
+    assert bool((rest == 7.0).all())
+    # same FP32 sums, rounded to BF16: at most one BF16 step apart
+    d = (yg[:, out_off:out_off + cout] - y2.double().cpu()).abs()
+    assert (d <= 2 ** -7 * yr.abs().clamp(min=1e-3) + 1e-6).all()
+
+
+def test_conv_tcgen05_rejects_bad_shapes(torch_cuda):
+    torch = torch_cuda
+    import ctypes as C
+
+    from musoc_solver_b200.unet import lib
+
+    L = lib()
+    t = torch.zeros(4096, dtype=torch.bfloat16, device="cuda")
+    f = torch.zeros(256, dtype=torch.float32, device="cuda")
+    p = lambda a: C.c_void_p(a.data_ptr())
+    # cin not in {16..256 powers of two}, cout above 256, misaligned offset
+    assert L.sevp_nn_conv3x3_tc(p(t), 48, 0, 48, p(t), p(f), p(t), 32, 0, 32, 1, 2, 2, 1, None) == 5
+    assert L.sevp_nn_conv3x3_tc(p(t), 16, 0, 16, p(t), p(f), p(t), 512, 0, 512, 1, 2, 2, 1, None) == 5
+    assert L.sevp_nn_conv3x3_tc(p(t), 32, 4, 16, p(t), p(f), p(t), 32, 0, 32, 1, 2, 2, 1, None) == 5
+
+
 def test_pool_upsample_exact(torch_cuda):
     torch = torch_cuda
     import ctypes as C
