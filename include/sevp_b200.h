@@ -198,6 +198,12 @@ int sevp_set_operator(sevp_ctx *ctx, const float *al, const float *ab, const flo
  * AT(i,j) = AB(i,j+1)); the kernels then read only AC, AR and AT. */
 int sevp_operator_symmetric(const sevp_ctx *ctx);
 /* force != 0: always read all five planes (call before sevp_set_operator). */
+/* CUDA graphs for the FP32 inner PCG iterations of mixed solves (default on):
+ * one check interval (check_every iterations of the two passes) is captured
+ * once per context on a private stream and replayed on the context stream.
+ * Not part of the reference interface. */
+int sevp_set_graphs(sevp_ctx *ctx, int enable);
+
 int sevp_set_full_coefficients(sevp_ctx *ctx, int force);
 /* Device bytes held by the tile influence data. */
 long long sevp_influence_bytes(const sevp_ctx *ctx);

@@ -855,6 +855,14 @@ struct sevp_ctx {
   unsigned *tickets = nullptr;
   long long launches = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // CUDA graph of a check interval of the FP32 inner PCG loop (captured on a
+  // private stream, replayed on the context stream); valid for the buffers
+  // and influence-data choice it was captured with
+  int use_graphs = 1;
+  cudaStream_t cap_stream = nullptr;
+  cudaGraphExec_t inner_graph = nullptr;
+  int inner_graph_ce = 0;
+  const void *inner_graph_key[3] = {nullptr, nullptr, nullptr};
   // optional per-kernel-class timing (CUDA events on the context stream)
   int prof = 0;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pool;
@@ -1072,6 +1080,8 @@ extern "C" int sevp_create(sevp_ctx **out, int nx, int ny, int periodic, void *s
 extern "C" int sevp_destroy(sevp_ctx *ctx) {
   if (!ctx) return SEVP_OK;
   cudaStreamSynchronize(ctx->stream);
+  if (ctx->inner_graph) cudaGraphExecDestroy(ctx->inner_graph);
+  if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
   free_work(ctx);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
@@ -1083,10 +1093,25 @@ extern "C" long long sevp_kernel_launches(const sevp_ctx *ctx) { return ctx ? ct
 
 extern "C" int sevp_operator_symmetric(const sevp_ctx *ctx) { return ctx ? ctx->sym : 0; }
 
+// Drops the captured inner-loop graph (the operator or buffers changed).
+static void drop_inner_graph(sevp_ctx *ctx) {
+  if (ctx->inner_graph) cudaGraphExecDestroy(ctx->inner_graph);
+  ctx->inner_graph = nullptr;
+  ctx->inner_graph_ce = 0;
+}
+
+extern "C" int sevp_set_graphs(sevp_ctx *ctx, int enable) {
+  if (!ctx) return SEVP_BAD_ARG;
+  ctx->use_graphs = enable ? 1 : 0;
+  if (!enable) drop_inner_graph(ctx);
+  return SEVP_OK;
+}
+
 extern "C" int sevp_set_full_coefficients(sevp_ctx *ctx, int force) {
   if (!ctx) return SEVP_BAD_ARG;
   ctx->force_full = force ? 1 : 0;
   if (force) ctx->sym = 0;
+  drop_inner_graph(ctx);
   return SEVP_OK;
 }
 
@@ -1105,6 +1130,7 @@ extern "C" long long sevp_influence_bytes(const sevp_ctx *ctx) {
 extern "C" int sevp_set_operator(sevp_ctx *ctx, const float *al, const float *ab, const float *ac,
                                  const float *ar, const float *at, const sevp_tiling *tl) {
   if (!ctx || !al || !ab || !ac || !ar || !at || !tl) return SEVP_BAD_ARG;
+  drop_inner_graph(ctx);
   const int tm = tl->tile_m, th = tl->tile_h;
   if (tm < 1 || tm > 32 || th < 1 || th > 32 || tl->sub_rows < 1) return SEVP_BAD_ARG;
   // the tile geometry needs ceil(nx/tm) etc. before the growth kernel runs
@@ -1280,8 +1306,7 @@ template <typename V>
 static int pcg_loop(sevp_ctx *ctx, V *x, V *r, V *z, V *p0, V *p1, V *q, int check_every,
                     int *iters_out) {
   V *pp[2] = {p0, p1};
-  int cur = 0;
-  for (;;) {
+  auto interval = [&](int &cur) -> int {  // check_every iterations of the two passes
     for (int k = 0; k < check_every; ++k) {
       OpPassA<V> op{z, pp[cur], pp[cur ^ 1], q, ctx->st};
       int s = launch_stencil(ctx, op, 3);
@@ -1289,6 +1314,54 @@ static int pcg_loop(sevp_ctx *ctx, V *x, V *r, V *z, V *p0, V *p1, V *q, int che
       s = launch_tile<V, true, true>(ctx, x, pp[cur ^ 1], r, q, z, 4);
       if (s) return s;
       cur ^= 1;
+    }
+    return SEVP_OK;
+  };
+  int cur = 0;
+  // FP32 inner loop: one graph replay per check interval (an even interval
+  // returns the p buffers to the same roles, so one capture serves all)
+  const bool graph = sizeof(V) == 4 && ctx->use_graphs && !ctx->prof && check_every % 2 == 0;
+  const void *key[3] = {(const void *)x, (const void *)p0,
+                        (const void *)(ctx->infl32_active ? ctx->d_mats32 : nullptr)};
+  if (graph && !(ctx->inner_graph && ctx->inner_graph_ce == check_every &&
+                 std::equal(key, key + 3, ctx->inner_graph_key))) {
+    drop_inner_graph(ctx);
+    if (!ctx->cap_stream)
+      SEVP_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking));
+    cudaStream_t run = ctx->stream;
+    const long long l0 = ctx->launches;
+    ctx->stream = ctx->cap_stream;
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(ctx->cap_stream, cudaStreamCaptureModeThreadLocal);
+    int s = SEVP_OK;
+    if (e == cudaSuccess) {
+      int c2 = 0;
+      s = interval(c2);
+      e = cudaStreamEndCapture(ctx->cap_stream, &g);
+    }
+    ctx->stream = run;
+    ctx->launches = l0;
+    if (s) {
+      if (g) cudaGraphDestroy(g);
+      return s;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&ctx->inner_graph, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+      ctx->inner_graph = nullptr;
+      sevp_internal_set_error(e, "capture of the inner PCG loop", __FILE__, __LINE__);
+      return SEVP_CUDA_ERROR;
+    }
+    ctx->inner_graph_ce = check_every;
+    std::copy(key, key + 3, ctx->inner_graph_key);
+  }
+  for (;;) {
+    if (graph) {
+      SEVP_CUDA_TRY(cudaGraphLaunch(ctx->inner_graph, ctx->stream));
+      ctx->launches += 2 * check_every;
+    } else {
+      int s = interval(cur);
+      if (s) return s;
     }
     int s = read_state(ctx);
     if (s) return s;

@@ -1,0 +1,72 @@
+"""Batched ensemble solves: all members in every kernel launch.
+
+The members (one grid size, each with its own coefficients and right-hand
+side) are stacked along y into one block-diagonal system
+(``problems.stack``); the tile height is chosen to divide a member's row
+count, so no tile crosses two members, and every pass of the PCG (stencil,
+tile SEVP) is one launch over all members.  The FP32 inner iterations of
+the mixed solve replay one CUDA graph per check interval.
+
+Stopping: the solver's test is on the stacked residual, so the tolerance
+handed to it is tightened by the smallest member's share of ||b||,
+  tol_stack = tol * min_k ||b_k|| / ||b||,
+which guarantees ||b_k - A_k x_k|| <= tol ||b_k|| for every member k; the
+per-member residuals are measured after the solve and reported.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import native as N
+from . import problems as P
+from .solver import SevpSolver
+
+
+def member_tile_height(ny: int, prefer=(16, 18, 20, 15, 24, 12, 10, 8)) -> int:
+    """A tile height that divides the member row count (tiles never straddle
+    two members), preferring heights near 16."""
+    for h in prefer:
+        if ny % h == 0:
+            return h
+    raise ValueError(f"no tile height in {prefer} divides {ny}")
+
+
+class EnsembleSolver:
+    def __init__(self, members, tile_m: int = 16, tile_h: int | None = None, growth_limit=1e10,
+                 device="cuda", stream=None):
+        import torch
+
+        self.torch = torch
+        self.members = list(members)
+        self.m = len(self.members)
+        self.ny, self.nx = self.members[0].ny, self.members[0].nx
+        self.problem = P.stack(self.members)
+        th = tile_h or member_tile_height(self.ny)
+        if self.ny % th:
+            raise ValueError("tile height must divide the member row count")
+        self.solver = SevpSolver(self.problem, tile_m=tile_m, tile_h=th, growth_limit=growth_limit,
+                                 device=device, stream=stream)
+        self.device = self.solver.device
+
+    def rhs(self):
+        """Stacked right-hand sides of the members, on the device."""
+        return self.torch.from_numpy(self.problem.b).to(self.device)
+
+    def member_norms(self, v):
+        return v.reshape(self.m, -1).norm(dim=1)
+
+    def solve(self, b, x=None, precision=1, tol=1e-12, max_iter=5000):
+        """Solves all members; returns (x, result, per-member relative
+        residuals as a host array)."""
+        bn = self.member_norms(b)
+        tol_stack = tol * float(bn.min() / b.norm()) if float(b.norm()) > 0 else tol
+        x, res = self.solver.solve(b, x=x, precision=precision, tol=tol_stack, max_iter=max_iter)
+        return x, res, self.member_residuals(b, x)
+
+    def member_residuals(self, b, x):
+        r = b - self.solver.apply(x)
+        bn = self.member_norms(b)
+        return (self.member_norms(r) / self.torch.where(bn > 0, bn, self.torch.ones_like(bn))).cpu().numpy()
+
+    def close(self):
+        self.solver.close()

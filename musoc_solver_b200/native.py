@@ -84,6 +84,7 @@ _SIGS = {
     "sevp_tile_layout": ([P, IP, IP, IP], C.c_int),
     "sevp_operator_symmetric": ([P], C.c_int),
     "sevp_set_full_coefficients": ([P, C.c_int], C.c_int),
+    "sevp_set_graphs": ([P, C.c_int], C.c_int),
     "sevp_inprod_noalloc": ([P, P, C.c_int, C.c_int, P, P], C.c_int),
     "sevp_profile": ([P, C.c_int], C.c_int),
     "sevp_set_warmstart": ([P, P, P, C.c_int], C.c_int),

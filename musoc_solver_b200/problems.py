@@ -264,6 +264,23 @@ def ensemble(members: int = 64, nx: int = 720, ny: int = 360, seed: int = 5,
     return out
 
 
+def stack(members) -> Problem:
+    """Members of one grid size stacked along y into one block-diagonal
+    problem.  Each member's north and south edge faces are closed (AT of its
+    last row and AB of its first row are zero), so no equation couples two
+    members; each row stays periodic in x with itself."""
+    ny, nx = members[0].ny, members[0].nx
+    for m in members:
+        if (m.ny, m.nx) != (ny, nx) or m.periodic != members[0].periodic:
+            raise ValueError("members must share grid size and periodicity")
+        if np.any(m.at[-1] != 0) or np.any(m.ab[0] != 0):
+            raise ValueError("member edges must be closed (AT of the last row, AB of the first)")
+    cat = lambda k: np.ascontiguousarray(np.concatenate([getattr(m, k) for m in members], axis=0))
+    return Problem(cat("al"), cat("ab"), cat("ac"), cat("ar"), cat("at"), cat("b"),
+                   periodic=members[0].periodic, name=f"stack{len(members)}x{nx}x{ny}",
+                   meta=dict(members=len(members), member_ny=ny))
+
+
 def idealised(i2: int = 180, j2: int = 90) -> Problem:
     """The reference's test stencil (``P/prep_GLOBAL.f90:246-261``):
     AL=AB=AR=AT=-0.25, AC=1, Neumann rows on the north and south edges,

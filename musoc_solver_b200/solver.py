@@ -177,6 +177,10 @@ class SevpSolver:
         return N.SolveOpts(int(precision), float(tol), int(max_iter), float(inner_tol),
                            int(use_guess), int(check_every), int(precond_fp32))
 
+    def graphs(self, enable: bool = True):
+        """CUDA-graph replay of the FP32 inner iterations (default on)."""
+        N.check(N.lib().sevp_set_graphs(self.h, int(bool(enable))), "sevp_set_graphs")
+
     @property
     def symmetric(self) -> bool:
         return bool(N.lib().sevp_operator_symmetric(self.h))
