@@ -111,9 +111,6 @@ constexpr int kStencilCols = 30;  // output columns per warp (32 loaded)
 #ifndef SEVP_TILE_MINB
 #define SEVP_TILE_MINB 3
 #endif
-#ifndef SEVP_STENCIL_RPW
-#define SEVP_STENCIL_RPW 16
-#endif
 
 // SYM: the operator is symmetric (AL(i,j) = AR(i-1,j), AB(i,j) = AT(i,j-1)),
 // so only AC, AR and AT are read; AL comes from the west lane's AR and AB
@@ -449,9 +446,11 @@ __global__ void __launch_bounds__(kTileWarps * 32, SEVP_TILE_MINB)
   double *dv = rho_s + (size_t)tg.hmax * 32;         // [32]
 
   double acc_rz = 0.0, acc_rr = 0.0;
-  const int gw = blockIdx.x * kTileWarps + wib;
-  const int b = gw / tg.txg;
-  if (b < tg.ty) {
+  // warps loop over the tile tasks with a grid-wide stride, so the grid can
+  // be capped at the resident CTAs (no partial last wave)
+  const int ntasks = tg.ty * tg.txg;
+  for (int gw = blockIdx.x * kTileWarps + wib; gw < ntasks; gw += gridDim.x * kTileWarps) {
+    const int b = gw / tg.txg;
     const int grp = gw - b * tg.txg;
     const int seg = lane / tg.wseg, n = lane - seg * tg.wseg, segbase = seg * tg.wseg;
     const int a = grp * tg.tpw + seg;
@@ -859,6 +858,7 @@ struct sevp_ctx {
   // private stream, replayed on the context stream); valid for the buffers
   // and influence-data choice it was captured with
   int use_graphs = 1;
+  int stencil_rpw = 0;  // rows per CTA of the stencil kernels (0: not chosen yet)
   cudaStream_t cap_stream = nullptr;
   cudaGraphExec_t inner_graph = nullptr;
   int inner_graph_ce = 0;
@@ -920,7 +920,26 @@ extern "C" const char *sevp_status_string(int s) {
   }
 }
 
-static int stencil_rpw(int ny) { return ny >= 1024 ? SEVP_STENCIL_RPW : 8; }
+// Rows per CTA of the stencil kernels, chosen once per context: a CTA loads
+// rpw + 2 rows, and the grid runs in ceil(CTAs / slots) waves, so pick the
+// rpw in [8, 32] that minimises waves x (rpw + 2) (ties: more rows).
+static int stencil_rpw(sevp_ctx *ctx) {
+  if (ctx->stencil_rpw > 0) return ctx->stencil_rpw;
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess)
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long long slots = (long long)sms * SEVP_STENCIL_MINB;
+  const long long gx = ceil_div(ceil_div(ctx->nx, kStencilCols), kStencilThreads / 32);
+  int best = 8;
+  long long best_cost = -1;
+  for (int rpw = 8; rpw <= 32; ++rpw) {
+    const long long ctas = gx * ceil_div(ctx->ny, rpw);
+    const long long cost = ((ctas + slots - 1) / slots) * (rpw + 2);
+    if (best_cost < 0 || cost <= best_cost) best = rpw, best_cost = cost;
+  }
+  ctx->stencil_rpw = std::max(1, std::min(best, ctx->ny));
+  return ctx->stencil_rpw;
+}
 
 static dim3 stencil_grid(const sevp_ctx *ctx, int rpw) {
   const int groups = ceil_div(ctx->nx, kStencilCols);
@@ -931,7 +950,7 @@ static size_t tile_warps(const TileGeom &tg) { return (size_t)tg.ty * tg.txg; }
 
 template <class Op>
 static int launch_stencil(sevp_ctx *ctx, const Op &op, int ticket_slot) {
-  int rpw = stencil_rpw(ctx->ny);
+  int rpw = stencil_rpw(ctx);
   dim3 grid = stencil_grid(ctx, rpw);
   GridDims gd{ctx->nx, ctx->ny, ctx->periodic};
   ProfScope ps(ctx, 1);
@@ -950,14 +969,22 @@ template <typename V, typename MT, bool UPDATE, bool DOTS, bool SYM>
 static int launch_tile_k(sevp_ctx *ctx, const MT *mats, V *x, const V *p, V *r, const V *q, V *z,
                          int ticket_slot) {
   const size_t warps = tile_warps(ctx->tg);
-  const unsigned blocks = (unsigned)((warps + kTileWarps - 1) / kTileWarps);
   const size_t smem = tile_smem_per_warp(ctx->tg.hmax) * kTileWarps;
   auto kern = k_tile_apply<V, MT, UPDATE, DOTS, SYM>;
   static size_t set_smem = 0;  // per instantiation (one device per process is assumed)
-  if (smem > 48 * 1024 && set_smem < smem) {
-    SEVP_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  static int slots = 0;         // resident CTAs on the device at set_smem
+  if (set_smem != smem) {
+    if (smem > 48 * 1024)
+      SEVP_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0, dev = 0, sms = 0;
+    SEVP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTileWarps * 32, smem));
+    SEVP_CUDA_TRY(cudaGetDevice(&dev));
+    SEVP_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    slots = std::max(1, per_sm) * sms;
     set_smem = smem;
   }
+  const unsigned blocks =
+      (unsigned)std::min<size_t>((warps + kTileWarps - 1) / kTileWarps, (size_t)slots);
   ProfScope ps(ctx, UPDATE ? 0 : 2);
   kern<<<blocks, kTileWarps * 32, smem, ctx->stream>>>(ctx->tg, ctx->c, mats, x, p, r, q, z, ctx->st,
                                                       ctx->partials, ctx->tickets + ticket_slot);
