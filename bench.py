@@ -53,7 +53,9 @@ sys.path.insert(0, ROOT)
 
 METRIC = "solves/s to 1e-12 rel. residual at 3600x2400: learned+mixed vs plain FP64 SEVP"
 NX, NY = 3600, 2400
-TILE_M, TILE_H, GROWTH = 16, 16, 1e10
+# tile shape of the CPU oracle arms; the GPU arm autotunes its own (16x8 is
+# what the autotuner picks on a B200 at 3600x2400)
+TILE_M, TILE_H, GROWTH = 16, 8, 1e10
 
 
 def parse():
@@ -73,6 +75,8 @@ def parse():
     ap.add_argument("--epochs", type=int, default=3)
     ap.add_argument("--coarse", type=int, default=4, choices=[1, 2, 4],
                     help="the network runs on the grid averaged over coarse x coarse cells")
+    ap.add_argument("--tiles", default="auto",
+                    help="tile shape MxH of the GPU solver, or 'auto' (measured at start-up)")
     ap.add_argument("--no-ensemble", action="store_true",
                     help="skip the 64-member 720x360 ensemble arm")
     ap.add_argument("--no-learned", action="store_true",
@@ -184,7 +188,7 @@ def dist_setup(args):
 
 
 # ------------------------------------------------------------ CPU oracle
-def cpu_solve_seconds(p, b, threads, tile_nb=None):
+def cpu_solve_seconds(p, b, threads, tile_nb=None, tiles=(TILE_M, TILE_H)):
     """One FP64 tile-SEVP PCG solve with the CPU oracle (setup excluded),
     with the same tile layout as the GPU solver."""
     os.environ["OMP_NUM_THREADS"] = str(threads)
@@ -193,8 +197,8 @@ def cpu_solve_seconds(p, b, threads, tile_nb=None):
     from musoc_solver_b200.solver import tile_sub_blocks
 
     if tile_nb is None:
-        tile_nb = tile_sub_blocks(p, TILE_M, TILE_H, GROWTH)
-    pc = O.TilePC(p, TILE_M, TILE_H, tile_nb=tile_nb)
+        tile_nb = tile_sub_blocks(p, tiles[0], tiles[1], GROWTH)
+    pc = O.TilePC(p, tiles[0], tiles[1], tile_nb=tile_nb)
     t = time.perf_counter()
     x, it, rel = pc.pcg(b, tol=1e-12)
     dt = time.perf_counter() - t
@@ -221,7 +225,7 @@ def run_reference(args, world, rank):
         "ms_per_step": 1e3 * total / len(times), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"{args.nx}x{args.ny} global grid, eddy right-hand-side sequence, "
-                               "FP64 tile-SEVP PCG (16x16 tiles) to 1e-12, zero guess",
+                               f"FP64 tile-SEVP PCG ({TILE_M}x{TILE_H} tiles) to 1e-12, zero guess",
                    "grid": [args.nx, args.ny], "tol": 1e-12, "l2": "inputs larger than L2"},
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "port",
                          "sample": "one full FP64 tile-SEVP PCG solve per step with the C oracle "
@@ -251,7 +255,7 @@ def run_ensemble(K, W, members=64, nx=720, ny=360):
     stream = e.solver.stream
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     out = {"workload": f"{members} members x {nx}x{ny}, +-5% depth noise, own right-hand sides, "
-                       f"stacked ({e.problem.nx}x{e.problem.ny}), tiles 16x{e.solver.tile_h}",
+                       f"stacked ({e.problem.nx}x{e.problem.ny}), tiles {e.solver.tile_m}x{e.solver.tile_h}",
            "setup_seconds": setup_s}
     for name, prec in (("mixed", 1), ("fp64", 0)):
         x = torch.zeros_like(b)
@@ -295,7 +299,17 @@ def run_native(args, world, rank, local, dist):
     nsteps = T + W + K
     p, rhs = make_sequence(args.nx, args.ny, nsteps)
     n = p.nx * p.ny
-    solver = SevpSolver(p, tile_m=TILE_M, tile_h=TILE_H, growth_limit=GROWTH,
+    # tile shape: measured on the first right-hand side (untimed)
+    tune_table = None
+    if args.tiles == "auto":
+        from musoc_solver_b200.autotune import autotune
+
+        best, tune_table = autotune(p, torch.from_numpy(rhs[0]).to(dev), precision=1,
+                                    growth_limit=GROWTH)
+        tiles = (best["tile_m"], best["tile_h"])
+    else:
+        tiles = tuple(int(v) for v in args.tiles.lower().split("x"))
+    solver = SevpSolver(p, tile_m=tiles[0], tile_h=tiles[1], growth_limit=GROWTH,
                         precond_fp32=args.precond_fp32)
     stream = solver.stream
     b_dev = [torch.from_numpy(b).to(dev) for b in rhs]
@@ -446,7 +460,7 @@ def run_native(args, world, rank, local, dist):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cores = os.cpu_count() or 1
-        dt, itc, relc = cpu_solve_seconds(p, rhs[timed[0]], cores, solver.tile_nb)
+        dt, itc, relc = cpu_solve_seconds(p, rhs[timed[0]], cores, solver.tile_nb, tiles)
         cpu = {"value": 1.0 / dt, "unit": "solves/s", "cores": cores, "kind": "port",
                "sample": f"one full FP64 tile-SEVP PCG solve of step {timed[0]} with the C oracle "
                          f"(OpenMP, {cores} threads, {itc} iterations, rel. residual {relc:.2e}), "
@@ -470,7 +484,10 @@ def run_native(args, world, rank, local, dist):
             "workload": f"{p.nx}x{p.ny} global grid (lat +-78, ~30% land, dt=60 s), eddy "
                         "right-hand-side sequence; mixed FP32 tile-SEVP PCG + FP64 iterative "
                         f"refinement to 1e-12 from warm start: {guess_name}",
-            "grid": [p.nx, p.ny], "tiles": [TILE_M, TILE_H], "marching_growth_limit": GROWTH,
+            "grid": [p.nx, p.ny], "tiles": list(tiles),
+            "tile_autotune": None if tune_table is None else
+            {f"{r['tile_m']}x{r['tile_h']}": round(r["ms"], 2) for r in tune_table},
+            "marching_growth_limit": GROWTH,
             "coefficient_planes": 3 if solver.symmetric else 5,
             "influence_fp32_in_inner_solve": bool(args.precond_fp32),
             "tol": 1e-12, "parallelism": f"replicas x{world}",

@@ -31,5 +31,6 @@ def test_members_differ_and_stack_rejects_open_edges():
 def test_member_tile_height_divides_rows():
     for ny in (24, 48, 360, 180, 90):
         h = member_tile_height(ny)
-        assert ny % h == 0 and 8 <= h <= 24
-    assert member_tile_height(360) == 18
+        assert ny % h == 0 and 6 <= h <= 24
+    assert member_tile_height(360) == 8
+    assert member_tile_height(45) == 15
