@@ -42,6 +42,14 @@ int sevp_nn_conv3x3_tc(const void *in, int in_ld, int in_off, int cin, const voi
                        const float *bias, void *out, int out_ld, int out_off, int cout, int B,
                        int H, int W, int relu, void *stream);
 
+/* The same forward convolution with both operands loaded by TMA (tensor-map
+ * loads with hardware zero fill at the image edges, 128-byte swizzle) and a
+ * warp-specialised producer / MMA issuer; tiles are 128 pixels of one image
+ * row.  cin in {16, 32, 64, 128, 192, 256}, other limits as above. */
+int sevp_nn_conv3x3_tma(const void *in, int in_ld, int in_off, int cin, const void *wk,
+                        const float *bias, void *out, int out_ld, int out_off, int cout, int B,
+                        int H, int W, int relu, void *stream);
+
 /* First error code (SEVP_TIMEOUT) a tensor-core kernel recorded since the
  * last call, 0 if none; clears it.  Synchronises the device. */
 int sevp_nn_tc_status(int *code);

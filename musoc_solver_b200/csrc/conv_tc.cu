@@ -19,8 +19,11 @@
 // Every wait on an mbarrier is bounded: on timeout the kernel records
 // SEVP_TIMEOUT in a device flag (read by sevp_nn_tc_status), skips its
 // stores, drains its copies, frees its TMEM and returns.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 #include <cstdint>
+#include <mutex>
 
 #include "common.cuh"
 
@@ -249,7 +252,235 @@ __global__ void __launch_bounds__(kTcThreads)
   if (failed) atomicCAS(&g_tc_error, 0, SEVP_TIMEOUT);
 }
 
+
+// ------------------------------------------------ TMA-fed variant (cin % 64 == 0)
+// The same implicit GEMM with the operands brought in by the tensor memory
+// accelerator: per step one 4-D tensor-map load of the tap-shifted A tile
+// (64 channels x 128 pixels of one image row; the unit zero-fills outside the
+// image, including negative coordinates) and one 2-D load of the tap's
+// K-major weights (64 channels x cout), both in the 128-byte swizzle that the
+// MMA's K-major SWIZZLE_128B descriptor reads (rows of 128 B, 8-row atoms
+// 1024 B apart, a K step of 16 advances the start address by 32 B).  Warp 0
+// lane 0 produces (TMA, full barriers with the byte count), warp 1 lane 0
+// issues the MMAs and releases stages (empty barriers), all four warps run
+// the epilogue.  The tiles are 128 consecutive pixels of one image row.
+constexpr int kTmStages = 4;
+
+// K-major swizzled descriptor for rows of KC BF16 (KC * 2 bytes = the
+// swizzle width): 8-row atoms are 8 * KC * 2 bytes apart; layout type 2,
+// 4, 6 = 128-, 64-, 32-byte swizzle.
+template <int KC>
+__device__ __forceinline__ uint64_t smem_desc_sw(uint32_t addr) {
+  constexpr uint64_t layout = KC == 64 ? 2 : (KC == 32 ? 4 : 6);
+  uint64_t d = 0;
+  d |= (uint64_t)((addr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((8u * KC * 2u) >> 4) << 32;  // stride byte offset: next 8 rows
+  d |= (uint64_t)1 << 46;                      // descriptor version of sm_100
+  d |= layout << 61;
+  return d;
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap *map, int c0, int c1,
+                                            int c2, int c3, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5}], [%6];\n" ::"r"(dst),
+      "l"((uint64_t)map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(bar)
+      : "memory");
+}
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int c0, int c1,
+                                            uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];\n" ::"r"(dst),
+      "l"((uint64_t)map), "r"(c0), "r"(c1), "r"(bar)
+      : "memory");
+}
+
+template <int KC>
+__global__ void __launch_bounds__(kTcThreads)
+    k_conv3x3_tma(const __grid_constant__ CUtensorMap tm_in, const __grid_constant__ CUtensorMap tm_w,
+                  const float *__restrict__ bias, bf16 *__restrict__ out, int out_ld, int out_off,
+                  int cin, int cout, int H, int W, int relu, uint32_t tmem_cols) {
+  extern __shared__ __align__(1024) unsigned char sm_raw[];
+  __shared__ __align__(8) uint64_t full[kTmStages], empty[kTmStages], done;
+  __shared__ uint32_t s_tmem;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int x0 = blockIdx.x * kTcM, y = blockIdx.y, img = blockIdx.z;
+  const uint32_t raw = smem_u32(sm_raw);
+  const uint32_t sbase = (raw + 1023u) & ~1023u;  // 1024-byte aligned stages
+  const uint32_t a_bytes = (uint32_t)kTcM * KC * 2, b_bytes = (uint32_t)cout * KC * 2;
+  const uint32_t tx_bytes = a_bytes + b_bytes;
+  const uint32_t stage_bytes = (tx_bytes + 1023u) & ~1023u;  // stages 1024-byte aligned
+  const int nkc = cin / KC, T = 9 * nkc;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                     smem_u32(&s_tmem)),
+                 "r"(tmem_cols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+  }
+  if (tid == 0) {
+    for (int s = 0; s < kTmStages; ++s) {
+      mbar_init(smem_u32(&full[s]), 1);
+      mbar_init(smem_u32(&empty[s]), 1);
+    }
+    mbar_init(smem_u32(&done), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = s_tmem;
+
+  bool failed = false;
+  int issued = 0;
+  if (warp == 0 && lane == 0) {  // producer
+    for (int s = 0; s < T; ++s) {
+      const int st = s % kTmStages;
+      if (s >= kTmStages &&
+          !mbar_wait(smem_u32(&empty[st]), (unsigned)((s / kTmStages) - 1) & 1u)) {
+        failed = true;
+        break;
+      }
+      const int tap = s / nkc, c0 = (s - tap * nkc) * KC;
+      const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+      const uint32_t a_s = sbase + st * stage_bytes, bar = smem_u32(&full[st]);
+      mbar_expect_tx(bar, tx_bytes);
+      tma_load_4d(a_s, &tm_in, c0, x0 + dx, y + dy, img, bar);
+      tma_load_2d(a_s + a_bytes, &tm_w, c0, tap * cout, bar);
+      issued = s + 1;
+    }
+  } else if (warp == 1 && lane == 0) {  // MMA issuer
+    const uint32_t idesc = instr_desc_bf16(kTcM, cout);
+    for (int s = 0; s < T; ++s) {
+      const int st = s % kTmStages;
+      if (!mbar_wait(smem_u32(&full[st]), (unsigned)(s / kTmStages) & 1u)) {
+        failed = true;
+        break;
+      }
+      tc_fence_after();
+      const uint32_t a_s = sbase + st * stage_bytes, b_s = a_s + a_bytes;
+#pragma unroll
+      for (int k16 = 0; k16 < KC / 16; ++k16)
+        tc_mma(tmem, smem_desc_sw<KC>(a_s + k16 * 32), smem_desc_sw<KC>(b_s + k16 * 32), idesc,
+               (s > 0 || k16 > 0) ? 1u : 0u);
+      tc_commit(smem_u32(&empty[st]));
+    }
+    if (!failed) tc_commit(smem_u32(&done));  // arrives once every MMA has completed
+  }
+  __syncwarp();
+  if (!mbar_wait(smem_u32(&done), 0u)) failed = true;
+  failed = __syncthreads_or(failed) != 0;
+  if (failed && warp == 0 && lane == 0) {
+    // drain the loads that may still be in flight (bounded) before the
+    // shared memory they target is released
+    for (int s = issued - kTmStages < 0 ? 0 : issued - kTmStages; s < issued; ++s)
+      mbar_wait(smem_u32(&full[s % kTmStages]), (unsigned)(s / kTmStages) & 1u);
+  }
+  tc_fence_after();
+  const int x = x0 + warp * 32 + lane;
+  const uint32_t tl = tmem + ((uint32_t)(warp * 32) << 16);
+  bf16 *dst_row = out + (((long long)img * H + y) * W + x) * out_ld + out_off;
+  for (int n0 = 0; n0 < cout; n0 += 16) {
+    uint32_t v[16];
+    tmem_ld16(tl + (uint32_t)n0, v);
+    if (x < W && !failed) {
+      __align__(16) bf16 o[16];
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        float f = __uint_as_float(v[q]);
+        if (bias) f += bias[n0 + q];
+        if (relu) f = fmaxf(f, 0.f);
+        o[q] = __float2bfloat16(f);
+      }
+      uint4 *d = reinterpret_cast<uint4 *>(dst_row + n0);
+      d[0] = *reinterpret_cast<const uint4 *>(&o[0]);
+      d[1] = *reinterpret_cast<const uint4 *>(&o[8]);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(tmem_cols)
+                 : "memory");
+  if (failed) atomicCAS(&g_tc_error, 0, SEVP_TIMEOUT);
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)f;
+  });
+  return fn;
+}
+
 bool aligned16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
+
+}  // namespace
+
+namespace {
+
+// The TMA-fed forward convolution: same arguments and result as
+// sevp_nn_conv3x3_tc.  Steps of 64 input channels (128-byte swizzle), or of
+// cin = 32 / 16 channels (64- / 32-byte swizzle).
+template <int KC>
+int launch_conv_tma(const void *in, int in_ld, int in_off, int cin, const void *wk,
+                           const float *bias, void *out, int out_ld, int out_off, int cout, int B,
+                           int H, int W, int relu, void *stream,
+                           PFN_cuTensorMapEncodeTiled_v12000 enc) {
+  const CUtensorMapSwizzle sw = KC == 64 ? CU_TENSOR_MAP_SWIZZLE_128B
+                                         : (KC == 32 ? CU_TENSOR_MAP_SWIZZLE_64B
+                                                     : CU_TENSOR_MAP_SWIZZLE_32B);
+  CUtensorMap tm_in, tm_w;
+  {
+    // activations: (channel, x, y, image), KC channels x 128 pixels per box
+    const cuuint64_t dims[4] = {(cuuint64_t)cin, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)B};
+    const cuuint64_t strides[3] = {(cuuint64_t)in_ld * 2, (cuuint64_t)W * in_ld * 2,
+                                   (cuuint64_t)H * W * in_ld * 2};
+    const cuuint32_t box[4] = {(cuuint32_t)KC, (cuuint32_t)kTcM, 1, 1};
+    const cuuint32_t es[4] = {1, 1, 1, 1};
+    if (enc(&tm_in, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, (void *)((const bf16 *)in + in_off), dims,
+            strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return SEVP_BAD_ARG;
+  }
+  {
+    // K-major weights (channel, tap * cout + n), KC channels x cout per box
+    const cuuint64_t dims[2] = {(cuuint64_t)cin, (cuuint64_t)9 * cout};
+    const cuuint64_t strides[1] = {(cuuint64_t)cin * 2};
+    const cuuint32_t box[2] = {(cuuint32_t)KC, (cuuint32_t)cout};
+    const cuuint32_t es[2] = {1, 1};
+    if (enc(&tm_w, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(wk), dims, strides, box, es,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return SEVP_BAD_ARG;
+  }
+  uint32_t cols = 32;
+  while (cols < (uint32_t)cout) cols <<= 1;
+  const size_t stage = ((size_t)kTcM * KC * 2 + (size_t)cout * KC * 2 + 1023) & ~(size_t)1023;
+  const size_t smem = (size_t)kTmStages * stage + 1024;
+  static size_t set_smem = 0;
+  if (smem > set_smem) {
+    SEVP_CUDA_TRY(cudaFuncSetAttribute(k_conv3x3_tma<KC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
+    set_smem = smem;
+  }
+  dim3 grid((unsigned)((W + kTcM - 1) / kTcM), (unsigned)H, (unsigned)B);
+  k_conv3x3_tma<KC><<<grid, kTcThreads, smem, (cudaStream_t)stream>>>(
+      tm_in, tm_w, bias, (bf16 *)out, out_ld, out_off, cin, cout, H, W, relu, cols);
+  SEVP_CUDA_TRY(cudaGetLastError());
+  return SEVP_OK;
+}
 
 }  // namespace
 
@@ -286,6 +517,29 @@ int sevp_nn_conv3x3_tc(const void *in, int in_ld, int in_off, int cin, const voi
       cout, B, H, W, relu, kc, cols);
   SEVP_CUDA_TRY(cudaGetLastError());
   return SEVP_OK;
+}
+
+int sevp_nn_conv3x3_tma(const void *in, int in_ld, int in_off, int cin, const void *wk,
+                        const float *bias, void *out, int out_ld, int out_off, int cout, int B, int H,
+                        int W, int relu, void *stream) {
+  if (!in || !wk || !out || B < 1 || H < 1 || W < 1) return SEVP_BAD_ARG;
+  if (!(cin == 16 || cin == 32 || cin == 64 || cin == 128 || cin == 192 || cin == 256))
+    return SEVP_BAD_ARG;
+  if (cout < 16 || cout > 256 || cout % 16) return SEVP_BAD_ARG;
+  if ((in_ld % 8) || (in_off % 8) || (out_ld % 8) || (out_off % 8) || in_off + cin > in_ld ||
+      out_off + cout > out_ld)
+    return SEVP_BAD_ARG;
+  if (!aligned16(in) || !aligned16(wk) || !aligned16(out)) return SEVP_BAD_ARG;
+  auto enc = tensor_map_encoder();
+  if (!enc) return SEVP_CUDA_ERROR;
+  if (cin == 16)
+    return launch_conv_tma<16>(in, in_ld, in_off, cin, wk, bias, out, out_ld, out_off, cout, B, H, W,
+                               relu, stream, enc);
+  if (cin == 32)
+    return launch_conv_tma<32>(in, in_ld, in_off, cin, wk, bias, out, out_ld, out_off, cout, B, H, W,
+                               relu, stream, enc);
+  return launch_conv_tma<64>(in, in_ld, in_off, cin, wk, bias, out, out_ld, out_off, cout, B, H, W,
+                             relu, stream, enc);
 }
 
 // First error a tensor-core kernel recorded since the last call (0 if none);

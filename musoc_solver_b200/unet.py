@@ -46,6 +46,9 @@ _SIGS = {
     "sevp_nn_conv3x3_tc": ([C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
                             C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                             C.c_int, C.c_void_p], C.c_int),
+    "sevp_nn_conv3x3_tma": ([C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                             C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                             C.c_int, C.c_void_p], C.c_int),
     "sevp_nn_tc_status": ([C.c_void_p], C.c_int),
     "sevp_nn_conv3x3_wgrad": ([C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int,
                                C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
@@ -188,10 +191,11 @@ class UNet:
                                                 self.sp), "transpose")
 
     def _conv(self, name, src, src_off, src_ld, dst, dst_off, dst_ld, lvl):
-        """Forward 3x3 conv + bias + ReLU on the tcgen05 tensor-core kernel."""
+        """Forward 3x3 conv + bias + ReLU on the tcgen05 tensor cores, operands
+        loaded by TMA."""
         _, ci, co = next(c for c in CONVS if c[0] == name)
         H, W = self.H >> lvl, self.W >> lvl
-        self._ck(lib().sevp_nn_conv3x3_tc(_p(src), src_ld, src_off, ci, _p(self.wt16[name]),
+        self._ck(lib().sevp_nn_conv3x3_tma(_p(src), src_ld, src_off, ci, _p(self.wt16[name]),
                                           _p(self.params[name][1]), _p(dst), dst_ld, dst_off, co,
                                           self.B, H, W, 1, self.sp), name)
 

@@ -190,6 +190,50 @@ def test_conv_tcgen05_forward(torch_cuda, cin, cout, H, W, in_ld, in_off, out_ld
     assert (d <= 2 ** -7 * yr.abs().clamp(min=1e-3) + 1e-6).all()
 
 
+@pytest.mark.parametrize("cin,cout,B,H,W,in_ld,in_off,out_ld,out_off",
+                         [(16, 32, 1, 7, 200, 16, 0, 32, 0), (32, 32, 2, 5, 129, 64, 32, 64, 0),
+                          (32, 64, 1, 4, 100, 32, 0, 128, 64),
+                          (64, 32, 1, 9, 150, 64, 0, 64, 32), (64, 64, 2, 5, 40, 128, 64, 64, 0),
+                          (128, 64, 1, 6, 256, 128, 0, 128, 64), (256, 128, 1, 4, 130, 256, 0, 128, 0),
+                          (128, 256, 1, 3, 20, 128, 0, 256, 0), (256, 256, 1, 2, 300, 256, 0, 256, 0)])
+def test_conv_tma_forward(torch_cuda, cin, cout, B, H, W, in_ld, in_off, out_ld, out_off):
+    """The TMA-fed tcgen05 conv (row tiles, ragged row ends, rows shorter than
+    a tile, two images, channel offsets) equals the cp.async tcgen05 conv
+    (the same MMA order) and matches torch FP64 on the same BF16 values."""
+    torch = torch_cuda
+    import ctypes as C
+
+    import torch.nn.functional as F
+
+    from musoc_solver_b200.unet import lib
+
+    L = lib()
+    rng = np.random.default_rng(cin * 13 + cout + W)
+    P = B * H * W
+    x = _bf(torch, rng.standard_normal((P, in_ld)))
+    w = _bf(torch, rng.normal(0, (2.0 / (9 * cin)) ** 0.5, (9, cin, cout)))
+    b = torch.from_numpy(rng.normal(0, 0.1, cout).astype(np.float32))
+    xd, bd = x.cuda(), b.cuda()
+    wk = w.cuda().permute(0, 2, 1).contiguous()
+    y1 = torch.full((P, out_ld), 5.0, dtype=torch.bfloat16, device="cuda")
+    y2 = torch.full((P, out_ld), 5.0, dtype=torch.bfloat16, device="cuda")
+    p = lambda t: C.c_void_p(t.data_ptr())
+    assert L.sevp_nn_conv3x3_tma(p(xd), in_ld, in_off, cin, p(wk), p(bd), p(y1), out_ld, out_off, cout,
+                                 B, H, W, 1, None) == 0
+    assert L.sevp_nn_conv3x3_tc(p(xd), in_ld, in_off, cin, p(wk), p(bd), p(y2), out_ld, out_off, cout,
+                                B, H, W, 1, None) == 0
+    code = C.c_int(-1)
+    assert L.sevp_nn_tc_status(C.byref(code)) == 0 and code.value == 0
+    assert torch.equal(y1, y2)
+    xr = x[:, in_off:in_off + cin].double().reshape(B, H, W, cin).permute(0, 3, 1, 2)
+    wr = w.double().reshape(3, 3, cin, cout).permute(3, 2, 0, 1)
+    yr = F.relu(F.conv2d(xr, wr, bias=b.double(), padding=1)).permute(0, 2, 3, 1).reshape(P, cout)
+    yg = y1.double().cpu()
+    assert (torch.norm(yg[:, out_off:out_off + cout] - yr) / torch.norm(yr)).item() < 4e-3
+    rest = torch.cat([yg[:, :out_off], yg[:, out_off + cout:]], dim=1)
+    assert bool((rest == 5.0).all())
+
+
 def test_conv_tcgen05_rejects_bad_shapes(torch_cuda):
     torch = torch_cuda
     import ctypes as C
