@@ -309,6 +309,76 @@ __global__ void k_head_fwd(const bf16 *x, int x_ld, int x_off, int C, const floa
     y[p] = s;
   }
 }
+// 8-channel (16-byte) versions of the forward pooling, upsampling and head,
+// used when channel counts, leading dimensions and offsets are multiples of
+// 8: the same arithmetic in the same order as the one-element kernels.
+__device__ __forceinline__ void bf8_to_f(const uint4 &v, float (&f)[8]) {
+  const bf16 *h = reinterpret_cast<const bf16 *>(&v);
+#pragma unroll
+  for (int q = 0; q < 8; ++q) f[q] = __bfloat162float(h[q]);
+}
+__global__ void k_pool_fwd8(const bf16 *in, int in_ld, int in_off, bf16 *out, int out_ld,
+                            int out_off, int C8, int B, int H, int W) {
+  const int Ho = H / 2, Wo = W / 2;
+  const long long n = (long long)B * Ho * Wo * C8;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(e % C8) * 8;
+    const long long q = e / C8;
+    const int x = (int)(q % Wo);
+    const long long t = q / Wo;
+    const int y = (int)(t % Ho);
+    const long long b = t / Ho;
+    const long long p = (b * H + 2 * y) * W + 2 * x;
+    float a[8], b1[8], c1[8], d[8];
+    bf8_to_f(*reinterpret_cast<const uint4 *>(in + p * in_ld + in_off + c), a);
+    bf8_to_f(*reinterpret_cast<const uint4 *>(in + (p + 1) * in_ld + in_off + c), b1);
+    bf8_to_f(*reinterpret_cast<const uint4 *>(in + (p + W) * in_ld + in_off + c), c1);
+    bf8_to_f(*reinterpret_cast<const uint4 *>(in + (p + W + 1) * in_ld + in_off + c), d);
+    __align__(16) bf16 o[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) o[k] = __float2bfloat16(0.25f * (((a[k] + b1[k]) + c1[k]) + d[k]));
+    *reinterpret_cast<uint4 *>(out + q * out_ld + out_off + c) = *reinterpret_cast<const uint4 *>(o);
+  }
+}
+// one thread per input pixel and 8 channels: writes the four output pixels
+__global__ void k_up_fwd8(const bf16 *in, int in_ld, int in_off, bf16 *out, int out_ld, int out_off,
+                          int C8, int B, int H, int W) {
+  const int Hi = H / 2, Wi = W / 2;
+  const long long n = (long long)B * Hi * Wi * C8;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(e % C8) * 8;
+    const long long q = e / C8;
+    const int x = (int)(q % Wi);
+    const long long t = q / Wi;
+    const int y = (int)(t % Hi);
+    const long long b = t / Hi;
+    const uint4 v = *reinterpret_cast<const uint4 *>(in + q * in_ld + in_off + c);
+    const long long p = (b * H + 2 * y) * W + 2 * x;
+    *reinterpret_cast<uint4 *>(out + p * out_ld + out_off + c) = v;
+    *reinterpret_cast<uint4 *>(out + (p + 1) * out_ld + out_off + c) = v;
+    *reinterpret_cast<uint4 *>(out + (p + W) * out_ld + out_off + c) = v;
+    *reinterpret_cast<uint4 *>(out + (p + W + 1) * out_ld + out_off + c) = v;
+  }
+}
+__global__ void k_head_fwd8(const bf16 *x, int x_ld, int x_off, int C, const float *w,
+                            const float *b, float *y, long long P) {
+  __shared__ float sw[256];
+  for (int c = threadIdx.x; c < C; c += blockDim.x) sw[c] = w[c];
+  __syncthreads();
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < P;
+       p += (long long)gridDim.x * blockDim.x) {
+    float s = b[0];
+    for (int c = 0; c < C; c += 8) {
+      float f[8];
+      bf8_to_f(*reinterpret_cast<const uint4 *>(x + p * x_ld + x_off + c), f);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) s += f[k] * sw[c + k];
+    }
+    y[p] = s;
+  }
+}
 // head backward: dx[p][c] = dy[p] * w[c] (bf16); dw[c] += sum_p dy[p] x[p][c]; db += sum dy
 __global__ void k_head_bwd(const bf16 *x, int x_ld, int x_off, int C, const float *w,
                            const float *dy, bf16 *dx, int dx_ld, int dx_off, float *dw, float *db,
@@ -443,7 +513,12 @@ int sevp_nn_pool(const void *in, int in_ld, int in_off, void *out, int out_ld, i
                  int B, int H, int W, int backward, int accumulate, void *stream) {
   if (!in || !out || (H % 2) || (W % 2)) return SEVP_BAD_ARG;
   cudaStream_t st = (cudaStream_t)stream;
-  if (!backward)
+  const bool v8 = C % 8 == 0 && in_ld % 8 == 0 && in_off % 8 == 0 && out_ld % 8 == 0 &&
+                  out_off % 8 == 0 && ((uintptr_t)in & 15) == 0 && ((uintptr_t)out & 15) == 0;
+  if (!backward && v8)
+    k_pool_fwd8<<<ew_grid((long long)B * H * W * C / 32), 256, 0, st>>>(
+        (const bf16 *)in, in_ld, in_off, (bf16 *)out, out_ld, out_off, C / 8, B, H, W);
+  else if (!backward)
     k_pool_fwd<<<ew_grid((long long)B * H * W * C / 4), 256, 0, st>>>(
         (const bf16 *)in, in_ld, in_off, (bf16 *)out, out_ld, out_off, C, B, H, W);
   else  // in = dOut (H/2 x W/2), out = dIn (H x W)
@@ -457,7 +532,12 @@ int sevp_nn_upsample(const void *in, int in_ld, int in_off, void *out, int out_l
                      int C, int B, int H, int W, int backward, void *stream) {
   if (!in || !out || (H % 2) || (W % 2)) return SEVP_BAD_ARG;
   cudaStream_t st = (cudaStream_t)stream;
-  if (!backward)  // in: H/2 x W/2, out: H x W
+  const bool v8 = C % 8 == 0 && in_ld % 8 == 0 && in_off % 8 == 0 && out_ld % 8 == 0 &&
+                  out_off % 8 == 0 && ((uintptr_t)in & 15) == 0 && ((uintptr_t)out & 15) == 0;
+  if (!backward && v8)  // in: H/2 x W/2, out: H x W
+    k_up_fwd8<<<ew_grid((long long)B * H * W * C / 32), 256, 0, st>>>(
+        (const bf16 *)in, in_ld, in_off, (bf16 *)out, out_ld, out_off, C / 8, B, H, W);
+  else if (!backward)
     k_up_fwd<<<ew_grid((long long)B * H * W * C), 256, 0, st>>>(
         (const bf16 *)in, in_ld, in_off, (bf16 *)out, out_ld, out_off, C, B, H, W);
   else  // in = dOut (H x W), out = dIn (H/2 x W/2)
@@ -474,7 +554,10 @@ int sevp_nn_head(const void *x, int x_ld, int x_off, int C, const float *w, cons
   cudaStream_t st = (cudaStream_t)stream;
   if (!backward) {
     if (!y || !b) return SEVP_BAD_ARG;
-    k_head_fwd<<<ew_grid(P), 256, 0, st>>>((const bf16 *)x, x_ld, x_off, C, w, b, y, P);
+    if (C % 8 == 0 && x_ld % 8 == 0 && x_off % 8 == 0 && ((uintptr_t)x & 15) == 0)
+      k_head_fwd8<<<ew_grid(P), 256, 0, st>>>((const bf16 *)x, x_ld, x_off, C, w, b, y, P);
+    else
+      k_head_fwd<<<ew_grid(P), 256, 0, st>>>((const bf16 *)x, x_ld, x_off, C, w, b, y, P);
   } else {
     if (!dy || !dx || !dw || !db) return SEVP_BAD_ARG;
     k_head_bwd<<<ew_grid(P), 256, 0, st>>>((const bf16 *)x, x_ld, x_off, C, w, dy, (bf16 *)dx, dx_ld,

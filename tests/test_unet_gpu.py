@@ -250,7 +250,10 @@ def test_conv_tcgen05_rejects_bad_shapes(torch_cuda):
     assert L.sevp_nn_conv3x3_tc(p(t), 32, 4, 16, p(t), p(f), p(t), 32, 0, 32, 1, 2, 2, 1, None) == 5
 
 
-def test_pool_upsample_exact(torch_cuda):
+@pytest.mark.parametrize("Cc", [16, 4])
+def test_pool_upsample_exact(torch_cuda, Cc):
+    """2x2 average pooling and nearest upsampling, exactly (8-channel
+    vector kernels for Cc = 16, one-element kernels for Cc = 4)."""
     torch = torch_cuda
     import ctypes as C
 
@@ -259,7 +262,7 @@ def test_pool_upsample_exact(torch_cuda):
     from musoc_solver_b200.unet import lib
 
     L = lib()
-    H, W, Cc = 8, 12, 16
+    H, W = 8, 12
     rng = np.random.default_rng(9)
     x = _bf(torch, rng.standard_normal((H * W, Cc))).cuda()
     p = lambda t: C.c_void_p(t.data_ptr())
