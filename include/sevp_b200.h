@@ -267,6 +267,34 @@ int sevp_profile_read(sevp_ctx *ctx, double *ms, long long *count);
 int sevp_inprod_noalloc(const double *r, const double *p, int i2, int j2, double *result,
                         void *stream);
 
+/* ---------------------------------------------------------------------
+ * EVP influence file, the record that PREP's INITFS writes
+ * (P/prep_GLOBAL.f90:320: WRITE(FNO_EVP) AL,AR,AB,AT,AC,RINV,RINV1,IE) and
+ * MAIN reads (M/input_GLOBAL.f90:440-443: READ(FN_EVP) AL,AR,AB,AT,AC,OAC,
+ * RINV,RINV1,IE): one big-endian Fortran unformatted sequential record in
+ * gfortran's framing (4-byte markers; records over 2147483639 bytes split
+ * into subrecords).  Host arrays, column-major as in the reference: the
+ * planes are (I2, J2) REAL*4, RINV / RINV1 hold n_rinv / n_rinv1 REAL*8
+ * ((I2, I2, NB0) and (I2, I2, NB1) for REP1, or the BIR strip shapes), IE
+ * NB0 INTEGER*4.  Influence data computed on the GPU by pre1_ / pre_ /
+ * sevp_pre_strips_ written here is read by MAIN unchanged.
+ * oac: NULL writes PREP's layout (no OAC plane); non-NULL writes MAIN's.
+ * The reader decides from the record length whether OAC is present, reports
+ * it in *has_oac (optional) and fills oac only if given; sizes that match
+ * neither layout return SEVP_BAD_ARG. */
+int sevp_evp_write(const char *path, int i2, int j2, const float *al, const float *ar,
+                   const float *ab, const float *at, const float *ac, const float *oac,
+                   const double *rinv, long long n_rinv, const double *rinv1, long long n_rinv1,
+                   const int *ie, int nb0);
+/* The same with a smaller subrecord limit (1 .. 2147483639 bytes). */
+int sevp_evp_write_sub(const char *path, int i2, int j2, const float *al, const float *ar,
+                       const float *ab, const float *at, const float *ac, const float *oac,
+                       const double *rinv, long long n_rinv, const double *rinv1, long long n_rinv1,
+                       const int *ie, int nb0, long long max_subrecord);
+int sevp_evp_read(const char *path, int i2, int j2, float *al, float *ar, float *ab, float *at,
+                  float *ac, float *oac, double *rinv, long long n_rinv, double *rinv1,
+                  long long n_rinv1, int *ie, int nb0, int *has_oac);
+
 #ifdef __cplusplus
 }
 #endif

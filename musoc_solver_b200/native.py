@@ -86,6 +86,13 @@ _SIGS = {
     "sevp_set_full_coefficients": ([P, C.c_int], C.c_int),
     "sevp_set_graphs": ([P, C.c_int], C.c_int),
     "sevp_inprod_noalloc": ([P, P, C.c_int, C.c_int, P, P], C.c_int),
+    "sevp_evp_write": ([C.c_char_p, C.c_int, C.c_int] + [P] * 6 + [P, C.c_longlong, P, C.c_longlong,
+                                                                P, C.c_int], C.c_int),
+    "sevp_evp_write_sub": ([C.c_char_p, C.c_int, C.c_int] + [P] * 6 + [P, C.c_longlong, P,
+                                                                    C.c_longlong, P, C.c_int,
+                                                                    C.c_longlong], C.c_int),
+    "sevp_evp_read": ([C.c_char_p, C.c_int, C.c_int] + [P] * 6 + [P, C.c_longlong, P, C.c_longlong,
+                                                               P, C.c_int, P], C.c_int),
     "sevp_profile": ([P, C.c_int], C.c_int),
     "sevp_set_warmstart": ([P, P, P, C.c_int], C.c_int),
     "sevp_solve_step": ([P, P, P, P, P, C.c_int, C.POINTER(SolveOpts), C.POINTER(Report)], C.c_int),

@@ -83,6 +83,43 @@ def test_pre1_rep1_bit_exact(L, oracle):
     assert np.linalg.norm(res) <= 1e-8 * np.linalg.norm(f)
 
 
+def test_pre1_evp_file_rep1(L, oracle, tmp_path):
+    """PREP -> MAIN through the EVP file: influence data computed by the GPU
+    pre1_ is written in PREP's record, read back as MAIN reads it, and the
+    GPU rep1_ on the read matrices equals the oracle's REP1 bit for bit."""
+    from musoc_solver_b200 import evp
+
+    p = _shifted_idealised(120, 60)
+    c = _coeffs(p)
+    j2, i2 = p.ac.shape
+    ie, ok = oracle.block_partition(j2, 6)
+    assert ok
+    nb = len(ie)
+    rinv = np.zeros((nb, i2, i2))
+    rinv1 = np.zeros((nb - 1, i2, i2))
+    h = np.zeros((j2 + 2, i2 + 2))
+    L.pre1_(*[_p(a) for a in c], _p(rinv), _p(rinv1), _p(h), _p(ie), _i(i2 + 2), _i(i2), _i(nb))
+    assert L.sevp_last_status() == 0
+    al, ab, ac, ar, at = c
+    evp.write(tmp_path / "EVP", al, ar, ab, at, ac, rinv, rinv1, ie)
+    r = evp.read(tmp_path / "EVP", i2, j2, rinv.shape, rinv1.shape, nb)
+    assert r["oac"] is None
+    rng = np.random.default_rng(3)
+    f = rng.standard_normal((j2, i2)).astype(np.float32)
+    x = np.zeros((j2 + 2, i2 + 2))
+    x[0] = rng.standard_normal(i2 + 2)
+    d0, d1, d2 = np.zeros((nb - 1, i2)), np.zeros(i2), np.zeros(i2)
+    hh = np.zeros((j2 + 2, i2 + 2))
+    xg = x.copy()
+    c2 = [np.ascontiguousarray(r[k]) for k in ("al", "ab", "ac", "ar", "at")]
+    L.rep1_(*[_p(a) for a in c2], _p(r["rinv"]), _p(r["rinv1"]), _p(d0), _p(d1), _p(d2), _p(f),
+            _p(hh), _p(xg), _p(r["ie"]), _i(i2 + 2), _i(i2), _i(nb))
+    assert L.sevp_last_status() == 0
+    r_o, r1_o, st = oracle.pre1(*c, ie)
+    xo = oracle.rep1(*c, r_o, r1_o, f, x, ie)
+    assert np.array_equal(xg, xo)
+
+
 def test_rep1_known_answer_constant(L, oracle):
     """FS_SOLVER's harness (M/fs_GLOBAL.f90:1814-1858): S = A*0 on the
     singular idealised stencil; SEVP returns a constant, i.e. x0 after the
