@@ -29,6 +29,8 @@
 #ifndef SEVP_B200_H
 #define SEVP_B200_H
 
+#include <stdint.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -266,6 +268,49 @@ int sevp_profile_read(sevp_ctx *ctx, double *ms, long long *count);
  * GPU race; calls ordered in one stream do not. */
 int sevp_inprod_noalloc(const double *r, const double *p, int i2, int j2, double *result,
                         void *stream);
+
+/* ---------------------------------------------------------------------
+ * Barotropic pressure correction of FS (M/fs_GLOBAL.f90:1154-1283), the
+ * ITMASK loop around the solve.  Device arrays, column-major with the
+ * reference's shapes: U (I0,J0,K1), V (I0,J1,K1), IU0 / IV0 (I0,J0) and
+ * IU (I0,J0,K1) / IV (I0,J1,K1) INTEGER*2, ODX / ODY / OCS (J0), CSV / ODYV
+ * (J1), ODZ (K1) REAL*4, S (I2,J2), P0 (I0,J0), SCR (I0,J0,4) REAL*4; X is
+ * the solver's unpadded (I2,J2) FP64 field (the interior of the reference's
+ * padded X).  The REAL*4 / REAL*8 steps follow the Fortran order, so the
+ * results equal the CPU oracle's bit for bit.  The reference's local
+ * override U = 1, V = 0 (:1173-1175) is not reproduced. */
+/* U(:,:,1) *= IU0 on interior (and, if periodic, the two wrap) U faces and
+ * V(:,:,1) *= IV0 on interior V faces (:1158-1171). */
+int sevp_fs_mask(int i0, int j0, float *u, float *v, const int16_t *iu0, const int16_t *iv0,
+                 int periodic, void *stream);
+/* S from continuity (FLAG_FS branch, :1177-1192): W integrated upwards from
+ * W(:,:,K0) = 0; S(I-1,J-1) = W(I,J,1).  s (REAL*4) and/or b (FP64 copy for
+ * the solver, multiplied by rscale(J-1) when rscale (J2 values) is given, to
+ * match a row-scaled symmetric operator) may be NULL. */
+int sevp_fs_rhs(int i0, int j0, int k0, const float *u, const float *v, const float *odx,
+                const float *ody, const float *ocs, const float *csv, const float *odz,
+                const float *rscale, float *s, double *b, void *stream);
+/* After the solve (:1216-1276): P0 += ODT X; SCR(:,:,1) / (:,:,2) = the U /
+ * V corrections -dX * ODX / ODYV (U periodic when periodic != 0), added to
+ * every layer (masked by IU / IV below the top) and accumulated in
+ * SCR(:,:,3) / (:,:,4); *vmax (device) = the largest top-layer velocity on
+ * land faces. */
+int sevp_fs_correct(int i0, int j0, int k0, const double *x, float odt, const float *odx,
+                    const float *odyv, const int16_t *iu, const int16_t *iv, const int16_t *iu0,
+                    const int16_t *iv0, float *p0, float *u, float *v, float *scr, int periodic,
+                    float *vmax, void *stream);
+/* The whole loop on the context's stream: mask, S, solve A X = S (the
+ * context's operator, I2 x J2, from zero; opts as for sevp_solve), correct,
+ * until the land velocity <= tolerance or mxmask passes.  b, x (I2*J2 FP64)
+ * and vmax_dev (one float) are device scratch supplied by the caller.
+ * Reports the passes, the final land velocity and the total PCG iterations. */
+int sevp_fs_barotropic(sevp_ctx *ctx, int i0, int j0, int k0, float *u, float *v, float *p0,
+                       float *scr, const int16_t *iu0, const int16_t *iv0, const int16_t *iu,
+                       const int16_t *iv, const float *odx, const float *ody, const float *ocs,
+                       const float *csv, const float *odyv, const float *odz,
+                       const float *rscale, float odt, int periodic, float tolerance, int mxmask,
+                       const sevp_solve_opts *opts, double *b, double *x, float *vmax_dev,
+                       int *itmask_out, float *vmax_out, int *iterations_out);
 
 /* ---------------------------------------------------------------------
  * EVP influence file, the record that PREP's INITFS writes

@@ -86,6 +86,13 @@ _SIGS = {
     "sevp_set_full_coefficients": ([P, C.c_int], C.c_int),
     "sevp_set_graphs": ([P, C.c_int], C.c_int),
     "sevp_inprod_noalloc": ([P, P, C.c_int, C.c_int, P, P], C.c_int),
+    "sevp_fs_mask": ([C.c_int, C.c_int, P, P, P, P, C.c_int, P], C.c_int),
+    "sevp_fs_rhs": ([C.c_int, C.c_int, C.c_int] + [P] * 11, C.c_int),
+    "sevp_fs_correct": ([C.c_int, C.c_int, C.c_int, P, C.c_float] + [P] * 10 + [C.c_int, P, P],
+                        C.c_int),
+    "sevp_fs_barotropic": ([P, C.c_int, C.c_int, C.c_int] + [P] * 15 + [C.c_float, C.c_int,
+                                                                      C.c_float, C.c_int] + [P] * 7,
+                           C.c_int),
     "sevp_evp_write": ([C.c_char_p, C.c_int, C.c_int] + [P] * 6 + [P, C.c_longlong, P, C.c_longlong,
                                                                 P, C.c_int], C.c_int),
     "sevp_evp_write_sub": ([C.c_char_p, C.c_int, C.c_int] + [P] * 6 + [P, C.c_longlong, P,

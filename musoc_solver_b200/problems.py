@@ -264,6 +264,100 @@ def ensemble(members: int = 64, nx: int = 720, ny: int = 360, seed: int = 5,
     return out
 
 
+@dataclass
+class FSState:
+    """A layered ocean state for the barotropic correction loop of FS, in the
+    reference's array shapes (C-order with I fastest): u (K1,J0,I0),
+    v (K1,J1,I0), p0 (J0,I0), scr (4,J0,I0); masks iu0 / iv0 (J0,I0),
+    iu (K1,J0,I0), iv (K1,J1,I0) int16; metrics odx / ody / ocs (J0),
+    csv / odyv (J1), odz (K1) float32; odt; and the symmetric (row-scaled)
+    operator with its row scale (J2) for the solve."""
+
+    u: np.ndarray
+    v: np.ndarray
+    p0: np.ndarray
+    scr: np.ndarray
+    iu0: np.ndarray
+    iv0: np.ndarray
+    iu: np.ndarray
+    iv: np.ndarray
+    odx: np.ndarray
+    ody: np.ndarray
+    ocs: np.ndarray
+    csv: np.ndarray
+    odyv: np.ndarray
+    odz: np.ndarray
+    odt: float
+    problem: Problem
+    rscale: np.ndarray
+
+    @property
+    def dims(self):
+        k1, j0, i0 = self.u.shape
+        return i0, j0, k1 + 1
+
+
+def fs_state(nx: int = 96, ny: int = 48, k1: int = 6, seed: int = 0, dt: float = 60.0,
+             lat_max: float = 78.0, speed: float = 0.1) -> FSState:
+    """Seeded layered state on the periodic global grid (interior nx x ny,
+    k1 layers of 4000 m in total).  Cells are wet in layer k where the
+    synthetic depth reaches the layer's top (the top layer counts as water
+    everywhere, as in the reference's solver coefficients); a face is wet
+    where both of its cells are.  The operator is the FLAG_FS form
+    div(sum_k dz_k mask_k grad) - 1/(g dt^2) with the reference's metric
+    factors (the assembly of P/prep_GLOBAL.f90:170-261), multiplied per row
+    by 1/(OCS(J) ODY(J)) so that it is symmetric; rscale is that factor."""
+    i2, j2 = nx, ny
+    i0, j0 = i2 + 2, j2 + 2
+    rng = np.random.default_rng(seed)
+    dlat = 2.0 * lat_max / ny
+    lat_c = -lat_max + (np.arange(j0) - 0.5) * dlat          # cell J = 1..J0
+    lat_v = -lat_max + np.arange(j0 - 1) * dlat              # V face J = 1..J1
+    dlon = np.deg2rad(360.0 / nx)
+    dy = EARTH_R * np.deg2rad(dlat)
+    odx = (1.0 / (EARTH_R * dlon * np.cos(np.deg2rad(lat_c)))).astype(np.float32)
+    ody = np.full(j0, 1.0 / dy, np.float32)
+    ocs = (1.0 / np.cos(np.deg2rad(lat_c))).astype(np.float32)
+    csv = np.cos(np.deg2rad(lat_v)).astype(np.float32)
+    odyv = np.full(j0 - 1, 1.0 / dy, np.float32)
+    dz = 4000.0 * np.linspace(1.0, 3.0, k1) / np.linspace(1.0, 3.0, k1).sum()
+    odz = (1.0 / dz).astype(np.float32)
+    ztop = np.concatenate([[0.0], np.cumsum(dz)[:-1]])
+    depth, _, _ = global_depth(nx, ny, seed)
+    dpad = np.zeros((j0, i0))
+    dpad[1:-1, 1:-1] = depth
+    dpad[:, 0], dpad[:, -1] = dpad[:, -2], dpad[:, 1]          # periodic ghost columns
+    wet = np.stack([dpad > ztop[k] + 1.0 for k in range(k1)])  # (K1, J0, I0)
+    wet[0] = dpad > 0.0
+    iu = np.zeros((k1, j0, i0), np.int16)
+    iu[:, :, :-1] = (wet[:, :, :-1] & wet[:, :, 1:])
+    iv = (wet[:, :-1, :] & wet[:, 1:, :]).astype(np.int16)
+    iu0, iv0 = iu[0].copy(), np.zeros((j0, i0), np.int16)
+    iv0[:-1] = iv[0]
+    u = (speed * rng.standard_normal((k1, j0, i0))).astype(np.float32)
+    v = (speed * rng.standard_normal((k1, j0 - 1, i0))).astype(np.float32)
+    p0 = np.zeros((j0, i0), np.float32)
+    scr = np.zeros((4, j0, i0), np.float32)
+    # face coefficients, one value per face, so the operator is exactly symmetric
+    w_row = (1.0 / (ocs[1:-1].astype(np.float64) * ody[1:-1]))  # rscale, J = 2..J1
+    hx = np.einsum("k,kji->ji", dz, np.where(np.arange(k1)[:, None, None] == 0, 1, iu))
+    hy = np.einsum("k,kji->ji", dz, np.where(np.arange(k1)[:, None, None] == 0, 1, iv))
+    cx = (hx[1:-1, :] * (odx[1:-1, None].astype(np.float64) ** 2) * w_row[:, None]).astype(np.float32)
+    cy = (hy * (csv[:, None].astype(np.float64) * odyv[:, None])).astype(np.float32)
+    ar = cx[:, 1:-1].copy()            # face east of cell I = 2..I1
+    al = cx[:, 0:-2].copy()            # face west of cell I (periodic through the ghost)
+    at = cy[1:, 1:-1].copy()
+    ab = cy[:-1, 1:-1].copy()
+    at[-1] = 0.0                       # closed north and south edges
+    ab[0] = 0.0
+    gamma = 1.0 / (9.81 * dt * dt)
+    ac = (-(al.astype(np.float64) + ar + ab + at) - gamma * w_row[:, None]).astype(np.float32)
+    prob = Problem(al, ab, ac, ar, at, np.zeros((j2, i2)), periodic=True, name=f"fs{nx}x{ny}x{k1}",
+                   meta=dict(gamma=gamma))
+    return FSState(u, v, p0, scr, iu0, iv0, iu, iv, odx, ody, ocs, csv, odyv, odz, np.float32(1.0 / dt),
+                   prob, w_row.astype(np.float32))
+
+
 def stack(members) -> Problem:
     """Members of one grid size stacked along y into one block-diagonal
     problem.  Each member's north and south edge faces are closed (AT of its

@@ -271,3 +271,46 @@ def apply(p, x):
     lib().or_apply(*[_c(a, np.float32) for a in p.coeffs()], p.nx, p.ny, int(p.periodic),
                    _c(x, np.float64), y)
     return y
+
+
+# ------------------------------------------------ barotropic correction of FS
+def _fs_sigs():
+    L = lib()
+    if getattr(L, "_fs_sigs", False):
+        return L
+    f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+    f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+    i16p = np.ctypeslib.ndpointer(np.int16, flags="C_CONTIGUOUS")
+    L.or_fs_mask.argtypes = [C.c_int, C.c_int, f32p, f32p, i16p, i16p, C.c_int]
+    L.or_fs_mask.restype = None
+    L.or_fs_rhs.argtypes = [C.c_int, C.c_int, C.c_int] + [f32p] * 8
+    L.or_fs_rhs.restype = None
+    L.or_fs_correct.argtypes = [C.c_int, C.c_int, C.c_int, f64p, C.c_float, f32p, f32p, i16p, i16p,
+                                i16p, i16p, f32p, f32p, f32p, f32p, C.c_int]
+    L.or_fs_correct.restype = C.c_float
+    L._fs_sigs = True
+    return L
+
+
+def fs_mask(u, v, iu0, iv0, periodic=True):
+    """In place on u (K1,J0,I0) and v (K1,J1,I0) (M/fs_GLOBAL.f90:1158-1171)."""
+    k1, j0, i0 = u.shape
+    _fs_sigs().or_fs_mask(i0, j0, u, v, iu0, iv0, int(periodic))
+
+
+def fs_rhs(u, v, odx, ody, ocs, csv, odz):
+    """S (J2,I2) from continuity (M/fs_GLOBAL.f90:1177-1192)."""
+    k1, j0, i0 = u.shape
+    s = np.zeros((j0 - 2, i0 - 2), np.float32)
+    _fs_sigs().or_fs_rhs(i0, j0, k1 + 1, u, v, odx, ody, ocs, csv, odz, s)
+    return s
+
+
+def fs_correct(x_interior, odt, odx, odyv, iu, iv, iu0, iv0, p0, u, v, scr, periodic=True):
+    """In place on p0, u, v, scr (4,J0,I0); x_interior is the (J2,I2) solution.
+    Returns the largest top-layer land velocity (M/fs_GLOBAL.f90:1216-1276)."""
+    k1, j0, i0 = u.shape
+    x = np.zeros((j0, i0))
+    x[1:-1, 1:-1] = x_interior
+    return float(_fs_sigs().or_fs_correct(i0, j0, k1 + 1, x, np.float32(odt), odx, odyv, iu, iv,
+                                          iu0, iv0, p0, u, v, scr, int(periodic)))

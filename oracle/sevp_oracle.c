@@ -1175,3 +1175,115 @@ int or_pcg(const tile_pc_t *pc, const float *al, const float *ab, const float *a
   free(r), free(z), free(p), free(q);
   return it;
 }
+
+/* ---------------------------------------------------------------------
+ * Barotropic pressure correction of FS (M/fs_GLOBAL.f90:1156-1283), the
+ * ITMASK loop around the elliptic solve.  Arrays column-major with the
+ * reference's shapes: U (I0,J0,K1), V (I0,J1,K1), IU0 / IV0 (I0,J0) and
+ * IU (I0,J0,K1) / IV (I0,J1,K1) INTEGER*2, ODX / ODY / OCS (J0), CSV / ODYV
+ * (J1), ODZ (K1), S (I2,J2), X / P0 (I0,J0), SCR (I0,J0,4); I1 = I0-1,
+ * I2 = I0-2, J1 = J0-1, J2 = J0-2, K1 = K0-1.  REAL*4 arithmetic is done in
+ * float, REAL*8 in double, in the Fortran evaluation order.
+ */
+#define U3(i, j, k) u[IX3(i0, j0, i, j, k)]
+#define V3(i, j, k) v[IX3(i0, j0 - 1, i, j, k)]
+
+/* Zero the top-layer advection velocity over land
+ * (M/fs_GLOBAL.f90:1158-1171; the periodic faces under LOPENW == 1). */
+void or_fs_mask(int i0, int j0, float *u, float *v, const int16_t *iu0, const int16_t *iv0,
+                int periodic) {
+  const int i1 = i0 - 1, i2 = i0 - 2, j1 = j0 - 1, j2 = j0 - 2;
+  for (int j = 2; j <= j1; ++j) {
+    for (int i = 2; i <= i2; ++i) U3(i, j, 1) = (float)iu0[IX(i0, i, j)] * U3(i, j, 1);
+    if (periodic) {
+      U3(1, j, 1) = (float)iu0[IX(i0, 1, j)] * U3(1, j, 1);
+      U3(i1, j, 1) = (float)iu0[IX(i0, i1, j)] * U3(i1, j, 1);
+    }
+  }
+  for (int j = 2; j <= j2; ++j)
+    for (int i = 2; i <= i1; ++i) V3(i, j, 1) = (float)iv0[IX(i0, i, j)] * V3(i, j, 1);
+}
+
+/* Free-surface right-hand side from continuity (FLAG_FS branch,
+ * M/fs_GLOBAL.f90:1177-1192): W integrated from W(:,:,K0) = 0 upwards,
+ *   W(I,J,K) = W(I,J,K+1) + ((U(I,J,K)-U(I-1,J,K))*ODX(J)
+ *              + (CSV(J)*V(I,J,K)-CSV(J-1)*V(I,J-1,K))*OCS(J)*ODY(J)) / ODZ(K),
+ * and S(I-1,J-1) = W(I,J,1). */
+void or_fs_rhs(int i0, int j0, int k0, const float *u, const float *v, const float *odx,
+               const float *ody, const float *ocs, const float *csv, const float *odz, float *s) {
+  const int i1 = i0 - 1, i2 = i0 - 2, j1 = j0 - 1, k1 = k0 - 1;
+  for (int j = 2; j <= j1; ++j)
+    for (int i = 2; i <= i1; ++i) {
+      float w = 0.f;
+      for (int k = k1; k >= 1; --k) {
+        const float temp1 = 1.f / odz[k - 1];
+        const float temp = ocs[j - 1] * ody[j - 1];
+        const float a = (U3(i, j, k) - U3(i - 1, j, k)) * odx[j - 1];
+        const float b = csv[j - 1] * V3(i, j, k) - csv[j - 2] * V3(i, j - 1, k);
+        w = w + (a + b * temp) * temp1;
+      }
+      s[IX(i2, i - 1, j - 1)] = w;
+    }
+}
+
+/* After the solve (M/fs_GLOBAL.f90:1216-1280): P0 += ODT*X; the current
+ * corrections SCR(:,:,1) (U faces, periodic under FLAG_PERIODIC_WE) and
+ * SCR(:,:,2) (V faces) from the gradients of X, added to every layer
+ * (IU / IV below the top) and accumulated in SCR(:,:,3) / SCR(:,:,4).
+ * Returns the largest top-layer velocity on land faces (the loop's test). */
+float or_fs_correct(int i0, int j0, int k0, const double *x, float odt, const float *odx,
+                    const float *odyv, const int16_t *iu, const int16_t *iv, const int16_t *iu0,
+                    const int16_t *iv0, float *p0, float *u, float *v, float *scr, int periodic) {
+  const int i1 = i0 - 1, i2 = i0 - 2, j1 = j0 - 1, j2 = j0 - 2, k1 = k0 - 1;
+  float *s1 = scr, *s2 = scr + (size_t)i0 * j0, *s3 = scr + 2 * (size_t)i0 * j0,
+        *s4 = scr + 3 * (size_t)i0 * j0;
+  for (int j = 2; j <= j1; ++j)
+    for (int i = 2; i <= i1; ++i)
+      p0[IX(i0, i, j)] = (float)((double)p0[IX(i0, i, j)] + (double)odt * x[IX(i0, i, j)]);
+  for (int j = 2; j <= j1; ++j) {
+    for (int i = 2; i <= i2; ++i)
+      s1[IX(i0, i, j)] = (float)(-((x[IX(i0, i + 1, j)] - x[IX(i0, i, j)]) * (double)odx[j - 1]));
+    s1[IX(i0, 1, j)] = 0.f;
+    s1[IX(i0, i1, j)] = 0.f;
+    if (periodic) {
+      s1[IX(i0, 1, j)] = (float)(-((x[IX(i0, 2, j)] - x[IX(i0, i1, j)]) * (double)odx[j - 1]));
+      s1[IX(i0, i1, j)] = s1[IX(i0, 1, j)];
+    }
+    for (int i = 1; i <= i1; ++i) {
+      const float c = s1[IX(i0, i, j)];
+      s3[IX(i0, i, j)] = s3[IX(i0, i, j)] + c;
+      U3(i, j, 1) = U3(i, j, 1) + c;
+      for (int k = 2; k <= k1; ++k) U3(i, j, k) = U3(i, j, k) + c * (float)iu[IX3(i0, j0, i, j, k)];
+    }
+  }
+  for (int j = 2; j <= j2; ++j)
+    for (int i = 2; i <= i1; ++i)
+      s2[IX(i0, i, j)] = (float)(-((x[IX(i0, i, j + 1)] - x[IX(i0, i, j)]) * (double)odyv[j - 1]));
+  for (int i = 2; i <= i1; ++i) {
+    s2[IX(i0, i, 1)] = 0.f;
+    s2[IX(i0, i, j1)] = 0.f;
+  }
+  for (int j = 1; j <= j1; ++j)
+    for (int i = 2; i <= i1; ++i) {
+      s4[IX(i0, i, j)] = s4[IX(i0, i, j)] + s2[IX(i0, i, j)];
+      V3(i, j, 1) = V3(i, j, 1) + s2[IX(i0, i, j)];
+    }
+  for (int k = 2; k <= k1; ++k)
+    for (int j = 1; j <= j1; ++j)
+      for (int i = 2; i <= i1; ++i)
+        V3(i, j, k) = V3(i, j, k) + s2[IX(i0, i, j)] * (float)iv[IX3(i0, j0 - 1, i, j, k)];
+  float tmp = 0.f;
+  for (int j = 2; j <= j1; ++j)
+    for (int i = 2; i <= i2; ++i) {
+      const float t = (float)(1 - iu0[IX(i0, i, j)]) * fabsf(U3(i, j, 1));
+      tmp = tmp > t ? tmp : t;
+    }
+  for (int j = 2; j <= j2; ++j)
+    for (int i = 2; i <= i1; ++i) {
+      const float t = (float)(1 - iv0[IX(i0, i, j)]) * fabsf(V3(i, j, 1));
+      tmp = tmp > t ? tmp : t;
+    }
+  return tmp;
+}
+#undef U3
+#undef V3
