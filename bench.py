@@ -77,6 +77,8 @@ def parse():
                     help="the network runs on the grid averaged over coarse x coarse cells")
     ap.add_argument("--tiles", default="auto",
                     help="tile shape MxH of the GPU solver, or 'auto' (measured at start-up)")
+    ap.add_argument("--no-fs", action="store_true",
+                    help="skip the barotropic correction loop arm (3600x2400, 20 layers)")
     ap.add_argument("--no-ensemble", action="store_true",
                     help="skip the 64-member 720x360 ensemble arm")
     ap.add_argument("--no-learned", action="store_true",
@@ -283,6 +285,60 @@ def run_ensemble(K, W, members=64, nx=720, ny=360):
     return out
 
 
+# ------------------------------------------------ barotropic correction loop
+def run_fs(nx, ny, k1, tiles, passes=3, peak=None):
+    """The FS barotropic correction (ITMASK loop) on a layered state: one
+    pass = land masking, continuity right-hand side, mixed solve, P0 and
+    velocity correction of every layer."""
+    import torch
+
+    from musoc_solver_b200 import problems as P
+    from musoc_solver_b200.barotropic import BarotropicCorrection
+
+    st = P.fs_state(nx, ny, k1, seed=7)
+    bc = BarotropicCorrection(st, tile_m=tiles[0], tile_h=tiles[1])
+    u, v, p0, scr = bc.upload()
+    stream = bc.solver.stream
+    bc.run(u, v, p0, scr, tolerance=0.0, mxmask=1)  # warm-up pass
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    n_pass, vmax, iters = bc.run(u, v, p0, scr, tolerance=0.0, mxmask=passes)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    t_loop = ev0.elapsed_time(ev1) / n_pass
+
+    def time_ms(fn, reps=5):
+        fn()
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(reps):
+            fn()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        return ev0.elapsed_time(ev1) / reps
+
+    n = nx * ny
+    t_rhs = time_ms(lambda: bc.rhs(u, v, b=bc.b))
+    t_cor = time_ms(lambda: bc.correct(bc.x, u, v, p0, scr))
+    # algorithmic bytes: rhs reads U and V of every layer, writes b; the
+    # correction reads X and masks, reads and writes U, V, P0 and 4 SCR planes
+    b_rhs = n * (8 * k1 + 8)
+    b_cor = n * (8 + 12 * k1 + 8 + 8 + 16)
+    gbs = lambda b, ms: b / (ms * 1e-3) / 1e9
+    out = {"workload": f"{nx}x{ny} interior, {k1} layers, land masks from the synthetic depth; "
+                       f"mixed solve to 1e-12, tiles {tiles[0]}x{tiles[1]}",
+           "ms_per_pass": t_loop, "passes": n_pass, "pcg_iterations": iters,
+           "land_velocity_after": vmax,
+           "rhs_ms": t_rhs, "rhs_gbs": gbs(b_rhs, t_rhs), "correct_ms": t_cor,
+           "correct_gbs": gbs(b_cor, t_cor)}
+    if peak:
+        out["rhs_frac"] = gbs(b_rhs, t_rhs) / peak
+        out["correct_frac"] = gbs(b_cor, t_cor) / peak
+    bc.close()
+    return out
+
+
 # ---------------------------------------------------------------- native
 def run_native(args, world, rank, local, dist):
     import torch
@@ -456,6 +512,11 @@ def run_native(args, world, rank, local, dist):
     if not args.no_ensemble:
         ens = run_ensemble(max(2, K // 2), max(1, min(W, 2)))
 
+    # ---- the barotropic correction loop around the solve (FS ITMASK loop)
+    fs = None
+    if not args.no_fs:
+        fs = run_fs(p.nx, p.ny, 20, tiles, peak=peak)
+
     # ---- CPU baseline (rank 0 at N = 1)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -521,6 +582,7 @@ def run_native(args, world, rank, local, dist):
                     "precondition_start": {"launches": prof["precond"][1],
                                            "avg_ms": prof["precond"][0] / max(prof["precond"][1], 1)}},
         "ensemble_c5": ens,
+        "fs_barotropic_loop": fs,
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
         "gpu_launches": int(launches_value),

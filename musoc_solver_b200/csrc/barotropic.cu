@@ -92,6 +92,7 @@ __global__ void k_fs_correct(int i0, int j0, int k0, const double *x, float odt,
     s3[o] = __fadd_rn(s3[o], c);
     const float top = __fadd_rn(u[IDX3(j0, i, j, 1)], c);
     u[IDX3(j0, i, j, 1)] = top;
+#pragma unroll 4
     for (int k = 2; k <= k1; ++k)
       u[IDX3(j0, i, j, k)] =
           __fadd_rn(u[IDX3(j0, i, j, k)], __fmul_rn(c, (float)iu[IDX3(j0, i, j, k)]));
@@ -105,6 +106,7 @@ __global__ void k_fs_correct(int i0, int j0, int k0, const double *x, float odt,
     s4[o] = __fadd_rn(s4[o], c);
     const float top = __fadd_rn(v[IDX3(j0 - 1, i, j, 1)], c);
     v[IDX3(j0 - 1, i, j, 1)] = top;
+#pragma unroll 4
     for (int k = 2; k <= k1; ++k)
       v[IDX3(j0 - 1, i, j, k)] =
           __fadd_rn(v[IDX3(j0 - 1, i, j, k)], __fmul_rn(c, (float)iv[IDX3(j0 - 1, i, j, k)]));
