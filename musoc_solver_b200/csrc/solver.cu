@@ -313,6 +313,9 @@ struct OpResidual {
 
 // --------------------------------------------------- tile apply kernel
 constexpr int kTileWarps = 8;
+// FP32-vector tiles up to this height use k_tile_short (measured faster
+// there; the FP64 kernel and taller tiles keep k_tile_apply)
+constexpr int kShortTileRows = 6;
 
 
 // Shared memory per warp: the tile's rows of z (FP64 marching state, 32
@@ -609,6 +612,215 @@ __global__ void __launch_bounds__(kTileWarps * 32, SEVP_TILE_MINB)
           V zv = (V)zs[k * 32 + lane];
           z[idx] = zv;
           if (DOTS) acc_rz += (double)r[idx] * (double)zv;
+        }
+      }
+      vnext = v;
+    }
+  }
+  if (DOTS) {
+    double v2[2] = {acc_rz, acc_rr};
+    TileFin fin{st};
+    reduce_and_finish<2>(v2, partials, ticket, fin);
+  }
+}
+
+// Tiles of at most HM rows (the short tiles the autotuner prefers): the same
+// algorithm as k_tile_apply, operation for operation, with every row of a
+// task loaded into registers at once (one memory round trip per task
+// instead of one per row) and the rows unrolled.  hh, nb and the sub-block
+// bounds are the same for all lanes of a warp, so the predicated rows keep
+// the warp converged for the shuffles and mat-vecs.
+template <typename V, typename MT, bool UPDATE, bool DOTS, bool SYM, int HM>
+__global__ void __launch_bounds__(kTileWarps * 32, 2)
+    k_tile_short(TileGeom tg, Coeffs c, const MT *__restrict__ mats, V *x, const V *p, V *r,
+                 const V *q, V *z, SolveState *st, double *partials, unsigned *ticket) {
+  if (DOTS && st->done) return;
+  constexpr bool kChain = sizeof(V) == 4;
+  __shared__ double dv_all[kTileWarps * 32];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  double *dv = dv_all + wib * 32;
+  double acc_rz = 0.0, acc_rr = 0.0;
+  double alpha = 0.0;
+  if (UPDATE) alpha = st->alpha;
+  const int ntasks = tg.ty * tg.txg;
+  for (int gw = blockIdx.x * kTileWarps + wib; gw < ntasks; gw += gridDim.x * kTileWarps) {
+    const int b = gw / tg.txg;
+    const int grp = gw - b * tg.txg;
+    const int seg = lane / tg.wseg, n = lane - seg * tg.wseg, segbase = seg * tg.wseg;
+    const int a = grp * tg.tpw + seg;
+    const int mw = (a < tg.tx) ? tile_width(tg, a) : 0;
+    const bool active = n < mw;
+    const int nx = tg.nx;
+    const int j0 = b * tg.th, hh = tile_height(tg, b), nb = tg.grp_nb[(size_t)b * tg.txg + grp];
+    const int i = a * tg.tm + n;
+    const MT *mt = mats + (mw > 0 ? tg.moff[(size_t)b * tg.tx + a] : 0);
+    const size_t msz = (size_t)mw * mw;
+    const size_t idx0 = (size_t)j0 * nx + i;
+
+    // ---- all loads of the task
+    V rr[HM], xx[UPDATE ? HM : 1], pp[UPDATE ? HM : 1], qq[UPDATE ? HM : 1];
+    float cc_[HM], ce_[HM], cn_[HM], cw_[SYM ? 1 : HM], cs_[SYM ? 1 : HM];
+#pragma unroll
+    for (int k = 0; k < HM; ++k) {
+      const bool ok = active && k < hh;
+      const size_t id = ok ? idx0 + (size_t)k * nx : 0;
+      rr[k] = ok ? r[id] : V(0);
+      if (UPDATE) {
+        xx[k] = ok ? x[id] : V(0);
+        pp[k] = ok ? p[id] : V(0);
+        qq[k] = ok ? q[id] : V(0);
+      }
+      cc_[k] = ok ? __ldg(c.ac + id) : 0.f;
+      ce_[k] = ok ? __ldg(c.ar + id) : 0.f;
+      cn_[k] = ok ? __ldg(c.at + id) : 0.f;
+      if (!SYM) {
+        cw_[k] = ok ? __ldg(c.al + id) : 0.f;
+        cs_[k] = ok ? __ldg(c.ab + id) : 0.f;
+      }
+    }
+
+    // ---- forward sweep (as k_tile_apply)
+    double zs[HM], rho[HM];
+    double zb = 0.0, zc = 0.0;
+    float cn_prev = 0.f;
+    int t = 0, kb = 0, ke = sub_start(1, hh, nb) - 1;
+#pragma unroll
+    for (int k = 0; k < HM; ++k) {
+      zs[k] = 0.0;
+      rho[k] = 0.0;
+      if (k < hh) {
+        double rv = 0.0;
+        double cw, cs;
+        if (SYM) {
+          const float arw = __shfl_up_sync(0xffffffffu, ce_[k], 1);
+          cw = (n == 0) ? 0.0 : (double)arw;
+          cs = (double)cn_prev;
+          cn_prev = cn_[k];
+        } else {
+          cw = cw_[k];
+          cs = cs_[k];
+        }
+        const double cc = cc_[k], ce = ce_[k];
+        const double cn = active ? (double)cn_[k] : 1.0;
+        const double rcp_k = kChain ? march_rcp(cn) : 0.0;
+        if (active) {
+          if (UPDATE) {
+            const size_t idx = idx0 + (size_t)k * nx;
+            const V xn = xx[k] + (V)alpha * pp[k];
+            const V rn = rr[k] - (V)alpha * qq[k];
+            x[idx] = xn;
+            r[idx] = rn;
+            rr[k] = rn;
+          }
+          rv = (double)rr[k];
+          acc_rr += rv * rv;
+        }
+        if (k == kb) zc = 0.0;
+        const double part = (kChain && active) ? (rv - cs * zb) - cc * zc : 0.0;
+        double zw = __shfl_up_sync(0xffffffffu, zc, 1);
+        double ze = __shfl_down_sync(0xffffffffu, zc, 1);
+        if (n == 0) zw = 0.0;
+        if (n >= mw - 1) ze = 0.0;
+        zs[k] = zc;
+        const double res = (kChain && active) ? (part - cw * zw) - ce * ze : 0.0;
+        if (k < ke) {
+          double zn;
+          if constexpr (kChain)
+            zn = res * rcp_k;
+          else
+            zn = active ? ((((rv - cw * zw) - cs * zb) - cc * zc) - ce * ze) / cn : 0.0;
+          zb = zc;
+          zc = zn;
+        } else {
+          double rh;
+          if constexpr (kChain)
+            rh = res;
+          else
+            rh = active ? (((rv - cw * zw) - cs * zb) - cc * zc) - ce * ze : 0.0;
+          rho[k] = rh;
+          if (t < nb - 1) {
+            dv[lane] = rh;
+            __syncwarp();
+            double sc = active ? seg_matvec<MT>(dv, segbase, mt + (size_t)(nb + t) * msz, mw, n) : 0.0;
+            __syncwarp();
+            zc = zc - sc;
+          }
+          zb = zc;
+          ++t;
+          kb = k + 1;
+          ke = sub_start(t + 1, hh, nb) - 1;
+        }
+      }
+    }
+    // ---- backward sweep (as k_tile_apply)
+    double vnext = 0.0;
+    for (t = nb - 1; t >= 0; --t) {
+      kb = sub_start(t, hh, nb);
+      ke = sub_start(t + 1, hh, nb) - 1;
+      double rho_ke = 0.0;
+      float cn_ke = 0.f, cnb = 0.f;
+#pragma unroll
+      for (int k = 0; k < HM; ++k) {
+        if (k == ke) rho_ke = rho[k], cn_ke = cn_[k];
+        if (k == kb - 1) cnb = cn_[k];
+      }
+      const double cnk = active ? (double)cn_ke : 0.0;
+      dv[lane] = rho_ke - cnk * vnext;
+      __syncwarp();
+      double v = active ? seg_matvec<MT>(dv, segbase, mt + (size_t)t * msz, mw, n) : 0.0;
+      __syncwarp();
+#pragma unroll
+      for (int k = 0; k < HM; ++k)
+        if (k == kb) zs[k] += v;
+      double hb = 0.0, hc = v;
+      if (!active) cnb = 0.f;
+      if (t > 0) {
+        dv[lane] = v * (double)cnb;
+        __syncwarp();
+        hb = active ? seg_matvec<MT>(dv, segbase, mt + (size_t)(nb + t - 1) * msz, mw, n) : 0.0;
+        __syncwarp();
+      }
+      float cn_prev_b = cnb;
+#pragma unroll
+      for (int k = 0; k < HM - 1; ++k) {
+        if (k >= kb && k < ke) {
+          const float ncc = active ? cc_[k] : 0.f, nce = active ? ce_[k] : 0.f;
+          const float ncn = active ? cn_[k] : 1.f;
+          double cw, cs;
+          if (SYM) {
+            const float arw = __shfl_up_sync(0xffffffffu, nce, 1);
+            cw = (n == 0) ? 0.0 : (double)arw;
+            cs = (double)cn_prev_b;
+            cn_prev_b = ncn;
+          } else {
+            cw = active ? cw_[k] : 0.f;
+            cs = active ? cs_[k] : 0.f;
+          }
+          const double cc = ncc, ce = nce, cn = ncn;
+          const double rcp_k = kChain ? march_rcp(cn) : 0.0;
+          const double part = kChain ? -(cs * hb) - cc * hc : 0.0;
+          double hw = __shfl_up_sync(0xffffffffu, hc, 1);
+          double he = __shfl_down_sync(0xffffffffu, hc, 1);
+          if (n == 0) hw = 0.0;
+          if (n >= mw - 1) he = 0.0;
+          double hn;
+          if constexpr (kChain)
+            hn = active ? ((part - cw * hw) - ce * he) * rcp_k : 0.0;
+          else
+            hn = active ? ((((-(cw * hw)) - cs * hb) - cc * hc) - ce * he) / cn : 0.0;
+          zs[k + 1] += hn;
+          hb = hc;
+          hc = hn;
+        }
+      }
+      if (active) {
+#pragma unroll
+        for (int k = 0; k < HM; ++k) {
+          if (k >= kb && k <= ke) {
+            const V zv = (V)zs[k];
+            z[idx0 + (size_t)k * nx] = zv;
+            if (DOTS) acc_rz += (double)rr[k] * (double)zv;
+          }
         }
       }
       vnext = v;
@@ -969,11 +1181,15 @@ template <typename V, typename MT, bool UPDATE, bool DOTS, bool SYM>
 static int launch_tile_k(sevp_ctx *ctx, const MT *mats, V *x, const V *p, V *r, const V *q, V *z,
                          int ticket_slot) {
   const size_t warps = tile_warps(ctx->tg);
-  const size_t smem = tile_smem_per_warp(ctx->tg.hmax) * kTileWarps;
-  auto kern = k_tile_apply<V, MT, UPDATE, DOTS, SYM>;
+  const bool short_tiles = sizeof(V) == 4 && ctx->tg.hmax <= kShortTileRows;
+  const size_t smem = short_tiles ? 0 : tile_smem_per_warp(ctx->tg.hmax) * kTileWarps;
+  auto kern = short_tiles ? k_tile_short<V, MT, UPDATE, DOTS, SYM, kShortTileRows>
+                          : k_tile_apply<V, MT, UPDATE, DOTS, SYM>;
   static size_t set_smem = 0;  // per instantiation (one device per process is assumed)
   static int slots = 0;         // resident CTAs on the device at set_smem
-  if (set_smem != smem) {
+  static int set_short = -1;
+  if (set_smem != smem || set_short != (int)short_tiles) {
+    set_short = (int)short_tiles;
     if (smem > 48 * 1024)
       SEVP_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0, dev = 0, sms = 0;
