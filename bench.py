@@ -149,9 +149,12 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-def ncu_traffic():
-    """Per-launch DRAM bytes of the tile pass-B kernel from the committed ncu
-    summary (profiles/), or None."""
+def ncu_traffic(nx, ny, tiles):
+    """Per-launch DRAM bytes of the FP32 tile pass-B kernel from the committed
+    ncu summary (profiles/), or None when the summary covers another grid or
+    tile shape (it is a 3600x2400 capture with 16x6 tiles)."""
+    if (nx, ny, tuple(tiles)) != (3600, 2400, (16, 6)):
+        return None
     path = os.path.join(ROOT, "profiles", "tile_pass_b_3600x2400.md")
     try:
         for line in open(path):
@@ -505,7 +508,8 @@ def run_native(args, world, rank, local, dist):
     bytes_per_launch = n * (4 * 4 + 3 * 4 + 4 * ncoef) + infl_bytes
     avg_s = tile_ms / 1e3 / max(tile_n, 1)
     achieved = bytes_per_launch / avg_s / 1e9 if tile_n else None
-    traffic = ncu_traffic()
+    traffic = ncu_traffic(p.nx, p.ny, tiles)
+    short_tiles = tiles[1] <= 6  # FP32 vectors with tiles up to 6 rows run the short-tile kernel
 
     # ---- 64-member ensemble (720x360 each), every launch over all members
     ens = None
@@ -572,7 +576,8 @@ def run_native(args, world, rank, local, dist):
                 "d2h_bytes_per_step": d2h},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                     "kernel": "k_tile_apply<float, update, dots> (PCG pass B)",
+                     "kernel": ("k_tile_short<float, update, dots>" if short_tiles
+                                else "k_tile_apply<float, update, dots>") + " (PCG pass B)",
                      "algorithmic_bytes_per_launch": bytes_per_launch,
                      "avg_launch_ms": avg_s * 1e3, "launches": tile_n,
                      "peak_source": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)"},

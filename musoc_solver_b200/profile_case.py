@@ -1,9 +1,9 @@
 """One solve on a synthetic global grid, as a target for ncu captures.
 
-    python -m musoc_solver_b200.profile_case --nx 3600 --ny 2400 --precision 1 --max-iter 3
+    python -m musoc_solver_b200.profile_case --nx 3600 --ny 2400 --tiles 16x6 --precision 1 --max-iter 3
 
-Builds ``problems.global_grid(nx, ny, seed=11)`` and a 16x16-tile solver
-(growth bound 1e10), then runs one solve with the given precision and
+Builds ``problems.global_grid(nx, ny, seed=11)`` and a solver with the given
+tiles (growth bound 1e10), then runs one solve with the given precision and
 iteration cap.  The first launch of each kernel belongs to the set-up, so
 skip one launch (``-s 1``) to capture a PCG iteration.
 """
@@ -16,6 +16,7 @@ def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--nx", type=int, default=3600)
     ap.add_argument("--ny", type=int, default=2400)
+    ap.add_argument("--tiles", default="16x16")
     ap.add_argument("--precision", type=int, default=1, choices=[0, 1])
     ap.add_argument("--max-iter", type=int, default=3)
     args = ap.parse_args(argv)
@@ -26,7 +27,8 @@ def main(argv=None):
 
     build.build()
     p = P.global_grid(args.nx, args.ny, seed=11)
-    s = SevpSolver(p, tile_m=16, tile_h=16, growth_limit=1e10)
+    tm, th = (int(v) for v in args.tiles.lower().split("x"))
+    s = SevpSolver(p, tile_m=tm, tile_h=th, growth_limit=1e10)
     b = torch.from_numpy(p.b).cuda()
     _, rep = s.solve(b, precision=args.precision, max_iter=args.max_iter)
     torch.cuda.synchronize()
