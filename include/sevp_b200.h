@@ -207,8 +207,25 @@ int sevp_operator_symmetric(const sevp_ctx *ctx);
 int sevp_set_graphs(sevp_ctx *ctx, int enable);
 
 int sevp_set_full_coefficients(sevp_ctx *ctx, int force);
-/* Device bytes held by the tile influence data. */
+/* Device bytes held by the tile influence data (block-Jacobi tiling). */
 long long sevp_influence_bytes(const sevp_ctx *ctx);
+/* Overlapping Schwarz preconditioner (not part of the reference interface;
+ * the reference's BIR method, M/fs_GLOBAL.f90:1902-1966, sweeps overlapping
+ * strips with 50 % overlap as a stand-alone solver).  shift != 0 adds a
+ * second tiling, the first one rolled west by `shift` columns (shift < 0:
+ * the shift nearest tile_m / 2 whose tile edges all fall inside tiles of
+ * the first tiling), and makes every preconditioner application the
+ * symmetric multiplicative Schwarz sweep over the two tilings:
+ *   z1 = M_a r,  z2 = M_b (r - A z1),  z = z1 + z2 + M_a (r - A (z1 + z2)).
+ * The residuals are formed from the couplings across the previous tiling's
+ * boundaries.  Tiles must be at most 8 rows high.  shift = 0 returns to the
+ * block-Jacobi preconditioner.  Kept across sevp_set_operator.  Returns
+ * SEVP_BAD_ARG when no valid shift exists or the tiles are too high. */
+int sevp_set_schwarz(sevp_ctx *ctx, int shift);
+/* Column shift of the second tiling, 0 when the preconditioner is block-Jacobi. */
+int sevp_schwarz_shift(const sevp_ctx *ctx);
+/* Device bytes held by the second tiling's influence data. */
+long long sevp_schwarz_influence_bytes(const sevp_ctx *ctx);
 /* Solves A x = b (device pointers, (nx, ny) column-major FP64). */
 int sevp_solve(sevp_ctx *ctx, const double *b, double *x, const sevp_solve_opts *opts,
                sevp_report *report);
@@ -235,7 +252,8 @@ int sevp_solve_step_host(sevp_ctx *ctx, const double *b_host, const double *eta1
                          const sevp_solve_opts *opts, sevp_report *report);
 /* y = A x on the unpadded grid (device pointers). */
 int sevp_apply(sevp_ctx *ctx, const double *x, double *y);
-/* z = M^{-1} r: block-Jacobi tiles solved by SEVP marching (device). */
+/* z = M^{-1} r: tiles solved by SEVP marching (device); block-Jacobi, or the
+ * Schwarz sweep after sevp_set_schwarz. */
 int sevp_precondition(sevp_ctx *ctx, const double *r, double *z);
 /* Same in the FP32 vector format of the mixed-precision inner solve. */
 int sevp_precondition_f32(sevp_ctx *ctx, const float *r, float *z);
@@ -247,7 +265,7 @@ long long sevp_kernel_launches(const sevp_ctx *ctx);
  * enable != 0 starts (and zeroes) it.  sevp_profile_read fills ms[4] and
  * count[4] for class 0 = tile pass B (update + precondition + dots),
  * 1 = stencil passes (apply, pass A, residuals), 2 = tile precondition
- * without update, 3 = unused. */
+ * without update, 3 = Schwarz stages on boundary couplings. */
 int sevp_profile(sevp_ctx *ctx, int enable);
 int sevp_profile_read(sevp_ctx *ctx, double *ms, long long *count);
 

@@ -439,7 +439,7 @@ template <typename V, typename MT, bool UPDATE, bool DOTS, bool SYM>
 __global__ void __launch_bounds__(kTileWarps * 32, SEVP_TILE_MINB)
     k_tile_apply(TileGeom tg, Coeffs c, const MT *__restrict__ mats, V *x, const V *p, V *r,
                  const V *q, V *z, SolveState *st, double *partials, unsigned *ticket) {
-  if (DOTS && st->done) return;
+  if ((DOTS || UPDATE) && st->done) return;
   constexpr bool kChain = sizeof(V) == 4;
   extern __shared__ __align__(16) unsigned char tsm[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -461,7 +461,7 @@ __global__ void __launch_bounds__(kTileWarps * 32, SEVP_TILE_MINB)
     const bool active = n < mw;
     const int nx = tg.nx;
     const int j0 = b * tg.th, hh = tile_height(tg, b), nb = tg.grp_nb[(size_t)b * tg.txg + grp];
-    const int i = a * tg.tm + n;
+    const int i = tile_col(tg, a, n);
     const MT *mt = mats + (mw > 0 ? tg.moff[(size_t)b * tg.tx + a] : 0);
     const size_t msz = (size_t)mw * mw;
     double alpha = 0.0;
@@ -624,17 +624,197 @@ __global__ void __launch_bounds__(kTileWarps * 32, SEVP_TILE_MINB)
   }
 }
 
+// SEVP march of one task with every row in registers: the forward sweep
+// (particular solution with zero guess rows and block-top corrections) and
+// the backward sweep (guess-row values and homogeneous corrections) of
+// k_tile_apply, operation for operation.  rhs(k) gives row k's right-hand
+// side (0 for inactive lanes; called once per row k < hh, in order, by all
+// lanes of the warp); emit(k, z) receives the solution of row k of an
+// active lane as soon as its sub-block is final.  hh, nb and the sub-block bounds are the same for all
+// lanes of a warp, so the predicated rows keep the warp converged for the
+// shuffles and mat-vecs.
+template <typename MT, bool SYM, bool kChain, int HM, class Rhs, class Emit>
+__device__ __forceinline__ void march_task_regs(const float (&cc_)[HM], const float (&ce_)[HM],
+                                                const float (&cn_)[HM],
+                                                const float (&cw_)[SYM ? 1 : HM],
+                                                const float (&cs_)[SYM ? 1 : HM], int hh, int nb,
+                                                int n, int mw, bool active, int lane, int segbase,
+                                                double *dv, const MT *mt, Rhs &&rhs, Emit &&emit) {
+  const size_t msz = (size_t)mw * mw;
+  // ---- forward sweep
+  double zs[HM], rho[HM];
+  double zb = 0.0, zc = 0.0;
+  float cn_prev = 0.f;
+  int t = 0, kb = 0, ke = sub_start(1, hh, nb) - 1;
+#pragma unroll
+  for (int k = 0; k < HM; ++k) {
+    zs[k] = 0.0;
+    rho[k] = 0.0;
+    if (k < hh) {
+      double cw, cs;
+      if (SYM) {
+        const float arw = __shfl_up_sync(0xffffffffu, ce_[k], 1);
+        cw = (n == 0) ? 0.0 : (double)arw;
+        cs = (double)cn_prev;
+        cn_prev = cn_[k];
+      } else {
+        cw = cw_[k];
+        cs = cs_[k];
+      }
+      const double cc = cc_[k], ce = ce_[k];
+      const double cn = active ? (double)cn_[k] : 1.0;
+      const double rcp_k = kChain ? march_rcp(cn) : 0.0;
+      const double rk = rhs(k);
+      if (k == kb) zc = 0.0;
+      const double part = (kChain && active) ? (rk - cs * zb) - cc * zc : 0.0;
+      double zw = __shfl_up_sync(0xffffffffu, zc, 1);
+      double ze = __shfl_down_sync(0xffffffffu, zc, 1);
+      if (n == 0) zw = 0.0;
+      if (n >= mw - 1) ze = 0.0;
+      zs[k] = zc;
+      const double res = (kChain && active) ? (part - cw * zw) - ce * ze : 0.0;
+      if (k < ke) {
+        double zn;
+        if constexpr (kChain)
+          zn = res * rcp_k;
+        else
+          zn = active ? ((((rk - cw * zw) - cs * zb) - cc * zc) - ce * ze) / cn : 0.0;
+        zb = zc;
+        zc = zn;
+      } else {
+        double rh;
+        if constexpr (kChain)
+          rh = res;
+        else
+          rh = active ? (((rk - cw * zw) - cs * zb) - cc * zc) - ce * ze : 0.0;
+        rho[k] = rh;
+        if (t < nb - 1) {
+          dv[lane] = rh;
+          __syncwarp();
+          double sc = active ? seg_matvec<MT>(dv, segbase, mt + (size_t)(nb + t) * msz, mw, n) : 0.0;
+          __syncwarp();
+          zc = zc - sc;
+        }
+        zb = zc;
+        ++t;
+        kb = k + 1;
+        ke = sub_start(t + 1, hh, nb) - 1;
+      }
+    }
+  }
+  // ---- backward sweep
+  double vnext = 0.0;
+  for (t = nb - 1; t >= 0; --t) {
+    kb = sub_start(t, hh, nb);
+    ke = sub_start(t + 1, hh, nb) - 1;
+    double rho_ke = 0.0;
+    float cn_ke = 0.f, cnb = 0.f;
+#pragma unroll
+    for (int k = 0; k < HM; ++k) {
+      if (k == ke) rho_ke = rho[k], cn_ke = cn_[k];
+      if (k == kb - 1) cnb = cn_[k];
+    }
+    const double cnk = active ? (double)cn_ke : 0.0;
+    dv[lane] = rho_ke - cnk * vnext;
+    __syncwarp();
+    double v = active ? seg_matvec<MT>(dv, segbase, mt + (size_t)t * msz, mw, n) : 0.0;
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < HM; ++k)
+      if (k == kb) zs[k] += v;
+    double hb = 0.0, hc = v;
+    if (!active) cnb = 0.f;
+    if (t > 0) {
+      dv[lane] = v * (double)cnb;
+      __syncwarp();
+      hb = active ? seg_matvec<MT>(dv, segbase, mt + (size_t)(nb + t - 1) * msz, mw, n) : 0.0;
+      __syncwarp();
+    }
+    float cn_prev_b = cnb;
+#pragma unroll
+    for (int k = 0; k < HM - 1; ++k) {
+      if (k >= kb && k < ke) {
+        const float ncc = active ? cc_[k] : 0.f, nce = active ? ce_[k] : 0.f;
+        const float ncn = active ? cn_[k] : 1.f;
+        double cw, cs;
+        if (SYM) {
+          const float arw = __shfl_up_sync(0xffffffffu, nce, 1);
+          cw = (n == 0) ? 0.0 : (double)arw;
+          cs = (double)cn_prev_b;
+          cn_prev_b = ncn;
+        } else {
+          cw = active ? cw_[k] : 0.f;
+          cs = active ? cs_[k] : 0.f;
+        }
+        const double cc = ncc, ce = nce, cn = ncn;
+        const double rcp_k = kChain ? march_rcp(cn) : 0.0;
+        const double part = kChain ? -(cs * hb) - cc * hc : 0.0;
+        double hw = __shfl_up_sync(0xffffffffu, hc, 1);
+        double he = __shfl_down_sync(0xffffffffu, hc, 1);
+        if (n == 0) hw = 0.0;
+        if (n >= mw - 1) he = 0.0;
+        double hn;
+        if constexpr (kChain)
+          hn = active ? ((part - cw * hw) - ce * he) * rcp_k : 0.0;
+        else
+          hn = active ? ((((-(cw * hw)) - cs * hb) - cc * hc) - ce * he) / cn : 0.0;
+        zs[k + 1] += hn;
+        hb = hc;
+        hc = hn;
+      }
+    }
+    if (active) {
+#pragma unroll
+      for (int k = 0; k < HM; ++k)
+        if (k >= kb && k <= ke) emit(k, zs[k]);
+    }
+    vnext = v;
+  }
+}
+
+// Asynchronous copy of one 4- or 8-byte element from global to shared
+// memory (zero-filled, with no global read, when pred is false).
+template <int BYTES>
+__device__ __forceinline__ void cp_async_elem(void *smem, const void *gmem, bool pred) {
+  const unsigned dst = (unsigned)__cvta_generic_to_shared(smem);
+  const int n = pred ? BYTES : 0;
+  if constexpr (BYTES == 4)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(dst), "l"(gmem), "r"(n)
+                 : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dst), "l"(gmem), "r"(n)
+                 : "memory");
+}
+
+// Coefficient rows of one task into registers.
+template <bool SYM, int HM>
+__device__ __forceinline__ void load_task_coeffs(const Coeffs &c, size_t idx0, int nx, int hh,
+                                                 bool active, float (&cc_)[HM], float (&ce_)[HM],
+                                                 float (&cn_)[HM], float (&cw_)[SYM ? 1 : HM],
+                                                 float (&cs_)[SYM ? 1 : HM]) {
+#pragma unroll
+  for (int k = 0; k < HM; ++k) {
+    const bool ok = active && k < hh;
+    const size_t id = ok ? idx0 + (size_t)k * nx : 0;
+    cc_[k] = ok ? __ldg(c.ac + id) : 0.f;
+    ce_[k] = ok ? __ldg(c.ar + id) : 0.f;
+    cn_[k] = ok ? __ldg(c.at + id) : 0.f;
+    if (!SYM) {
+      cw_[k] = ok ? __ldg(c.al + id) : 0.f;
+      cs_[k] = ok ? __ldg(c.ab + id) : 0.f;
+    }
+  }
+}
+
 // Tiles of at most HM rows (the short tiles the autotuner prefers): the same
-// algorithm as k_tile_apply, operation for operation, with every row of a
-// task loaded into registers at once (one memory round trip per task
-// instead of one per row) and the rows unrolled.  hh, nb and the sub-block
-// bounds are the same for all lanes of a warp, so the predicated rows keep
-// the warp converged for the shuffles and mat-vecs.
+// algorithm as k_tile_apply, with every row of a task loaded into registers
+// at once (one memory round trip per task instead of one per row) and the
+// rows unrolled.
 template <typename V, typename MT, bool UPDATE, bool DOTS, bool SYM, int HM>
 __global__ void __launch_bounds__(kTileWarps * 32, 2)
     k_tile_short(TileGeom tg, Coeffs c, const MT *__restrict__ mats, V *x, const V *p, V *r,
                  const V *q, V *z, SolveState *st, double *partials, unsigned *ticket) {
-  if (DOTS && st->done) return;
+  if ((DOTS || UPDATE) && st->done) return;
   constexpr bool kChain = sizeof(V) == 4;
   __shared__ double dv_all[kTileWarps * 32];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -652,9 +832,8 @@ __global__ void __launch_bounds__(kTileWarps * 32, 2)
     const bool active = n < mw;
     const int nx = tg.nx;
     const int j0 = b * tg.th, hh = tile_height(tg, b), nb = tg.grp_nb[(size_t)b * tg.txg + grp];
-    const int i = a * tg.tm + n;
+    const int i = tile_col(tg, a, n);
     const MT *mt = mats + (mw > 0 ? tg.moff[(size_t)b * tg.tx + a] : 0);
-    const size_t msz = (size_t)mw * mw;
     const size_t idx0 = (size_t)j0 * nx + i;
 
     // ---- all loads of the task
@@ -670,163 +849,155 @@ __global__ void __launch_bounds__(kTileWarps * 32, 2)
         pp[k] = ok ? p[id] : V(0);
         qq[k] = ok ? q[id] : V(0);
       }
-      cc_[k] = ok ? __ldg(c.ac + id) : 0.f;
-      ce_[k] = ok ? __ldg(c.ar + id) : 0.f;
-      cn_[k] = ok ? __ldg(c.at + id) : 0.f;
-      if (!SYM) {
-        cw_[k] = ok ? __ldg(c.al + id) : 0.f;
-        cs_[k] = ok ? __ldg(c.ab + id) : 0.f;
-      }
     }
+    load_task_coeffs<SYM, HM>(c, idx0, nx, hh, active, cc_, ce_, cn_, cw_, cs_);
 
-    // ---- forward sweep (as k_tile_apply)
-    double zs[HM], rho[HM];
-    double zb = 0.0, zc = 0.0;
-    float cn_prev = 0.f;
-    int t = 0, kb = 0, ke = sub_start(1, hh, nb) - 1;
-#pragma unroll
-    for (int k = 0; k < HM; ++k) {
-      zs[k] = 0.0;
-      rho[k] = 0.0;
-      if (k < hh) {
-        double rv = 0.0;
-        double cw, cs;
-        if (SYM) {
-          const float arw = __shfl_up_sync(0xffffffffu, ce_[k], 1);
-          cw = (n == 0) ? 0.0 : (double)arw;
-          cs = (double)cn_prev;
-          cn_prev = cn_[k];
-        } else {
-          cw = cw_[k];
-          cs = cs_[k];
-        }
-        const double cc = cc_[k], ce = ce_[k];
-        const double cn = active ? (double)cn_[k] : 1.0;
-        const double rcp_k = kChain ? march_rcp(cn) : 0.0;
-        if (active) {
-          if (UPDATE) {
-            const size_t idx = idx0 + (size_t)k * nx;
-            const V xn = xx[k] + (V)alpha * pp[k];
-            const V rn = rr[k] - (V)alpha * qq[k];
-            x[idx] = xn;
-            r[idx] = rn;
-            rr[k] = rn;
-          }
-          rv = (double)rr[k];
-          acc_rr += rv * rv;
-        }
-        if (k == kb) zc = 0.0;
-        const double part = (kChain && active) ? (rv - cs * zb) - cc * zc : 0.0;
-        double zw = __shfl_up_sync(0xffffffffu, zc, 1);
-        double ze = __shfl_down_sync(0xffffffffu, zc, 1);
-        if (n == 0) zw = 0.0;
-        if (n >= mw - 1) ze = 0.0;
-        zs[k] = zc;
-        const double res = (kChain && active) ? (part - cw * zw) - ce * ze : 0.0;
-        if (k < ke) {
-          double zn;
-          if constexpr (kChain)
-            zn = res * rcp_k;
-          else
-            zn = active ? ((((rv - cw * zw) - cs * zb) - cc * zc) - ce * ze) / cn : 0.0;
-          zb = zc;
-          zc = zn;
-        } else {
-          double rh;
-          if constexpr (kChain)
-            rh = res;
-          else
-            rh = active ? (((rv - cw * zw) - cs * zb) - cc * zc) - ce * ze : 0.0;
-          rho[k] = rh;
-          if (t < nb - 1) {
-            dv[lane] = rh;
-            __syncwarp();
-            double sc = active ? seg_matvec<MT>(dv, segbase, mt + (size_t)(nb + t) * msz, mw, n) : 0.0;
-            __syncwarp();
-            zc = zc - sc;
-          }
-          zb = zc;
-          ++t;
-          kb = k + 1;
-          ke = sub_start(t + 1, hh, nb) - 1;
-        }
+    // row k's right-hand side: the residual, after the fused update
+    // x += alpha p, r -= alpha q
+    auto rhs = [&](int k) -> double {
+      if (!active) return 0.0;
+      if (UPDATE) {
+        const size_t idx = idx0 + (size_t)k * nx;
+        const V xn = xx[k] + (V)alpha * pp[k];
+        const V rn = rr[k] - (V)alpha * qq[k];
+        x[idx] = xn;
+        r[idx] = rn;
+        rr[k] = rn;
       }
-    }
-    // ---- backward sweep (as k_tile_apply)
-    double vnext = 0.0;
-    for (t = nb - 1; t >= 0; --t) {
-      kb = sub_start(t, hh, nb);
-      ke = sub_start(t + 1, hh, nb) - 1;
-      double rho_ke = 0.0;
-      float cn_ke = 0.f, cnb = 0.f;
-#pragma unroll
-      for (int k = 0; k < HM; ++k) {
-        if (k == ke) rho_ke = rho[k], cn_ke = cn_[k];
-        if (k == kb - 1) cnb = cn_[k];
-      }
-      const double cnk = active ? (double)cn_ke : 0.0;
-      dv[lane] = rho_ke - cnk * vnext;
-      __syncwarp();
-      double v = active ? seg_matvec<MT>(dv, segbase, mt + (size_t)t * msz, mw, n) : 0.0;
-      __syncwarp();
-#pragma unroll
-      for (int k = 0; k < HM; ++k)
-        if (k == kb) zs[k] += v;
-      double hb = 0.0, hc = v;
-      if (!active) cnb = 0.f;
-      if (t > 0) {
-        dv[lane] = v * (double)cnb;
-        __syncwarp();
-        hb = active ? seg_matvec<MT>(dv, segbase, mt + (size_t)(nb + t - 1) * msz, mw, n) : 0.0;
-        __syncwarp();
-      }
-      float cn_prev_b = cnb;
-#pragma unroll
-      for (int k = 0; k < HM - 1; ++k) {
-        if (k >= kb && k < ke) {
-          const float ncc = active ? cc_[k] : 0.f, nce = active ? ce_[k] : 0.f;
-          const float ncn = active ? cn_[k] : 1.f;
-          double cw, cs;
-          if (SYM) {
-            const float arw = __shfl_up_sync(0xffffffffu, nce, 1);
-            cw = (n == 0) ? 0.0 : (double)arw;
-            cs = (double)cn_prev_b;
-            cn_prev_b = ncn;
-          } else {
-            cw = active ? cw_[k] : 0.f;
-            cs = active ? cs_[k] : 0.f;
-          }
-          const double cc = ncc, ce = nce, cn = ncn;
-          const double rcp_k = kChain ? march_rcp(cn) : 0.0;
-          const double part = kChain ? -(cs * hb) - cc * hc : 0.0;
-          double hw = __shfl_up_sync(0xffffffffu, hc, 1);
-          double he = __shfl_down_sync(0xffffffffu, hc, 1);
-          if (n == 0) hw = 0.0;
-          if (n >= mw - 1) he = 0.0;
-          double hn;
-          if constexpr (kChain)
-            hn = active ? ((part - cw * hw) - ce * he) * rcp_k : 0.0;
-          else
-            hn = active ? ((((-(cw * hw)) - cs * hb) - cc * hc) - ce * he) / cn : 0.0;
-          zs[k + 1] += hn;
-          hb = hc;
-          hc = hn;
-        }
-      }
-      if (active) {
-#pragma unroll
-        for (int k = 0; k < HM; ++k) {
-          if (k >= kb && k <= ke) {
-            const V zv = (V)zs[k];
-            z[idx0 + (size_t)k * nx] = zv;
-            if (DOTS) acc_rz += (double)rr[k] * (double)zv;
-          }
-        }
-      }
-      vnext = v;
-    }
+      const double rv = (double)rr[k];
+      acc_rr += rv * rv;
+      return rv;
+    };
+    auto emit = [&](int k, double zk) {
+      const V zv = (V)zk;
+      z[idx0 + (size_t)k * nx] = zv;
+      if (DOTS) acc_rz += (double)rr[k] * (double)zv;
+    };
+    march_task_regs<MT, SYM, kChain, HM>(cc_, ce_, cn_, cw_, cs_, hh, nb, n, mw, active, lane,
+                                         segbase, dv, mt, rhs, emit);
   }
   if (DOTS) {
+    double v2[2] = {acc_rz, acc_rr};
+    TileFin fin{st};
+    reduce_and_finish<2>(v2, partials, ticket, fin);
+  }
+}
+
+// One stage of the overlapping (two-tiling, symmetric multiplicative)
+// Schwarz preconditioner on the tiling tg.  The stage's right-hand side is
+// the residual left by the previous stage, r - A z_prev; because the
+// previous stage solved its own tiles exactly, that residual is minus the
+// couplings of its correction w across the boundaries of the previous
+// stage's tiling (column shift xo): west/east neighbours inside this tile
+// come by shuffle (the two tilings' column boundaries never coincide), and
+// the tile rows' halo neighbours south and north are loaded.  The tile
+// solves then run as in k_tile_short.
+// MODE 0: out = M rhs.  MODE 1: out = base + w + M rhs.  MODE 2: as 1,
+// plus r.z and r.r and the finish of the PCG iteration (TileFin).
+// st may be null outside a PCG loop (MODE 0 and 1); in the loop a finished
+// solve skips the stage.
+template <typename V, typename MT, bool SYM, int HM, int MODE>
+__global__ void __launch_bounds__(kTileWarps * 32, 2)
+    k_tile_couple(TileGeom tg, int xo, int periodic, Coeffs c, const MT *__restrict__ mats,
+                  const V *w, const V *base, const V *r, V *out, SolveState *st,
+                  double *partials, unsigned *ticket) {
+  if (st && st->done) return;
+  constexpr bool kChain = sizeof(V) == 4;
+  // base and residual rows of the final stage, staged by cp.async (one
+  // slot per lane and row, read back only by the lane that copied it)
+  constexpr int kStage = MODE == 2 ? 2 : (MODE == 1 ? 1 : 0);
+  __shared__ double dv_all[kTileWarps * 32];
+  __shared__ __align__(16) V stg_all[kStage ? kTileWarps * kStage * HM * 32 : 1];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  double *dv = dv_all + wib * 32;
+  V *stg = stg_all + (kStage ? wib * kStage * HM * 32 : 0);
+  double acc_rz = 0.0, acc_rr = 0.0;
+  const int ntasks = tg.ty * tg.txg;
+  for (int gw = blockIdx.x * kTileWarps + wib; gw < ntasks; gw += gridDim.x * kTileWarps) {
+    const int b = gw / tg.txg;
+    const int grp = gw - b * tg.txg;
+    const int seg = lane / tg.wseg, n = lane - seg * tg.wseg, segbase = seg * tg.wseg;
+    const int a = grp * tg.tpw + seg;
+    const int mw = (a < tg.tx) ? tile_width(tg, a) : 0;
+    const bool active = n < mw;
+    const int nx = tg.nx;
+    const int j0 = b * tg.th, hh = tile_height(tg, b), nb = tg.grp_nb[(size_t)b * tg.txg + grp];
+    const int i = tile_col(tg, a, n);
+    const MT *mt = mats + (mw > 0 ? tg.moff[(size_t)b * tg.tx + a] : 0);
+    const size_t idx0 = (size_t)j0 * nx + i;
+    if constexpr (kStage > 0) {
+#pragma unroll
+      for (int k = 0; k < HM; ++k) {
+        const bool ok = active && k < hh;
+        const size_t id = ok ? idx0 + (size_t)k * nx : 0;
+        cp_async_elem<sizeof(V)>(stg + k * 32 + lane, base + id, ok);
+        if constexpr (kStage == 2) cp_async_elem<sizeof(V)>(stg + (HM + k) * 32 + lane, r + id, ok);
+      }
+      asm volatile("cp.async.commit_group;\n" ::: "memory");
+    }
+    // boundaries of the previous stage's tiling at this column
+    int qc = i - xo;
+    if (qc < 0) qc += nx;
+    bool wb = active && qc % tg.tm == 0;
+    bool eb = active && ((qc + 1) % tg.tm == 0 || qc == nx - 1);
+    if (!periodic && i == 0) wb = false;
+    if (!periodic && i == nx - 1) eb = false;
+    const bool has_s = active && j0 > 0, has_n = active && j0 + hh < tg.ny;
+
+    // ---- loads: w rows and halo rows, coefficients
+    V wv[HM];
+#pragma unroll
+    for (int k = 0; k < HM; ++k) {
+      const bool ok = active && k < hh;
+      wv[k] = ok ? w[idx0 + (size_t)k * nx] : V(0);
+    }
+    const V ws = has_s ? w[idx0 - nx] : V(0);
+    const V wn = has_n ? w[idx0 + (size_t)hh * nx] : V(0);
+    float cc_[HM], ce_[HM], cn_[HM], cw_[SYM ? 1 : HM], cs_[SYM ? 1 : HM];
+    load_task_coeffs<SYM, HM>(c, idx0, nx, hh, active, cc_, ce_, cn_, cw_, cs_);
+    // AB of the tile's first row: the row below's AT when symmetric
+    float ab0;
+    if constexpr (SYM)
+      ab0 = has_s ? __ldg(c.at + idx0 - nx) : 0.f;
+    else
+      ab0 = cs_[0];
+
+    // row k's right-hand side: minus the couplings of w across the previous
+    // tiling's boundaries (the shuffles run on all lanes)
+    auto rhs = [&](int k) -> double {
+      const double wwv = __shfl_up_sync(0xffffffffu, (double)wv[k], 1);
+      const double wev = __shfl_down_sync(0xffffffffu, (double)wv[k], 1);
+      float alv;
+      if constexpr (SYM)
+        alv = __shfl_up_sync(0xffffffffu, ce_[k], 1);
+      else
+        alv = cw_[k];
+      double v = 0.0;
+      if (wb) v -= (double)alv * wwv;
+      if (eb) v -= (double)ce_[k] * wev;
+      if (k == 0 && has_s) v -= (double)ab0 * (double)ws;
+      if (k == hh - 1 && has_n) v -= (double)cn_[k] * (double)wn;
+      return active ? v : 0.0;
+    };
+    if constexpr (kStage > 0) asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    auto emit = [&](int k, double zk) {
+      const size_t id = idx0 + (size_t)k * nx;
+      if constexpr (MODE == 0) {
+        out[id] = (V)zk;
+      } else {
+        const V zv = (V)(((double)stg[k * 32 + lane] + (double)wv[k]) + zk);
+        out[id] = zv;
+        if constexpr (MODE == 2) {
+          const double rr = (double)stg[(HM + k) * 32 + lane];
+          acc_rz += rr * (double)zv;
+          acc_rr += rr * rr;
+        }
+      }
+    };
+    march_task_regs<MT, SYM, kChain, HM>(cc_, ce_, cn_, cw_, cs_, hh, nb, n, mw, active, lane,
+                                         segbase, dv, mt, rhs, emit);
+  }
+  if constexpr (MODE == 2) {
     double v2[2] = {acc_rz, acc_rr};
     TileFin fin{st};
     reduce_and_finish<2>(v2, partials, ticket, fin);
@@ -852,7 +1023,7 @@ __global__ void k_tile_growth(TileGeom tg, Coeffs c, double log_growth, int *s_t
   bool bad = false;
   for (int e = lane; e < mw * (hh - 1); e += 32) {
     const int k = e / mw, n = e % mw;
-    const size_t idx = (size_t)(b * tg.th + k) * tg.nx + a * tg.tm + n;
+    const size_t idx = (size_t)(b * tg.th + k) * tg.nx + tile_col(tg, a, n);
     double at = fabs((double)c.at[idx]);
     double num = fabs((double)c.ac[idx]) + fabs((double)c.al[idx]) + fabs((double)c.ar[idx]);
     if (at == 0.0) bad = true;
@@ -886,7 +1057,7 @@ __global__ void __launch_bounds__(1024)
   const int a = tile % tg.tx, b = tile / tg.tx;
   const int mw = tile_width(tg, a), hh = tile_height(tg, b);
   const int nb = tg.grp_nb[(size_t)b * tg.txg + a / tg.tpw];
-  const int i0 = a * tg.tm, j0 = b * tg.th;
+  const int j0 = b * tg.th;
   const int lane = threadIdx.x & 31, g = threadIdx.x >> 5;
   const int TM = 32;
   float *cf = (float *)psm;  // [5][hmax][32]
@@ -904,7 +1075,8 @@ __global__ void __launch_bounds__(1024)
     int k = e / TM, n = e % TM;
     float w = 0.f, s = 0.f, cc = 0.f, ee = 0.f, nn = 0.f;
     if (n < mw) {
-      size_t idx = (size_t)(j0 + k) * tg.nx + i0 + n;
+      const int col = tile_col(tg, a, n);
+      size_t idx = (size_t)(j0 + k) * tg.nx + col;
       w = c.al[idx], s = c.ab[idx], cc = c.ac[idx], ee = c.ar[idx], nn = c.at[idx];
     }
     cf[(0 * hm + k) * TM + n] = w;
@@ -1026,24 +1198,52 @@ __global__ void __launch_bounds__(1024)
 // ======================================================================
 using namespace sevp;
 
+// One tile set of the preconditioner: geometry, sub-block counts per warp
+// group and per tile, and the influence data (FP64, plus an FP32 copy built
+// on demand for the mixed solve's inner iterations).
+struct Tiling {
+  TileGeom tg{};
+  Coeffs c{};                   // the planes its kernels read
+  float *d_al = nullptr, *d_ar = nullptr;  // seam-cut AL/AR copies (closed grids, shifted tiling)
+  int *d_grp_nb = nullptr;
+  long long *d_moff = nullptr;
+  double *d_mats = nullptr;
+  float *d_mats32 = nullptr;
+  long long mats_elems = 0;
+  std::vector<int> grp_nb;   // per warp group (ty * txg)
+  std::vector<int> tile_nb;  // effective sub-blocks per tile (ty * tx)
+  bool built = false;
+  void release() {
+    for (void *p : {(void *)d_grp_nb, (void *)d_moff, (void *)d_mats, (void *)d_mats32,
+                    (void *)d_al, (void *)d_ar})
+      if (p) cudaFree(p);
+    d_grp_nb = nullptr, d_moff = nullptr, d_mats = nullptr, d_mats32 = nullptr;
+    d_al = nullptr, d_ar = nullptr;
+    mats_elems = 0;
+    built = false;
+  }
+};
+
 struct sevp_ctx {
   int nx = 0, ny = 0, periodic = 0;
   int device = 0;
   cudaStream_t stream = nullptr;
   Coeffs c{};
   bool have_op = false;
-  // tiles
-  TileGeom tg{};
-  int *d_grp_nb = nullptr;
+  // tiles: ta is the block-Jacobi tiling; tb the shifted second tiling of
+  // the overlapping Schwarz preconditioner (built when schwarz_req != 0)
+  Tiling ta, tb;
   int sym = 0;                  // operator exactly symmetric: 3-plane kernels
   int force_full = 0;           // use the 5-plane kernels regardless
-  float *d_mats32 = nullptr;    // FP32 copy of the influence data (built on demand)
-  bool infl32_active = false;   // current solve uses d_mats32 for FP32 vectors
-  long long *d_moff = nullptr;
-  double *d_mats = nullptr;
-  long long mats_elems = 0;
-  std::vector<int> grp_nb;   // per warp group (ty * txg)
-  std::vector<int> tile_nb;  // effective sub-blocks per tile (ty * tx)
+  bool infl32_active = false;   // current solve uses the FP32 influence copies
+  // the tiling request of the last sevp_set_operator (the second tiling is
+  // built from it)
+  sevp_tiling treq{};
+  std::vector<int> treq_rows, treq_tiles;
+  int schwarz_req = 0;  // requested column shift of tb: 0 off, -1 automatic
+  // Schwarz work vectors: first-stage z and second-stage correction
+  double *s1_64 = nullptr, *s2_64 = nullptr;
+  float *s1_32 = nullptr, *s2_32 = nullptr;
   // work vectors
   size_t n = 0;
   double *r64 = nullptr, *z64 = nullptr, *p64[2] = {nullptr, nullptr}, *q64 = nullptr;
@@ -1074,7 +1274,7 @@ struct sevp_ctx {
   cudaStream_t cap_stream = nullptr;
   cudaGraphExec_t inner_graph = nullptr;
   int inner_graph_ce = 0;
-  const void *inner_graph_key[3] = {nullptr, nullptr, nullptr};
+  const void *inner_graph_key[4] = {nullptr, nullptr, nullptr, nullptr};
   // optional per-kernel-class timing (CUDA events on the context stream)
   int prof = 0;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pool;
@@ -1177,32 +1377,41 @@ static int launch_stencil(sevp_ctx *ctx, const Op &op, int ticket_slot) {
   return SEVP_OK;
 }
 
+// Resident CTAs of a kernel on the current device at the given shared
+// memory (queried once per kernel and size; one device per process is
+// assumed).
+template <typename K>
+static int resident_ctas(K kern, size_t smem, size_t &set_smem, int &slots) {
+  if (slots > 0 && set_smem == smem) return SEVP_OK;
+  // static plus dynamic shared memory above 48 KB needs the opt-in
+  if (smem > 0)
+    SEVP_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0, dev = 0, sms = 0;
+  SEVP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTileWarps * 32, smem));
+  SEVP_CUDA_TRY(cudaGetDevice(&dev));
+  SEVP_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  slots = std::max(1, per_sm) * sms;
+  set_smem = smem;
+  return SEVP_OK;
+}
+
 template <typename V, typename MT, bool UPDATE, bool DOTS, bool SYM>
-static int launch_tile_k(sevp_ctx *ctx, const MT *mats, V *x, const V *p, V *r, const V *q, V *z,
-                         int ticket_slot) {
-  const size_t warps = tile_warps(ctx->tg);
-  const bool short_tiles = sizeof(V) == 4 && ctx->tg.hmax <= kShortTileRows;
-  const size_t smem = short_tiles ? 0 : tile_smem_per_warp(ctx->tg.hmax) * kTileWarps;
+static int launch_tile_k(sevp_ctx *ctx, const Tiling &T, const MT *mats, V *x, const V *p, V *r,
+                         const V *q, V *z, int ticket_slot) {
+  const size_t warps = tile_warps(T.tg);
+  const bool short_tiles = sizeof(V) == 4 && T.tg.hmax <= kShortTileRows;
+  const size_t smem = short_tiles ? 0 : tile_smem_per_warp(T.tg.hmax) * kTileWarps;
   auto kern = short_tiles ? k_tile_short<V, MT, UPDATE, DOTS, SYM, kShortTileRows>
                           : k_tile_apply<V, MT, UPDATE, DOTS, SYM>;
-  static size_t set_smem = 0;  // per instantiation (one device per process is assumed)
-  static int slots = 0;         // resident CTAs on the device at set_smem
-  static int set_short = -1;
-  if (set_smem != smem || set_short != (int)short_tiles) {
-    set_short = (int)short_tiles;
-    if (smem > 48 * 1024)
-      SEVP_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int per_sm = 0, dev = 0, sms = 0;
-    SEVP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTileWarps * 32, smem));
-    SEVP_CUDA_TRY(cudaGetDevice(&dev));
-    SEVP_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    slots = std::max(1, per_sm) * sms;
-    set_smem = smem;
-  }
-  const unsigned blocks =
-      (unsigned)std::min<size_t>((warps + kTileWarps - 1) / kTileWarps, (size_t)slots);
+  // per instantiation and kernel choice
+  static size_t set_smem[2] = {0, 0};
+  static int slots[2] = {0, 0};
+  int s = resident_ctas(kern, smem, set_smem[short_tiles], slots[short_tiles]);
+  if (s) return s;
+  const unsigned blocks = (unsigned)std::min<size_t>((warps + kTileWarps - 1) / kTileWarps,
+                                                     (size_t)slots[short_tiles]);
   ProfScope ps(ctx, UPDATE ? 0 : 2);
-  kern<<<blocks, kTileWarps * 32, smem, ctx->stream>>>(ctx->tg, ctx->c, mats, x, p, r, q, z, ctx->st,
+  kern<<<blocks, kTileWarps * 32, smem, ctx->stream>>>(T.tg, T.c, mats, x, p, r, q, z, ctx->st,
                                                       ctx->partials, ctx->tickets + ticket_slot);
   ctx->launches++;
   SEVP_CUDA_TRY(cudaGetLastError());
@@ -1212,17 +1421,96 @@ static int launch_tile_k(sevp_ctx *ctx, const MT *mats, V *x, const V *p, V *r, 
 // Dispatch: symmetric-coefficient variant when the operator is symmetric;
 // FP32 influence matrices only for FP32 vectors when the solve asks for them.
 template <typename V, bool UPDATE, bool DOTS>
-static int launch_tile(sevp_ctx *ctx, V *x, const V *p, V *r, const V *q, V *z, int ticket_slot) {
+static int launch_tile(sevp_ctx *ctx, const Tiling &T, V *x, const V *p, V *r, const V *q, V *z,
+                       int ticket_slot) {
   if constexpr (sizeof(V) == 4) {
-    if (ctx->infl32_active && ctx->d_mats32) {
+    if (ctx->infl32_active && T.d_mats32) {
       if (ctx->sym)
-        return launch_tile_k<V, float, UPDATE, DOTS, true>(ctx, ctx->d_mats32, x, p, r, q, z, ticket_slot);
-      return launch_tile_k<V, float, UPDATE, DOTS, false>(ctx, ctx->d_mats32, x, p, r, q, z, ticket_slot);
+        return launch_tile_k<V, float, UPDATE, DOTS, true>(ctx, T, T.d_mats32, x, p, r, q, z, ticket_slot);
+      return launch_tile_k<V, float, UPDATE, DOTS, false>(ctx, T, T.d_mats32, x, p, r, q, z, ticket_slot);
     }
   }
   if (ctx->sym)
-    return launch_tile_k<V, double, UPDATE, DOTS, true>(ctx, ctx->d_mats, x, p, r, q, z, ticket_slot);
-  return launch_tile_k<V, double, UPDATE, DOTS, false>(ctx, ctx->d_mats, x, p, r, q, z, ticket_slot);
+    return launch_tile_k<V, double, UPDATE, DOTS, true>(ctx, T, T.d_mats, x, p, r, q, z, ticket_slot);
+  return launch_tile_k<V, double, UPDATE, DOTS, false>(ctx, T, T.d_mats, x, p, r, q, z, ticket_slot);
+}
+
+// Tile rows the Schwarz stage kernel holds in registers.
+constexpr int kCoupleMaxRows = 8;
+
+template <typename V, typename MT, bool SYM, int HM, int MODE>
+static int launch_couple_k(sevp_ctx *ctx, const Tiling &T, int xo, const MT *mats, const V *w,
+                           const V *base, const V *r, V *out, SolveState *st, int ticket_slot) {
+  auto kern = k_tile_couple<V, MT, SYM, HM, MODE>;
+  static size_t set_smem = 0;
+  static int slots = 0;
+  int s = resident_ctas(kern, 0, set_smem, slots);
+  if (s) return s;
+  const size_t warps = tile_warps(T.tg);
+  const unsigned blocks =
+      (unsigned)std::min<size_t>((warps + kTileWarps - 1) / kTileWarps, (size_t)slots);
+  ProfScope ps(ctx, 3);
+  kern<<<blocks, kTileWarps * 32, 0, ctx->stream>>>(T.tg, xo, ctx->periodic, T.c, mats, w, base,
+                                                   r, out, st, ctx->partials,
+                                                   ctx->tickets + ticket_slot);
+  ctx->launches++;
+  SEVP_CUDA_TRY(cudaGetLastError());
+  return SEVP_OK;
+}
+
+template <typename V, typename MT, bool SYM, int MODE>
+static int launch_couple_h(sevp_ctx *ctx, const Tiling &T, int xo, const MT *mats, const V *w,
+                           const V *base, const V *r, V *out, SolveState *st, int ticket_slot) {
+  if (T.tg.hmax <= 6)
+    return launch_couple_k<V, MT, SYM, 6, MODE>(ctx, T, xo, mats, w, base, r, out, st, ticket_slot);
+  return launch_couple_k<V, MT, SYM, kCoupleMaxRows, MODE>(ctx, T, xo, mats, w, base, r, out, st,
+                                                           ticket_slot);
+}
+
+// One Schwarz stage on tiling T after a stage on the tiling with column
+// shift xo (see k_tile_couple for MODE).
+template <typename V, int MODE>
+static int launch_couple(sevp_ctx *ctx, const Tiling &T, int xo, const V *w, const V *base,
+                         const V *r, V *out, SolveState *st, int ticket_slot) {
+  if constexpr (sizeof(V) == 4) {
+    if (ctx->infl32_active && T.d_mats32) {
+      if (ctx->sym)
+        return launch_couple_h<V, float, true, MODE>(ctx, T, xo, T.d_mats32, w, base, r, out, st, ticket_slot);
+      return launch_couple_h<V, float, false, MODE>(ctx, T, xo, T.d_mats32, w, base, r, out, st, ticket_slot);
+    }
+  }
+  if (ctx->sym)
+    return launch_couple_h<V, double, true, MODE>(ctx, T, xo, T.d_mats, w, base, r, out, st, ticket_slot);
+  return launch_couple_h<V, double, false, MODE>(ctx, T, xo, T.d_mats, w, base, r, out, st, ticket_slot);
+}
+
+static bool schwarz_on(const sevp_ctx *ctx) { return ctx->schwarz_req != 0 && ctx->tb.built; }
+
+template <typename V>
+static void schwarz_bufs(sevp_ctx *ctx, V *&s1, V *&s2) {
+  if constexpr (sizeof(V) == 4)
+    s1 = ctx->s1_32, s2 = ctx->s2_32;
+  else
+    s1 = ctx->s1_64, s2 = ctx->s2_64;
+}
+
+// z = M^-1 r with the preconditioner the context is set to.  UPDATE fuses
+// x += alpha p, r -= alpha q before it (PCG pass B); DOTS accumulates r.z
+// and r.r and finishes the iteration on the device.  With the Schwarz
+// preconditioner: z1 = M_a r, z2 = M_b (r - A z1), z = z1 + z2 + M_a (r -
+// A (z1 + z2)), the residuals formed from the tile-boundary couplings.
+template <typename V, bool UPDATE, bool DOTS>
+static int precondition_pass(sevp_ctx *ctx, V *x, const V *p, V *r, const V *q, V *z) {
+  if (!schwarz_on(ctx)) return launch_tile<V, UPDATE, DOTS>(ctx, ctx->ta, x, p, r, q, z, 4);
+  V *s1, *s2;
+  schwarz_bufs(ctx, s1, s2);
+  int s = launch_tile<V, UPDATE, false>(ctx, ctx->ta, x, p, r, q, s1, 4);
+  if (s) return s;
+  SolveState *st = DOTS ? ctx->st : nullptr;
+  s = launch_couple<V, 0>(ctx, ctx->tb, ctx->ta.tg.xs, s1, nullptr, nullptr, s2, st, 4);
+  if (s) return s;
+  if (DOTS) return launch_couple<V, 2>(ctx, ctx->ta, ctx->tb.tg.xs, s2, s1, r, z, ctx->st, 4);
+  return launch_couple<V, 1>(ctx, ctx->ta, ctx->tb.tg.xs, s2, s1, nullptr, z, nullptr, 4);
 }
 
 // Folds recorded event pairs into per-class totals (synchronises the stream).
@@ -1258,11 +1546,12 @@ extern "C" int sevp_profile_read(sevp_ctx *ctx, double *ms, long long *count) {
 static void free_work(sevp_ctx *ctx) {
   void *ptrs[] = {ctx->r64, ctx->z64, ctx->p64[0], ctx->p64[1], ctx->q64, ctx->x64s, ctx->r32,
                   ctx->z32, ctx->p32[0], ctx->p32[1], ctx->q32, ctx->d32, ctx->bh, ctx->xh,
-                  ctx->e1h, ctx->e2h,
-                  ctx->d_grp_nb, ctx->d_moff, ctx->d_mats, ctx->st, ctx->partials, ctx->tickets,
-                  ctx->d_mats32};
+                  ctx->e1h, ctx->e2h, ctx->st, ctx->partials, ctx->tickets,
+                  ctx->s1_64, ctx->s2_64, ctx->s1_32, ctx->s2_32};
   for (void *p : ptrs)
     if (p) cudaFree(p);
+  ctx->ta.release();
+  ctx->tb.release();
   if (ctx->h_st) cudaFreeHost(ctx->h_st);
   for (auto &pr : ctx->ev_pool) cudaEventDestroy(pr.first), cudaEventDestroy(pr.second);
   ctx->ev_pool.clear();
@@ -1360,14 +1649,189 @@ extern "C" int sevp_set_full_coefficients(sevp_ctx *ctx, int force) {
 
 extern "C" int sevp_tile_layout(const sevp_ctx *ctx, int *tiles_x, int *tiles_y, int *nb_per_tile) {
   if (!ctx || !ctx->have_op || !tiles_x || !tiles_y) return SEVP_BAD_ARG;
-  *tiles_x = ctx->tg.tx;
-  *tiles_y = ctx->tg.ty;
+  *tiles_x = ctx->ta.tg.tx;
+  *tiles_y = ctx->ta.tg.ty;
   if (nb_per_tile)
-    for (size_t t = 0; t < ctx->tile_nb.size(); ++t) nb_per_tile[t] = ctx->tile_nb[t];
+    for (size_t t = 0; t < ctx->ta.tile_nb.size(); ++t) nb_per_tile[t] = ctx->ta.tile_nb[t];
   return SEVP_OK;
 }
 extern "C" long long sevp_influence_bytes(const sevp_ctx *ctx) {
-  return ctx ? ctx->mats_elems * 8 : 0;
+  return ctx ? ctx->ta.mats_elems * 8 : 0;
+}
+
+// Builds tile set T with column shift xs from the context's tiling request:
+// sub-block heights per tile (explicit, per tile row, or from the marching
+// growth bound measured on the device), warp-group counts, the influence
+// data layout, and the influence data (k_tile_precompute).
+static int build_tiling(sevp_ctx *ctx, Tiling &T, int xs) {
+  const sevp_tiling *tl = &ctx->treq;
+  const int tm = tl->tile_m, th = tl->tile_h;
+  T.release();
+  TileGeom &tg = T.tg;
+  tg = TileGeom{};
+  tg.nx = ctx->nx, tg.ny = ctx->ny, tg.tm = tm, tg.th = th;
+  tg.tx = ceil_div(ctx->nx, tm);
+  tg.ty = ceil_div(ctx->ny, th);
+  tg.wseg = tm <= 8 ? 8 : (tm <= 16 ? 16 : 32);
+  tg.tpw = 32 / tg.wseg;
+  tg.txg = ceil_div(tg.tx, tg.tpw);
+  tg.hmax = th;
+  tg.xs = xs;
+  T.c = ctx->c;
+  if (xs != 0 && !ctx->periodic) {
+    // closed grid: the shifted tiling's wrapped tile must not couple
+    // column nx-1 to column 0
+    const size_t bytes = ctx->n * sizeof(float);
+    SEVP_CUDA_TRY(cudaMalloc((void **)&T.d_al, bytes));
+    SEVP_CUDA_TRY(cudaMalloc((void **)&T.d_ar, bytes));
+    SEVP_CUDA_TRY(cudaMemcpyAsync(T.d_al, ctx->c.al, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    SEVP_CUDA_TRY(cudaMemcpyAsync(T.d_ar, ctx->c.ar, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    const size_t pitch = (size_t)ctx->nx * sizeof(float);
+    SEVP_CUDA_TRY(cudaMemset2DAsync(T.d_al, pitch, 0, sizeof(float), ctx->ny, ctx->stream));
+    SEVP_CUDA_TRY(cudaMemset2DAsync(T.d_ar + (ctx->nx - 1), pitch, 0, sizeof(float), ctx->ny,
+                                    ctx->stream));
+    T.c.al = T.d_al;
+    T.c.ar = T.d_ar;
+  }
+  // sub-block height per tile
+  const int ntiles = tg.tx * tg.ty;
+  std::vector<int> s_tile(ntiles, std::max(1, tl->sub_rows));
+  if (!ctx->treq_tiles.empty()) {
+    // given per tile of the unshifted tiling: a shifted tile takes the
+    // smallest height of the unshifted tiles it overlaps
+    for (int t = 0; t < ntiles; ++t) {
+      const int a = t % tg.tx, b = t / tg.tx;
+      int v = INT32_MAX;
+      for (int n = 0; n < tile_width(tg, a); ++n)
+        v = std::min(v, ctx->treq_tiles[(size_t)b * tg.tx + tile_col(tg, a, n) / tm]);
+      s_tile[t] = v;
+    }
+  } else if (!ctx->treq_rows.empty()) {
+    for (int t = 0; t < ntiles; ++t) s_tile[t] = ctx->treq_rows[t / tg.tx];
+  } else if (tl->growth_limit > 1.0) {
+    int *d_s = nullptr;
+    SEVP_CUDA_TRY(cudaMalloc((void **)&d_s, sizeof(int) * ntiles));
+    k_tile_growth<<<(ntiles + 7) / 8, 256, 0, ctx->stream>>>(tg, T.c, log(tl->growth_limit), d_s);
+    ctx->launches++;
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(s_tile.data(), d_s, sizeof(int) * ntiles, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(d_s);
+    if (e != cudaSuccess) {
+      sevp_internal_set_error(e, "tile growth", __FILE__, __LINE__);
+      return SEVP_CUDA_ERROR;
+    }
+  }
+  T.grp_nb.assign((size_t)tg.ty * tg.txg, 1);
+  for (int t = 0; t < ntiles; ++t) {
+    const int a = t % tg.tx, b = t / tg.tx;
+    if (s_tile[t] < 1) return SEVP_BAD_ARG;
+    const int nb = ceil_div(tile_height(tg, b), std::min(s_tile[t], tile_height(tg, b)));
+    int &g = T.grp_nb[(size_t)b * tg.txg + a / tg.tpw];
+    g = std::max(g, nb);
+  }
+  int nbmax = 1;
+  for (int v : T.grp_nb) nbmax = std::max(nbmax, v);
+  tg.nbmax = nbmax;
+  T.tile_nb.assign(ntiles, 1);
+  std::vector<long long> moff((size_t)ntiles);
+  long long off = 0;
+  for (int b = 0; b < tg.ty; ++b)
+    for (int a = 0; a < tg.tx; ++a) {
+      const int mw = tile_width(tg, a), nb = T.grp_nb[(size_t)b * tg.txg + a / tg.tpw];
+      T.tile_nb[(size_t)b * tg.tx + a] = nb;
+      moff[(size_t)b * tg.tx + a] = off;
+      off += (long long)(2 * nb - 1) * mw * mw;
+      off = (off + 1) & ~1LL;  // 16-byte aligned start for every tile
+    }
+  T.mats_elems = off;
+  SEVP_CUDA_TRY(cudaMalloc((void **)&T.d_grp_nb, sizeof(int) * T.grp_nb.size()));
+  SEVP_CUDA_TRY(cudaMalloc((void **)&T.d_moff, sizeof(long long) * moff.size()));
+  SEVP_CUDA_TRY(cudaMalloc((void **)&T.d_mats, sizeof(double) * std::max<long long>(off, 1)));
+  SEVP_CUDA_TRY(cudaMemcpyAsync(T.d_grp_nb, T.grp_nb.data(), sizeof(int) * T.grp_nb.size(),
+                                cudaMemcpyHostToDevice, ctx->stream));
+  SEVP_CUDA_TRY(cudaMemcpyAsync(T.d_moff, moff.data(), sizeof(long long) * moff.size(),
+                                cudaMemcpyHostToDevice, ctx->stream));
+  tg.grp_nb = T.d_grp_nb;
+  tg.moff = T.d_moff;
+  // partial-sum capacity for the tile grid
+  size_t tblocks = (tile_warps(tg) + kTileWarps - 1) / kTileWarps;
+  if (tblocks * 2 + 64 > ctx->partials_n) {
+    SEVP_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    cudaFree(ctx->partials);
+    ctx->partials_n = tblocks * 2 + 64;
+    SEVP_CUDA_TRY(cudaMalloc((void **)&ctx->partials, ctx->partials_n * 8));
+  }
+  // tile-apply shared memory must fit
+  if (tile_smem_per_warp(tg.hmax) * kTileWarps > 220 * 1024) return SEVP_BAD_ARG;
+  // precompute
+  int *d_status = nullptr;
+  SEVP_CUDA_TRY(cudaMalloc((void **)&d_status, sizeof(int)));
+  SEVP_CUDA_TRY(cudaMemsetAsync(d_status, 0, sizeof(int), ctx->stream));
+  size_t psmem = (size_t)5 * tg.hmax * 32 * sizeof(float) + (size_t)(32 * 32 * 3 + 32 * 64 + 32) * 8;
+  SEVP_CUDA_TRY(cudaFuncSetAttribute(k_tile_precompute, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)psmem));
+  k_tile_precompute<<<tg.ty * tg.tx, 1024, psmem, ctx->stream>>>(tg, T.c, T.d_mats, d_status);
+  ctx->launches++;
+  SEVP_CUDA_TRY(cudaGetLastError());
+  int h_status = 0;
+  SEVP_CUDA_TRY(cudaMemcpyAsync(&h_status, d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  SEVP_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  cudaFree(d_status);
+  if (h_status) return SEVP_SINGULAR;
+  T.built = true;
+  return SEVP_OK;
+}
+
+// Column cuts of the tiling with shift xs: the first column of every tile.
+static std::vector<char> tiling_cuts(const sevp_ctx *ctx, int xs) {
+  std::vector<char> cut((size_t)ctx->nx, 0);
+  const int tm = ctx->treq.tile_m;
+  for (int a = 0; a < ceil_div(ctx->nx, tm); ++a) cut[(size_t)((a * tm + xs) % ctx->nx)] = 1;
+  return cut;
+}
+
+// Column shift of the second Schwarz tiling: the requested one, or for
+// shift < 0 the one nearest tile_m / 2 whose tile edges all lie strictly
+// inside tiles of the unshifted tiling (and the other way round), so that
+// every coupling a stage needs is between two lanes of one tile.  0: none.
+static int schwarz_shift(const sevp_ctx *ctx, int req) {
+  const int tm = ctx->treq.tile_m;
+  if (tm < 2 || ctx->nx < 2) return 0;
+  const std::vector<char> ca = tiling_cuts(ctx, 0);
+  auto ok = [&](int xs) {
+    if (xs < 1 || xs >= tm || xs >= ctx->nx) return false;
+    const std::vector<char> cb = tiling_cuts(ctx, xs);
+    for (int c = 0; c < ctx->nx; ++c)
+      if (ca[c] && cb[c]) return false;
+    return true;
+  };
+  if (req > 0) return ok(req) ? req : 0;
+  for (int d = 0; d < tm; ++d) {
+    if (ok(tm / 2 - d)) return tm / 2 - d;
+    if (ok(tm / 2 + d)) return tm / 2 + d;
+  }
+  return 0;
+}
+
+// (Re)builds the second tiling and the Schwarz work vectors.
+static int build_schwarz(sevp_ctx *ctx) {
+  ctx->tb.release();
+  if (!ctx->schwarz_req) return SEVP_OK;
+  if (ctx->treq.tile_h > kCoupleMaxRows) return SEVP_BAD_ARG;
+  const int xs = schwarz_shift(ctx, ctx->schwarz_req);
+  if (!xs) return SEVP_BAD_ARG;
+  const size_t n = ctx->n;
+  if (!ctx->s1_64) {
+    SEVP_CUDA_TRY(cudaMalloc((void **)&ctx->s1_64, n * 8));
+    SEVP_CUDA_TRY(cudaMalloc((void **)&ctx->s2_64, n * 8));
+    SEVP_CUDA_TRY(cudaMalloc((void **)&ctx->s1_32, n * 4));
+    SEVP_CUDA_TRY(cudaMalloc((void **)&ctx->s2_32, n * 4));
+  }
+  int s = build_tiling(ctx, ctx->tb, xs);
+  if (s) ctx->tb.release();
+  return s;
 }
 
 extern "C" int sevp_set_operator(sevp_ctx *ctx, const float *al, const float *ab, const float *ac,
@@ -1376,7 +1840,7 @@ extern "C" int sevp_set_operator(sevp_ctx *ctx, const float *al, const float *ab
   drop_inner_graph(ctx);
   const int tm = tl->tile_m, th = tl->tile_h;
   if (tm < 1 || tm > 32 || th < 1 || th > 32 || tl->sub_rows < 1) return SEVP_BAD_ARG;
-  // the tile geometry needs ceil(nx/tm) etc. before the growth kernel runs
+  ctx->have_op = false;
   ctx->c = Coeffs{al, ab, ac, ar, at};
   {
     int *d_asym = nullptr;
@@ -1398,97 +1862,40 @@ extern "C" int sevp_set_operator(sevp_ctx *ctx, const float *al, const float *ab
     }
     ctx->sym = (!h_asym && !ctx->force_full) ? 1 : 0;
   }
-  if (ctx->d_mats32) cudaFree(ctx->d_mats32), ctx->d_mats32 = nullptr;
-  TileGeom &tg = ctx->tg;
-  tg.nx = ctx->nx, tg.ny = ctx->ny, tg.tm = tm, tg.th = th;
-  tg.tx = ceil_div(ctx->nx, tm);
-  tg.ty = ceil_div(ctx->ny, th);
-  tg.wseg = tm <= 8 ? 8 : (tm <= 16 ? 16 : 32);
-  tg.tpw = 32 / tg.wseg;
-  tg.txg = ceil_div(tg.tx, tg.tpw);
-  tg.hmax = th;
-  // sub-block height per tile
-  const int ntiles = tg.tx * tg.ty;
-  std::vector<int> s_tile(ntiles, std::max(1, tl->sub_rows));
-  if (tl->sub_rows_by_tile) {
-    for (int t = 0; t < ntiles; ++t) s_tile[t] = tl->sub_rows_by_tile[t];
-  } else if (tl->sub_rows_by_tile_row) {
-    for (int t = 0; t < ntiles; ++t) s_tile[t] = tl->sub_rows_by_tile_row[t / tg.tx];
-  } else if (tl->growth_limit > 1.0) {
-    int *d_s = nullptr;
-    SEVP_CUDA_TRY(cudaMalloc((void **)&d_s, sizeof(int) * ntiles));
-    k_tile_growth<<<(ntiles + 7) / 8, 256, 0, ctx->stream>>>(tg, ctx->c, log(tl->growth_limit), d_s);
-    ctx->launches++;
-    cudaError_t e = cudaGetLastError();
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(s_tile.data(), d_s, sizeof(int) * ntiles, cudaMemcpyDeviceToHost, ctx->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-    cudaFree(d_s);
-    if (e != cudaSuccess) {
-      sevp_internal_set_error(e, "tile growth", __FILE__, __LINE__);
-      return SEVP_CUDA_ERROR;
-    }
-  }
-  ctx->grp_nb.assign((size_t)tg.ty * tg.txg, 1);
-  for (int t = 0; t < ntiles; ++t) {
-    const int a = t % tg.tx, b = t / tg.tx;
-    if (s_tile[t] < 1) return SEVP_BAD_ARG;
-    const int nb = ceil_div(tile_height(tg, b), std::min(s_tile[t], tile_height(tg, b)));
-    int &g = ctx->grp_nb[(size_t)b * tg.txg + a / tg.tpw];
-    g = std::max(g, nb);
-  }
-  int nbmax = 1;
-  for (int v : ctx->grp_nb) nbmax = std::max(nbmax, v);
-  tg.nbmax = nbmax;
-  ctx->tile_nb.assign(ntiles, 1);
-  std::vector<long long> moff((size_t)ntiles);
-  long long off = 0;
-  for (int b = 0; b < tg.ty; ++b)
-    for (int a = 0; a < tg.tx; ++a) {
-      const int mw = tile_width(tg, a), nb = ctx->grp_nb[(size_t)b * tg.txg + a / tg.tpw];
-      ctx->tile_nb[(size_t)b * tg.tx + a] = nb;
-      moff[(size_t)b * tg.tx + a] = off;
-      off += (long long)(2 * nb - 1) * mw * mw;
-      off = (off + 1) & ~1LL;  // 16-byte aligned start for every tile
-    }
-  ctx->mats_elems = off;
-  if (ctx->d_grp_nb) cudaFree(ctx->d_grp_nb), ctx->d_grp_nb = nullptr;
-  if (ctx->d_moff) cudaFree(ctx->d_moff), ctx->d_moff = nullptr;
-  if (ctx->d_mats) cudaFree(ctx->d_mats), ctx->d_mats = nullptr;
-  SEVP_CUDA_TRY(cudaMalloc((void **)&ctx->d_grp_nb, sizeof(int) * ctx->grp_nb.size()));
-  SEVP_CUDA_TRY(cudaMalloc((void **)&ctx->d_moff, sizeof(long long) * moff.size()));
-  SEVP_CUDA_TRY(cudaMalloc((void **)&ctx->d_mats, sizeof(double) * std::max<long long>(off, 1)));
-  SEVP_CUDA_TRY(cudaMemcpyAsync(ctx->d_grp_nb, ctx->grp_nb.data(), sizeof(int) * ctx->grp_nb.size(),
-                                cudaMemcpyHostToDevice, ctx->stream));
-  SEVP_CUDA_TRY(cudaMemcpyAsync(ctx->d_moff, moff.data(), sizeof(long long) * moff.size(),
-                                cudaMemcpyHostToDevice, ctx->stream));
-  tg.grp_nb = ctx->d_grp_nb;
-  tg.moff = ctx->d_moff;
-  // partial-sum capacity for the tile grid
-  size_t tblocks = (tile_warps(tg) + kTileWarps - 1) / kTileWarps;
-  if (tblocks * 2 + 64 > ctx->partials_n) {
-    cudaFree(ctx->partials);
-    ctx->partials_n = tblocks * 2 + 64;
-    SEVP_CUDA_TRY(cudaMalloc((void **)&ctx->partials, ctx->partials_n * 8));
-  }
-  // tile-apply shared memory must fit
-  if (tile_smem_per_warp(tg.hmax) * kTileWarps > 220 * 1024) return SEVP_BAD_ARG;
-  // precompute
-  int *d_status = nullptr;
-  SEVP_CUDA_TRY(cudaMalloc((void **)&d_status, sizeof(int)));
-  SEVP_CUDA_TRY(cudaMemsetAsync(d_status, 0, sizeof(int), ctx->stream));
-  size_t psmem = (size_t)5 * tg.hmax * 32 * sizeof(float) + (size_t)(32 * 32 * 3 + 32 * 64 + 32) * 8;
-  SEVP_CUDA_TRY(cudaFuncSetAttribute(k_tile_precompute, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)psmem));
-  k_tile_precompute<<<tg.ty * tg.tx, 1024, psmem, ctx->stream>>>(tg, ctx->c, ctx->d_mats, d_status);
-  ctx->launches++;
-  SEVP_CUDA_TRY(cudaGetLastError());
-  int h_status = 0;
-  SEVP_CUDA_TRY(cudaMemcpyAsync(&h_status, d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-  SEVP_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-  cudaFree(d_status);
+  // keep the request (the second tiling is built from it later too)
+  ctx->treq = *tl;
+  const int tx = ceil_div(ctx->nx, tm), ty = ceil_div(ctx->ny, th);
+  ctx->treq_tiles.clear();
+  ctx->treq_rows.clear();
+  if (tl->sub_rows_by_tile)
+    ctx->treq_tiles.assign(tl->sub_rows_by_tile, tl->sub_rows_by_tile + (size_t)tx * ty);
+  else if (tl->sub_rows_by_tile_row)
+    ctx->treq_rows.assign(tl->sub_rows_by_tile_row, tl->sub_rows_by_tile_row + ty);
+  ctx->treq.sub_rows_by_tile = nullptr;
+  ctx->treq.sub_rows_by_tile_row = nullptr;
+  int s = build_tiling(ctx, ctx->ta, 0);
+  if (s) return s;
   ctx->have_op = true;
-  return h_status ? SEVP_SINGULAR : SEVP_OK;
+  s = build_schwarz(ctx);
+  if (s) ctx->schwarz_req = 0;  // the block-Jacobi operator stays usable
+  return s;
+}
+
+extern "C" int sevp_set_schwarz(sevp_ctx *ctx, int shift) {
+  if (!ctx || !ctx->have_op) return SEVP_BAD_ARG;
+  drop_inner_graph(ctx);
+  ctx->schwarz_req = shift;
+  int s = build_schwarz(ctx);
+  if (s) ctx->schwarz_req = 0;
+  return s;
+}
+
+extern "C" int sevp_schwarz_shift(const sevp_ctx *ctx) {
+  return (ctx && schwarz_on(ctx)) ? ctx->tb.tg.xs : 0;
+}
+
+extern "C" long long sevp_schwarz_influence_bytes(const sevp_ctx *ctx) {
+  return (ctx && schwarz_on(ctx)) ? ctx->tb.mats_elems * 8 : 0;
 }
 
 extern "C" int sevp_apply(sevp_ctx *ctx, const double *x, double *y) {
@@ -1499,14 +1906,14 @@ extern "C" int sevp_apply(sevp_ctx *ctx, const double *x, double *y) {
 
 extern "C" int sevp_precondition(sevp_ctx *ctx, const double *r, double *z) {
   if (!ctx || !ctx->have_op || !r || !z) return SEVP_BAD_ARG;
-  return launch_tile<double, false, false>(ctx, nullptr, nullptr, const_cast<double *>(r), nullptr,
-                                           z, 1);
+  return precondition_pass<double, false, false>(ctx, nullptr, nullptr, const_cast<double *>(r),
+                                                 nullptr, z);
 }
 
 extern "C" int sevp_precondition_f32(sevp_ctx *ctx, const float *r, float *z) {
   if (!ctx || !ctx->have_op || !r || !z) return SEVP_BAD_ARG;
-  return launch_tile<float, false, false>(ctx, nullptr, nullptr, const_cast<float *>(r), nullptr, z,
-                                          1);
+  return precondition_pass<float, false, false>(ctx, nullptr, nullptr, const_cast<float *>(r),
+                                                nullptr, z);
 }
 
 static int read_state(sevp_ctx *ctx) {
@@ -1549,12 +1956,12 @@ template <typename V>
 static int pcg_loop(sevp_ctx *ctx, V *x, V *r, V *z, V *p0, V *p1, V *q, int check_every,
                     int *iters_out) {
   V *pp[2] = {p0, p1};
-  auto interval = [&](int &cur) -> int {  // check_every iterations of the two passes
+  auto interval = [&](int &cur) -> int {  // check_every iterations of passes A and B
     for (int k = 0; k < check_every; ++k) {
       OpPassA<V> op{z, pp[cur], pp[cur ^ 1], q, ctx->st};
       int s = launch_stencil(ctx, op, 3);
       if (s) return s;
-      s = launch_tile<V, true, true>(ctx, x, pp[cur ^ 1], r, q, z, 4);
+      s = precondition_pass<V, true, true>(ctx, x, pp[cur ^ 1], r, q, z);
       if (s) return s;
       cur ^= 1;
     }
@@ -1564,10 +1971,11 @@ static int pcg_loop(sevp_ctx *ctx, V *x, V *r, V *z, V *p0, V *p1, V *q, int che
   // FP32 inner loop: one graph replay per check interval (an even interval
   // returns the p buffers to the same roles, so one capture serves all)
   const bool graph = sizeof(V) == 4 && ctx->use_graphs && !ctx->prof && check_every % 2 == 0;
-  const void *key[3] = {(const void *)x, (const void *)p0,
-                        (const void *)(ctx->infl32_active ? ctx->d_mats32 : nullptr)};
+  const void *key[4] = {(const void *)x, (const void *)p0,
+                        (const void *)(ctx->infl32_active ? ctx->ta.d_mats32 : nullptr),
+                        (const void *)(schwarz_on(ctx) ? ctx->tb.d_mats : nullptr)};
   if (graph && !(ctx->inner_graph && ctx->inner_graph_ce == check_every &&
-                 std::equal(key, key + 3, ctx->inner_graph_key))) {
+                 std::equal(key, key + 4, ctx->inner_graph_key))) {
     drop_inner_graph(ctx);
     if (!ctx->cap_stream)
       SEVP_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking));
@@ -1596,12 +2004,12 @@ static int pcg_loop(sevp_ctx *ctx, V *x, V *r, V *z, V *p0, V *p1, V *q, int che
       return SEVP_CUDA_ERROR;
     }
     ctx->inner_graph_ce = check_every;
-    std::copy(key, key + 3, ctx->inner_graph_key);
+    std::copy(key, key + 4, ctx->inner_graph_key);
   }
   for (;;) {
     if (graph) {
       SEVP_CUDA_TRY(cudaGraphLaunch(ctx->inner_graph, ctx->stream));
-      ctx->launches += 2 * check_every;
+      ctx->launches += (schwarz_on(ctx) ? 4 : 2) * check_every;
     } else {
       int s = interval(cur);
       if (s) return s;
@@ -1643,7 +2051,7 @@ static int solve_fp64(sevp_ctx *ctx, const double *b, double *x, const sevp_solv
       break;
     }
     // z = M^{-1} r, rz; then iterate
-    s = launch_tile<double, false, true>(ctx, nullptr, nullptr, ctx->r64, nullptr, ctx->z64, 4);
+    s = precondition_pass<double, false, true>(ctx, nullptr, nullptr, ctx->r64, nullptr, ctx->z64);
     if (s) return s;
     int it = 0;
     s = pcg_loop<double>(ctx, x, ctx->r64, ctx->z64, ctx->p64[0], ctx->p64[1], ctx->q64,
@@ -1658,15 +2066,19 @@ static int solve_fp64(sevp_ctx *ctx, const double *b, double *x, const sevp_solv
 }
 
 // FP32 PCG inside FP64 iterative refinement.
-static int ensure_mats32(sevp_ctx *ctx) {
-  if (ctx->d_mats32) return SEVP_OK;
-  const size_t n = (size_t)std::max<long long>(ctx->mats_elems, 1);
-  SEVP_CUDA_TRY(cudaMalloc((void **)&ctx->d_mats32, n * sizeof(float)));
+static int ensure_mats32_of(sevp_ctx *ctx, Tiling &T) {
+  if (T.d_mats32 || !T.built) return SEVP_OK;
+  const size_t n = (size_t)std::max<long long>(T.mats_elems, 1);
+  SEVP_CUDA_TRY(cudaMalloc((void **)&T.d_mats32, n * sizeof(float)));
   k_to_float<<<(unsigned)std::min<size_t>((n + 255) / 256, 148 * 32), 256, 0, ctx->stream>>>(
-      ctx->d_mats, ctx->d_mats32, n);
+      T.d_mats, T.d_mats32, n);
   ctx->launches++;
   SEVP_CUDA_TRY(cudaGetLastError());
   return SEVP_OK;
+}
+static int ensure_mats32(sevp_ctx *ctx) {
+  int s = ensure_mats32_of(ctx, ctx->ta);
+  return s ? s : ensure_mats32_of(ctx, ctx->tb);
 }
 
 static int solve_mixed(sevp_ctx *ctx, const double *b, double *x, const sevp_solve_opts *o,
@@ -1717,7 +2129,7 @@ static int solve_mixed(sevp_ctx *ctx, const double *b, double *x, const sevp_sol
     }
     // inner solve A d = r32 from d = 0
     SEVP_CUDA_TRY(cudaMemsetAsync(ctx->d32, 0, ctx->n * 4, ctx->stream));
-    s = launch_tile<float, false, true>(ctx, nullptr, nullptr, ctx->r32, nullptr, ctx->z32, 4);
+    s = precondition_pass<float, false, true>(ctx, nullptr, nullptr, ctx->r32, nullptr, ctx->z32);
     if (s) return s;
     int it = 0;
     s = pcg_loop<float>(ctx, ctx->d32, ctx->r32, ctx->z32, ctx->p32[0], ctx->p32[1], ctx->q32,
@@ -1983,7 +2395,9 @@ extern "C" int sevp_nn_features(sevp_ctx *ctx, const double *eta1, const double 
   ctx->launches++;
   s = launch_residual<double>(ctx, e, nullptr, nullptr, b, ctx->r64, 0, 0.0);
   if (s) return s;
-  s = launch_tile<double, false, false>(ctx, nullptr, nullptr, ctx->r64, nullptr, m, 1);
+  // the feature is the block-Jacobi preconditioner's response (what the
+  // network was trained on), whichever preconditioner the solves use
+  s = launch_tile<double, false, false>(ctx, ctx->ta, nullptr, nullptr, ctx->r64, nullptr, m, 1);
   if (s) return s;
   k_rms3<<<grid_for(ctx->n), 256, 0, ctx->stream>>>(ctx->r64, m, d, ctx->n, ctx->partials,
                                                    ctx->tickets + 5, scales);

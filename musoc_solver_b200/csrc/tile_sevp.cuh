@@ -20,6 +20,15 @@
 //   R1_t    t = 0..nb-2  minus Sinv_t times the guess-row -> top-row map
 //                        (the reference's RINV1)
 // stored consecutively: Sinv_0..Sinv_{nb-1}, R1_0..R1_{nb-2}.
+//
+// Shifted tilings (the second tiling of the overlapping Schwarz
+// preconditioner): with a column shift xs, tile column a covers the grid
+// columns (a*tm + n + xs) mod nx, n = 0..mw-1, i.e. the standard tiling of
+// the grid rolled west by xs; the tile that reaches the last column wraps
+// to column 0.  On a periodic grid that tile couples across the seam like
+// any other column pair.  On a closed grid the tiling reads AL and AR planes
+// whose couplings across the seam are zero, so that tile holds two
+// independent pieces.
 #pragma once
 #include "common.cuh"
 
@@ -32,6 +41,7 @@ struct TileGeom {
   int txg;    // tile groups per tile row = ceil(tx / tpw)
   int hmax;   // max tile height (= th)
   int nbmax;  // max sub-blocks per tile
+  int xs;     // column shift of the tiling (0 <= xs < nx)
   const int *grp_nb;         // [ty * txg] sub-blocks of the tiles of one warp group
   const long long *moff;     // [ty * tx] offset of each tile's influence data
 };
@@ -45,5 +55,12 @@ __host__ __device__ inline int tile_height(const TileGeom &g, int b) {
   return h < g.th ? h : g.th;
 }
 __host__ __device__ inline int sub_start(int t, int hh, int nb) { return (t * hh) / nb; }
+// Grid column of lane n of tile column a (n < tile_width; 0 otherwise).
+__host__ __device__ inline int tile_col(const TileGeom &g, int a, int n) {
+  int c = a * g.tm + n;
+  if (c >= g.nx) return 0;
+  c += g.xs;
+  return c >= g.nx ? c - g.nx : c;
+}
 
 }  // namespace sevp

@@ -85,6 +85,9 @@ _SIGS = {
     "sevp_operator_symmetric": ([P], C.c_int),
     "sevp_set_full_coefficients": ([P, C.c_int], C.c_int),
     "sevp_set_graphs": ([P, C.c_int], C.c_int),
+    "sevp_set_schwarz": ([P, C.c_int], C.c_int),
+    "sevp_schwarz_shift": ([P], C.c_int),
+    "sevp_schwarz_influence_bytes": ([P], C.c_longlong),
     "sevp_inprod_noalloc": ([P, P, C.c_int, C.c_int, P, P], C.c_int),
     "sevp_fs_mask": ([C.c_int, C.c_int, P, P, P, P, C.c_int, P], C.c_int),
     "sevp_fs_rhs": ([C.c_int, C.c_int, C.c_int] + [P] * 11, C.c_int),

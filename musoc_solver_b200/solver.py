@@ -99,7 +99,8 @@ class SevpSolver:
 
     def __init__(self, problem, tile_m: int = 16, tile_h: int = 16, sub_rows=None,
                  growth_limit: float = 1e10, device: str = "cuda", stream=None,
-                 full_coefficients: bool = False, precond_fp32: bool = False):
+                 full_coefficients: bool = False, precond_fp32: bool = False,
+                 schwarz=False):
         import torch
 
         self.precond_fp32 = bool(precond_fp32)
@@ -131,6 +132,8 @@ class SevpSolver:
         N.check(N.lib().sevp_set_operator(self.h, *[N.ptr(t) for t in self.coef],
                                           C.byref(self.tiling)), "sevp_set_operator")
         self.tile_nb = self.layout()
+        if schwarz:
+            self.set_schwarz(-1 if schwarz is True else int(schwarz))
 
     def layout(self) -> np.ndarray:
         """Sub-blocks used by each tile, shape (tiles_y, tiles_x)."""
@@ -164,11 +167,12 @@ class SevpSolver:
         N.check(N.lib().sevp_profile(self.h, int(enable)), "sevp_profile")
 
     def profile_read(self):
-        """{class: (total_ms, launches)} for 'tile', 'stencil', 'precond'."""
+        """{class: (total_ms, launches)} for 'tile', 'stencil', 'precond', 'couple'."""
         ms = (C.c_double * 4)()
         n = (C.c_longlong * 4)()
         N.check(N.lib().sevp_profile_read(self.h, ms, n), "sevp_profile_read")
-        return {"tile": (ms[0], n[0]), "stencil": (ms[1], n[1]), "precond": (ms[2], n[2])}
+        return {"tile": (ms[0], n[0]), "stencil": (ms[1], n[1]), "precond": (ms[2], n[2]),
+                "couple": (ms[3], n[3])}
 
     def opts(self, precision=0, tol=1e-12, max_iter=5000, inner_tol=1e-5, use_guess=False,
              check_every=4, precond_fp32=None):
@@ -176,6 +180,21 @@ class SevpSolver:
             precond_fp32 = self.precond_fp32
         return N.SolveOpts(int(precision), float(tol), int(max_iter), float(inner_tol),
                            int(use_guess), int(check_every), int(precond_fp32))
+
+    def set_schwarz(self, shift: int = -1):
+        """Overlapping Schwarz preconditioner: a second tiling rolled west by
+        ``shift`` columns (-1: about half a tile), applied as the symmetric
+        multiplicative sweep first tiling -> second -> first.  0 returns to
+        block-Jacobi.  Tiles must be at most 8 rows high."""
+        N.check(N.lib().sevp_set_schwarz(self.h, int(shift)), "sevp_set_schwarz")
+
+    @property
+    def schwarz_shift(self) -> int:
+        """Column shift of the second tiling (0: block-Jacobi)."""
+        return int(N.lib().sevp_schwarz_shift(self.h))
+
+    def schwarz_influence_bytes(self) -> int:
+        return int(N.lib().sevp_schwarz_influence_bytes(self.h))
 
     def graphs(self, enable: bool = True):
         """CUDA-graph replay of the FP32 inner iterations (default on)."""
