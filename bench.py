@@ -77,6 +77,10 @@ def parse():
                     help="the network runs on the grid averaged over coarse x coarse cells")
     ap.add_argument("--tiles", default="auto",
                     help="tile shape MxH of the GPU solver, or 'auto' (measured at start-up)")
+    ap.add_argument("--precond", default="auto", choices=["auto", "bj", "schwarz"],
+                    help="block-Jacobi tiles, the overlapping Schwarz sweep, or 'auto' (measured)")
+    ap.add_argument("--inner-tol", default="auto",
+                    help="relative reduction of each FP32 inner solve, or 'auto' (measured)")
     ap.add_argument("--no-fs", action="store_true",
                     help="skip the barotropic correction loop arm (3600x2400, 20 layers)")
     ap.add_argument("--no-ensemble", action="store_true",
@@ -149,16 +153,18 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-def ncu_traffic(nx, ny, tiles):
-    """Per-launch DRAM bytes of the FP32 tile pass-B kernel from the committed
-    ncu summary (profiles/), or None when the summary covers another grid or
-    tile shape (it is a 3600x2400 capture with 16x6 tiles)."""
+def ncu_traffic(nx, ny, tiles, kernel="passb"):
+    """Per-launch DRAM bytes from the committed ncu summaries (profiles/):
+    the FP32 pass-B kernel ("passb") or the Schwarz stage kernel averaged
+    over stages 2 and 3 ("couple"); None when the summary covers another
+    grid or tile shape (they are 3600x2400 captures with 16x6 tiles)."""
     if (nx, ny, tuple(tiles)) != (3600, 2400, (16, 6)):
         return None
-    path = os.path.join(ROOT, "profiles", "tile_pass_b_3600x2400.md")
+    name, key = {"passb": ("tile_pass_b_3600x2400.md", "traffic_bytes_per_launch_mixed:"),
+                 "couple": ("schwarz_stages_3600x2400.md", "traffic_bytes_per_launch_avg:")}[kernel]
     try:
-        for line in open(path):
-            if line.startswith("traffic_bytes_per_launch_mixed:"):
+        for line in open(os.path.join(ROOT, "profiles", name)):
+            if line.startswith(key):
                 return float(line.split(":")[1])
     except OSError:
         pass
@@ -244,7 +250,7 @@ def run_reference(args, world, rank):
 
 
 # --------------------------------------------------------------- ensemble
-def run_ensemble(K, W, members=64, nx=720, ny=360):
+def run_ensemble(K, W, members=64, nx=720, ny=360, schwarz=False, inner_tol=1e-5):
     """64 members x 720x360 (independently perturbed depths and right-hand
     sides) stacked into one system: every kernel launch covers all members."""
     import torch
@@ -262,16 +268,21 @@ def run_ensemble(K, W, members=64, nx=720, ny=360):
     out = {"workload": f"{members} members x {nx}x{ny}, +-5% depth noise, own right-hand sides, "
                        f"stacked ({e.problem.nx}x{e.problem.ny}), tiles {e.solver.tile_m}x{e.solver.tile_h}",
            "setup_seconds": setup_s}
-    for name, prec in (("mixed", 1), ("fp64", 0)):
+    arms = [("mixed", 1, False), ("fp64", 0, False)]
+    if schwarz:
+        arms += [("mixed_schwarz", 1, True), ("fp64_schwarz", 0, True)]
+    for name, prec, sw in arms:
+        if sw != bool(e.solver.schwarz_shift):
+            e.solver.set_schwarz(-1 if sw else 0)
         x = torch.zeros_like(b)
         for _ in range(W):
-            e.solve(b, x=x.zero_(), precision=prec)
+            e.solve(b, x=x.zero_(), precision=prec, inner_tol=inner_tol)
         torch.cuda.synchronize()
         ev0.record(stream)
         res = None
         for _ in range(K):
             x.zero_()
-            x, res, _ = e.solve(b, x=x, precision=prec)
+            x, res, _ = e.solve(b, x=x, precision=prec, inner_tol=inner_tol)
         ev1.record(stream)
         torch.cuda.synchronize()
         t = ev0.elapsed_time(ev1) / 1e3
@@ -280,16 +291,18 @@ def run_ensemble(K, W, members=64, nx=720, ny=360):
                      "iterations": res.iterations, "max_member_rel_residual": float(rel.max())}
         if name == "mixed":
             xm = x.clone()
+        if name == "fp64":
+            x64 = x.clone()
     # per-member error of the mixed solve against the FP64 solve
-    d = (xm - x).reshape(members, -1).abs().amax(dim=1)
-    ref = x.reshape(members, -1).abs().amax(dim=1)
+    d = (xm - x64).reshape(members, -1).abs().amax(dim=1)
+    ref = x64.reshape(members, -1).abs().amax(dim=1)
     out["mixed"]["max_member_rel_err_vs_fp64"] = float((d / ref).max())
     e.close()
     return out
 
 
 # ------------------------------------------------ barotropic correction loop
-def run_fs(nx, ny, k1, tiles, passes=3, peak=None):
+def run_fs(nx, ny, k1, tiles, passes=3, peak=None, schwarz=False, inner_tol=1e-5):
     """The FS barotropic correction (ITMASK loop) on a layered state: one
     pass = land masking, continuity right-hand side, mixed solve, P0 and
     velocity correction of every layer."""
@@ -299,14 +312,14 @@ def run_fs(nx, ny, k1, tiles, passes=3, peak=None):
     from musoc_solver_b200.barotropic import BarotropicCorrection
 
     st = P.fs_state(nx, ny, k1, seed=7)
-    bc = BarotropicCorrection(st, tile_m=tiles[0], tile_h=tiles[1])
+    bc = BarotropicCorrection(st, tile_m=tiles[0], tile_h=tiles[1], schwarz=schwarz)
     u, v, p0, scr = bc.upload()
     stream = bc.solver.stream
-    bc.run(u, v, p0, scr, tolerance=0.0, mxmask=1)  # warm-up pass
+    bc.run(u, v, p0, scr, tolerance=0.0, mxmask=1, inner_tol=inner_tol)  # warm-up pass
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     ev0.record(stream)
-    n_pass, vmax, iters = bc.run(u, v, p0, scr, tolerance=0.0, mxmask=passes)
+    n_pass, vmax, iters = bc.run(u, v, p0, scr, tolerance=0.0, mxmask=passes, inner_tol=inner_tol)
     ev1.record(stream)
     torch.cuda.synchronize()
     t_loop = ev0.elapsed_time(ev1) / n_pass
@@ -330,7 +343,8 @@ def run_fs(nx, ny, k1, tiles, passes=3, peak=None):
     b_cor = n * (8 + 12 * k1 + 8 + 8 + 16)
     gbs = lambda b, ms: b / (ms * 1e-3) / 1e9
     out = {"workload": f"{nx}x{ny} interior, {k1} layers, land masks from the synthetic depth; "
-                       f"mixed solve to 1e-12, tiles {tiles[0]}x{tiles[1]}",
+                       f"mixed solve to 1e-12, tiles {tiles[0]}x{tiles[1]}"
+                       f"{', Schwarz preconditioner' if schwarz else ''}",
            "ms_per_pass": t_loop, "passes": n_pass, "pcg_iterations": iters,
            "land_velocity_after": vmax,
            "rhs_ms": t_rhs, "rhs_gbs": gbs(b_rhs, t_rhs), "correct_ms": t_cor,
@@ -359,17 +373,26 @@ def run_native(args, world, rank, local, dist):
     p, rhs = make_sequence(args.nx, args.ny, nsteps)
     n = p.nx * p.ny
     # tile shape: measured on the first right-hand side (untimed)
-    tune_table = None
-    if args.tiles == "auto":
-        from musoc_solver_b200.autotune import autotune
+    # tile shape, preconditioner and inner tolerance: measured on the first
+    # right-hand side (untimed) unless all three are given
+    from musoc_solver_b200.autotune import CANDIDATES, SCHWARZ_MAX_ROWS, autotune
 
-        best, tune_table = autotune(p, torch.from_numpy(rhs[0]).to(dev), precision=1,
-                                    growth_limit=GROWTH)
-        tiles = (best["tile_m"], best["tile_h"])
+    tune_table = None
+    cands = CANDIDATES if args.tiles == "auto" else (
+        tuple(int(v) for v in args.tiles.lower().split("x")),)
+    sw_opts = {"auto": (False, True), "bj": (False,), "schwarz": (True,)}[args.precond]
+    itols = (1e-5, 1e-6) if args.inner_tol == "auto" else (float(args.inner_tol),)
+    if len(cands) * len(sw_opts) * len(itols) > 1:
+        best, tune_table = autotune(p, torch.from_numpy(rhs[0]).to(dev), candidates=cands,
+                                    precision=1, growth_limit=GROWTH, schwarz=sw_opts,
+                                    inner_tols=itols)
+        tiles, use_sw, itol = (best["tile_m"], best["tile_h"]), best["schwarz"], best["inner_tol"]
     else:
-        tiles = tuple(int(v) for v in args.tiles.lower().split("x"))
+        tiles, use_sw, itol = cands[0], sw_opts[0], itols[0]
+    if use_sw and tiles[1] > SCHWARZ_MAX_ROWS:
+        raise SystemExit(f"the Schwarz preconditioner needs tiles of at most {SCHWARZ_MAX_ROWS} rows")
     solver = SevpSolver(p, tile_m=tiles[0], tile_h=tiles[1], growth_limit=GROWTH,
-                        precond_fp32=args.precond_fp32)
+                        precond_fp32=args.precond_fp32, schwarz=use_sw)
     stream = solver.stream
     b_dev = [torch.from_numpy(b).to(dev) for b in rhs]
     torch.cuda.synchronize()
@@ -417,13 +440,14 @@ def run_native(args, world, rank, local, dist):
     def run_arm(mode, hist):
         """Warm-up and timed steps of a sequence arm; hist holds the solutions."""
         for k in range(T, T + W):
-            solver.solve_step(b_dev[k], hist[k - 1], hist[k - 2], hist[k], guess=mode, precision=1)
+            solver.solve_step(b_dev[k], hist[k - 1], hist[k - 2], hist[k], guess=mode, precision=1,
+                              inner_tol=itol)
         barrier()
         reps = []
         ev0.record(stream)
         for k in timed:
             _, r = solver.solve_step(b_dev[k], hist[k - 1], hist[k - 2], hist[k], guess=mode,
-                                     precision=1)
+                                     precision=1, inner_tol=itol)
             reps.append(r)
         ev1.record(stream)
         torch.cuda.synchronize()
@@ -452,26 +476,38 @@ def run_native(args, world, rank, local, dist):
         solver.solve(b_dev[k], x=ref_x.zero_(), precision=0)
         errs.append(float((eta[k] - ref_x).abs().max() / ref_x.abs().max()))
 
-    # ---- plain FP64 SEVP-PCG from a zero guess
+    # ---- plain FP64 SEVP-PCG from a zero guess (block-Jacobi tiles)
+    def fp64_zero_arm():
+        xz = torch.zeros_like(eta[0])
+        for k in range(T, T + W):
+            solver.solve(b_dev[k], x=xz.zero_(), precision=0)
+        barrier()
+        ev0.record(stream)
+        its = []
+        for k in timed:
+            _, r = solver.solve(b_dev[k], x=xz.zero_(), precision=0)
+            its.append(r.iterations)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        return max_over_ranks(ev0.elapsed_time(ev1) / 1e3), its
+
+    if use_sw:
+        solver.set_schwarz(0)
+    t_fp64, it64 = fp64_zero_arm()
+    fp64_sw = None
+    if use_sw:
+        solver.set_schwarz(-1)
+        t_sw, it_sw = fp64_zero_arm()
+        fp64_sw = {"value": world * K / t_sw, "unit": "solves/s", "ms_per_step": 1e3 * t_sw / K,
+                   "mean_iterations": float(np.mean(it_sw))}
     xz = torch.zeros_like(eta[0])
-    for k in range(T, T + W):
-        solver.solve(b_dev[k], x=xz.zero_(), precision=0)
-    barrier()
-    ev0.record(stream)
-    it64 = []
-    for k in timed:
-        _, r = solver.solve(b_dev[k], x=xz.zero_(), precision=0)
-        it64.append(r.iterations)
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    t_fp64 = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
 
     # ---- mixed precision from a zero guess (isolates the precision gain)
     barrier()
     ev0.record(stream)
     itmz = []
     for k in timed:
-        _, r = solver.solve(b_dev[k], x=xz.zero_(), precision=1)
+        _, r = solver.solve(b_dev[k], x=xz.zero_(), precision=1, inner_tol=itol)
         itmz.append(r.iterations)
     ev1.record(stream)
     torch.cuda.synchronize()
@@ -485,41 +521,60 @@ def run_native(args, world, rank, local, dist):
         eta_host[k][:] = eta[k].cpu().numpy()
     for k in range(T, T + W):
         solver.solve_step_host(b_host[k], eta_host[k - 1], eta_host[k - 2], eta_host[k],
-                               guess=guess_mode, precision=1)
+                               guess=guess_mode, precision=1, inner_tol=itol)
     barrier()
     t0 = time.perf_counter()
     l1 = solver.launches()
     for k in timed:
         solver.solve_step_host(b_host[k], eta_host[k - 1], eta_host[k - 2], eta_host[k],
-                               guess=guess_mode, precision=1)
+                               guess=guess_mode, precision=1, inner_tol=itol)
     torch.cuda.synchronize()
     t_e2e = max_over_ranks(time.perf_counter() - t0)
     launches_e2e = solver.launches() - l1
     h2d = 8 * n * (3 if guess_mode in (N.GUESS_LINEAR, N.GUESS_LEARNED) else 2)
     d2h = 8 * n
 
-    # ---- roofline of the dominant kernel (tile SEVP pass B, FP32 vectors)
+    # ---- roofline of the dominant kernel (FP32 vectors): pass B with the
+    #      block-Jacobi preconditioner, the Schwarz stage kernel otherwise
     peak, peak_kind = measured_peak_hbm()
     tile_ms, tile_n = prof["tile"]
-    infl = solver.influence_bytes()
+    cpl_ms, cpl_n = prof["couple"]
     ncoef = 3 if solver.symmetric else 5
-    infl_bytes = infl // 2 if args.precond_fp32 else infl
-    # x,p,r,q in; x,r,z out; coefficient planes; influence data
-    bytes_per_launch = n * (4 * 4 + 3 * 4 + 4 * ncoef) + infl_bytes
-    avg_s = tile_ms / 1e3 / max(tile_n, 1)
-    achieved = bytes_per_launch / avg_s / 1e9 if tile_n else None
-    traffic = ncu_traffic(p.nx, p.ny, tiles)
+    scale = 0.5 if args.precond_fp32 else 1.0
+    infl_a = int(solver.influence_bytes() * scale)
+    infl_b = int(solver.schwarz_influence_bytes() * scale)
+    # pass B: x,p,r,q in; x,r,z out (without r.z and z with the Schwarz
+    # preconditioner: z1 out); coefficient planes; influence data
+    b_passb = n * (4 * 4 + 3 * 4 + 4 * ncoef) + infl_a
+    # Schwarz stages, per launch averaged over stage 2 (w in, z2 out) and
+    # stage 3 (w, z1, r in, z out): halo rows of w (2 per tile row) and of
+    # AT (symmetric storage), coefficient planes, the tiling's influence data
+    halo = (2 * 4 + (4 if solver.symmetric else 0)) / tiles[1]
+    b_stage2 = n * (4 + 4 + halo + 4 * ncoef) + infl_b
+    b_stage3 = n * (4 + 4 + 4 + 4 + halo + 4 * ncoef) + infl_a
+    b_couple = 0.5 * (b_stage2 + b_stage3)
     short_tiles = tiles[1] <= 6  # FP32 vectors with tiles up to 6 rows run the short-tile kernel
+    passb_name = ("k_tile_short<float, update, dots>" if short_tiles
+                  else "k_tile_apply<float, update, dots>") + " (PCG pass B)"
+    if use_sw and cpl_n:
+        dom_name = "k_tile_couple<float> (Schwarz stages 2 and 3, averaged per launch)"
+        bytes_per_launch, avg_s, dom_n = b_couple, cpl_ms / 1e3 / cpl_n, cpl_n
+        traffic = ncu_traffic(p.nx, p.ny, tiles, "couple")
+    else:
+        dom_name = passb_name
+        bytes_per_launch, avg_s, dom_n = b_passb, tile_ms / 1e3 / max(tile_n, 1), tile_n
+        traffic = ncu_traffic(p.nx, p.ny, tiles, "passb")
+    achieved = bytes_per_launch / avg_s / 1e9 if dom_n else None
 
     # ---- 64-member ensemble (720x360 each), every launch over all members
     ens = None
     if not args.no_ensemble:
-        ens = run_ensemble(max(2, K // 2), max(1, min(W, 2)))
+        ens = run_ensemble(max(2, K // 2), max(1, min(W, 2)), schwarz=True, inner_tol=itol)
 
     # ---- the barotropic correction loop around the solve (FS ITMASK loop)
     fs = None
     if not args.no_fs:
-        fs = run_fs(p.nx, p.ny, 20, tiles, peak=peak)
+        fs = run_fs(p.nx, p.ny, 20, tiles, peak=peak, schwarz=use_sw, inner_tol=itol)
 
     # ---- CPU baseline (rank 0 at N = 1)
     cpu = None
@@ -550,8 +605,12 @@ def run_native(args, world, rank, local, dist):
                         "right-hand-side sequence; mixed FP32 tile-SEVP PCG + FP64 iterative "
                         f"refinement to 1e-12 from warm start: {guess_name}",
             "grid": [p.nx, p.ny], "tiles": list(tiles),
+            "preconditioner": (f"overlapping Schwarz, second tiling shifted by "
+                               f"{solver.schwarz_shift} columns" if use_sw else "block-Jacobi tiles"),
+            "inner_tol": itol,
             "tile_autotune": None if tune_table is None else
-            {f"{r['tile_m']}x{r['tile_h']}": round(r["ms"], 2) for r in tune_table},
+            {f"{r['tile_m']}x{r['tile_h']}{' schwarz' if r['schwarz'] else ''} itol={r['inner_tol']:g}":
+             round(r["ms"], 2) for r in tune_table},
             "marching_growth_limit": GROWTH,
             "coefficient_planes": 3 if solver.symmetric else 5,
             "influence_fp32_in_inner_solve": bool(args.precond_fp32),
@@ -560,7 +619,9 @@ def run_native(args, world, rank, local, dist):
         },
         "fp64_plain": {"value": world * K / t_fp64, "unit": "solves/s",
                        "ms_per_step": 1e3 * t_fp64 / K,
-                       "mean_iterations": float(np.mean(it64))},
+                       "mean_iterations": float(np.mean(it64)),
+                       "preconditioner": "block-Jacobi tiles"},
+        "fp64_schwarz_zero_guess": fp64_sw,
         "mixed_zero_guess": {"value": world * K / t_mixed0, "unit": "solves/s",
                              "mean_iterations": float(np.mean(itmz))},
         "linear_mixed": {"value": world * K / t_lin, "unit": "solves/s",
@@ -576,12 +637,17 @@ def run_native(args, world, rank, local, dist):
                 "d2h_bytes_per_step": d2h},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                     "kernel": ("k_tile_short<float, update, dots>" if short_tiles
-                                else "k_tile_apply<float, update, dots>") + " (PCG pass B)",
+                     "kernel": dom_name,
                      "algorithmic_bytes_per_launch": bytes_per_launch,
-                     "avg_launch_ms": avg_s * 1e3, "launches": tile_n,
+                     "avg_launch_ms": avg_s * 1e3, "launches": dom_n,
                      "peak_source": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)"},
-        "kernels": {"tile_pass_b": {"launches": tile_n, "avg_ms": avg_s * 1e3},
+        "kernels": {"tile_pass_b": {"launches": tile_n,
+                                    "avg_ms": tile_ms / max(tile_n, 1),
+                                    "hbm_frac": (b_passb / (tile_ms / 1e3 / tile_n) / 1e9 / peak)
+                                    if tile_n else None},
+                    "schwarz_stages": {"launches": cpl_n, "avg_ms": cpl_ms / max(cpl_n, 1),
+                                       "hbm_frac": (b_couple / (cpl_ms / 1e3 / cpl_n) / 1e9 / peak)
+                                       if cpl_n else None},
                     "stencil": {"launches": prof["stencil"][1],
                                 "avg_ms": prof["stencil"][0] / max(prof["stencil"][1], 1)},
                     "precondition_start": {"launches": prof["precond"][1],

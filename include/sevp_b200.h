@@ -222,6 +222,17 @@ long long sevp_influence_bytes(const sevp_ctx *ctx);
  * block-Jacobi preconditioner.  Kept across sevp_set_operator.  Returns
  * SEVP_BAD_ARG when no valid shift exists or the tiles are too high. */
 int sevp_set_schwarz(sevp_ctx *ctx, int shift);
+/* PCG coefficient record (not part of the reference interface; the
+ * reference estimates extreme eigenvalues with a 10-step Lanczos run,
+ * M/sevp.f90:618-694).  cap > 0: every later FP64 solve (precision 0)
+ * writes alpha_j and beta_j of its first PCG run, j = 1..cap, into a device
+ * buffer; cap = 0 stops recording and frees the buffer.  The CG-Lanczos
+ * tridiagonal built from them has the extreme Ritz values of the
+ * preconditioned operator M^-1 A. */
+int sevp_record_coefficients(sevp_ctx *ctx, int cap);
+/* Copies the last recorded coefficients to host arrays of cap entries;
+ * *count = iterations recorded (0 when nothing was recorded). */
+int sevp_read_coefficients(sevp_ctx *ctx, double *alpha, double *beta, int cap, int *count);
 /* Column shift of the second tiling, 0 when the preconditioner is block-Jacobi. */
 int sevp_schwarz_shift(const sevp_ctx *ctx);
 /* Device bytes held by the second tiling's influence data. */

@@ -23,13 +23,14 @@ class BarotropicCorrection:
     """Device copies of a state's masks and metrics, a solver for its
     operator, and the loop's scratch."""
 
-    def __init__(self, state, tile_m=16, tile_h=8, device="cuda"):
+    def __init__(self, state, tile_m=16, tile_h=8, device="cuda", schwarz=False):
         import torch
 
         self.torch = torch
         self.st = state
         self.i0, self.j0, self.k0 = state.dims
-        self.solver = SevpSolver(state.problem, tile_m=tile_m, tile_h=tile_h, device=device)
+        self.solver = SevpSolver(state.problem, tile_m=tile_m, tile_h=tile_h, device=device,
+                                 schwarz=schwarz)
         dev = self.solver.device
         t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
         self.d = {k: t(getattr(state, k)) for k in ("iu0", "iv0", "iu", "iv", "odx", "ody", "ocs",
@@ -69,10 +70,10 @@ class BarotropicCorrection:
         return float(self.vmax.item())
 
     def run(self, u, v, p0, scr, tolerance=1e-3, mxmask=18, precision=1, tol=1e-12,
-            periodic=True):
+            periodic=True, inner_tol=1e-5):
         """The whole loop; returns (passes, final land velocity, PCG iterations)."""
         d = self.d
-        o = self.solver.opts(precision, tol)
+        o = self.solver.opts(precision, tol, inner_tol=inner_tol)
         it, vm, iters = C.c_int(), C.c_float(), C.c_int()
         s = N.lib().sevp_fs_barotropic(
             self.solver.h, self.i0, self.j0, self.k0, N.ptr(u), N.ptr(v), N.ptr(p0), N.ptr(scr),

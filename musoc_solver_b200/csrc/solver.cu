@@ -43,6 +43,10 @@ struct SolveState {
   double bb64;    // ||b||^2 (residual kernel)
   int iter, max_iter, done, status;
   unsigned ticket[4];
+  // optional record of the PCG coefficients: alpha_j at hist[2 (j-1)],
+  // beta_j at hist[2 (j-1) + 1] for iterations j = 1..hist_cap
+  double *hist;
+  int hist_cap;
 };
 
 struct Coeffs {
@@ -259,6 +263,7 @@ struct OpPassA {
       st->done = 1;
     } else {
       st->alpha = st->rz / s[0];
+      if (st->hist && st->iter <= st->hist_cap) st->hist[2 * (st->iter - 1)] = st->alpha;
     }
   }
 };
@@ -424,6 +429,8 @@ struct TileFin {
       return;
     }
     st->beta = first ? 0.0 : rz / st->rz;
+    if (st->hist && st->iter >= 1 && st->iter <= st->hist_cap)
+      st->hist[2 * (st->iter - 1) + 1] = st->beta;
     st->rz = rz;
   }
 };
@@ -624,6 +631,98 @@ __global__ void __launch_bounds__(kTileWarps * 32, SEVP_TILE_MINB)
   }
 }
 
+// The march of march_task_regs for a full-height task with one sub-block
+// (hh == HM, nb == 1, the common case): the same operations in straight-line
+// code, without the sub-block bookkeeping.
+template <typename MT, bool SYM, bool kChain, int HM, class Rhs, class Emit>
+__device__ __forceinline__ void march_task_full(const float (&cc_)[HM], const float (&ce_)[HM],
+                                                const float (&cn_)[HM],
+                                                const float (&cw_)[SYM ? 1 : HM],
+                                                const float (&cs_)[SYM ? 1 : HM], int n, int mw,
+                                                bool active, int lane, int segbase, double *dv,
+                                                const MT *mt, Rhs &&rhs, Emit &&emit) {
+  double zs[HM];
+  double zb = 0.0, zc = 0.0, rho = 0.0;
+  float cn_prev = 0.f;
+#pragma unroll
+  for (int k = 0; k < HM; ++k) {
+    double cw, cs;
+    if (SYM) {
+      const float arw = __shfl_up_sync(0xffffffffu, ce_[k], 1);
+      cw = (n == 0) ? 0.0 : (double)arw;
+      cs = (double)cn_prev;
+      cn_prev = cn_[k];
+    } else {
+      cw = cw_[k];
+      cs = cs_[k];
+    }
+    const double cc = cc_[k], ce = ce_[k];
+    const double cn = active ? (double)cn_[k] : 1.0;
+    const double rk = rhs(k);
+    const double part = (kChain && active) ? (rk - cs * zb) - cc * zc : 0.0;
+    double zw = __shfl_up_sync(0xffffffffu, zc, 1);
+    double ze = __shfl_down_sync(0xffffffffu, zc, 1);
+    if (n == 0) zw = 0.0;
+    if (n >= mw - 1) ze = 0.0;
+    zs[k] = zc;
+    const double res = (kChain && active) ? (part - cw * zw) - ce * ze : 0.0;
+    if (k < HM - 1) {
+      double zn;
+      if constexpr (kChain)
+        zn = res * march_rcp(cn);
+      else
+        zn = active ? ((((rk - cw * zw) - cs * zb) - cc * zc) - ce * ze) / cn : 0.0;
+      zb = zc;
+      zc = zn;
+    } else {
+      if constexpr (kChain)
+        rho = res;
+      else
+        rho = active ? (((rk - cw * zw) - cs * zb) - cc * zc) - ce * ze : 0.0;
+    }
+  }
+  dv[lane] = rho;
+  __syncwarp();
+  const double v = active ? seg_matvec<MT>(dv, segbase, mt, mw, n) : 0.0;
+  __syncwarp();
+  zs[0] += v;
+  double hb = 0.0, hc = v;
+  float cn_prev_b = 0.f;
+#pragma unroll
+  for (int k = 0; k < HM - 1; ++k) {
+    const float ncc = active ? cc_[k] : 0.f, nce = active ? ce_[k] : 0.f;
+    const float ncn = active ? cn_[k] : 1.f;
+    double cw, cs;
+    if (SYM) {
+      const float arw = __shfl_up_sync(0xffffffffu, nce, 1);
+      cw = (n == 0) ? 0.0 : (double)arw;
+      cs = (double)cn_prev_b;
+      cn_prev_b = ncn;
+    } else {
+      cw = active ? cw_[k] : 0.f;
+      cs = active ? cs_[k] : 0.f;
+    }
+    const double cc = ncc, ce = nce, cn = ncn;
+    const double part = kChain ? -(cs * hb) - cc * hc : 0.0;
+    double hw = __shfl_up_sync(0xffffffffu, hc, 1);
+    double he = __shfl_down_sync(0xffffffffu, hc, 1);
+    if (n == 0) hw = 0.0;
+    if (n >= mw - 1) he = 0.0;
+    double hn;
+    if constexpr (kChain)
+      hn = active ? ((part - cw * hw) - ce * he) * march_rcp(cn) : 0.0;
+    else
+      hn = active ? ((((-(cw * hw)) - cs * hb) - cc * hc) - ce * he) / cn : 0.0;
+    zs[k + 1] += hn;
+    hb = hc;
+    hc = hn;
+  }
+  if (active) {
+#pragma unroll
+    for (int k = 0; k < HM; ++k) emit(k, zs[k]);
+  }
+}
+
 // SEVP march of one task with every row in registers: the forward sweep
 // (particular solution with zero guess rows and block-top corrections) and
 // the backward sweep (guess-row values and homogeneous corrections) of
@@ -640,6 +739,11 @@ __device__ __forceinline__ void march_task_regs(const float (&cc_)[HM], const fl
                                                 const float (&cs_)[SYM ? 1 : HM], int hh, int nb,
                                                 int n, int mw, bool active, int lane, int segbase,
                                                 double *dv, const MT *mt, Rhs &&rhs, Emit &&emit) {
+  if (nb == 1 && hh == HM) {
+    march_task_full<MT, SYM, kChain, HM>(cc_, ce_, cn_, cw_, cs_, n, mw, active, lane, segbase,
+                                         dv, mt, rhs, emit);
+    return;
+  }
   const size_t msz = (size_t)mw * mw;
   // ---- forward sweep
   double zs[HM], rho[HM];
@@ -1241,6 +1345,9 @@ struct sevp_ctx {
   sevp_tiling treq{};
   std::vector<int> treq_rows, treq_tiles;
   int schwarz_req = 0;  // requested column shift of tb: 0 off, -1 automatic
+  // PCG coefficient record of FP64 solves (sevp_record_coefficients)
+  double *hist = nullptr;
+  int hist_cap = 0;
   // Schwarz work vectors: first-stage z and second-stage correction
   double *s1_64 = nullptr, *s2_64 = nullptr;
   float *s1_32 = nullptr, *s2_32 = nullptr;
@@ -1547,7 +1654,7 @@ static void free_work(sevp_ctx *ctx) {
   void *ptrs[] = {ctx->r64, ctx->z64, ctx->p64[0], ctx->p64[1], ctx->q64, ctx->x64s, ctx->r32,
                   ctx->z32, ctx->p32[0], ctx->p32[1], ctx->q32, ctx->d32, ctx->bh, ctx->xh,
                   ctx->e1h, ctx->e2h, ctx->st, ctx->partials, ctx->tickets,
-                  ctx->s1_64, ctx->s2_64, ctx->s1_32, ctx->s2_32};
+                  ctx->s1_64, ctx->s2_64, ctx->s1_32, ctx->s2_32, ctx->hist};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   ctx->ta.release();
@@ -1890,6 +1997,39 @@ extern "C" int sevp_set_schwarz(sevp_ctx *ctx, int shift) {
   return s;
 }
 
+extern "C" int sevp_record_coefficients(sevp_ctx *ctx, int cap) {
+  if (!ctx || cap < 0) return SEVP_BAD_ARG;
+  SEVP_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  if (ctx->hist) cudaFree(ctx->hist), ctx->hist = nullptr;
+  ctx->hist_cap = 0;
+  if (cap > 0) {
+    SEVP_CUDA_TRY(cudaMalloc((void **)&ctx->hist, sizeof(double) * 2 * (size_t)cap));
+    SEVP_CUDA_TRY(cudaMemsetAsync(ctx->hist, 0, sizeof(double) * 2 * (size_t)cap, ctx->stream));
+    ctx->hist_cap = cap;
+  }
+  return SEVP_OK;
+}
+
+extern "C" int sevp_read_coefficients(sevp_ctx *ctx, double *alpha, double *beta, int cap,
+                                      int *count) {
+  if (!ctx || !alpha || !beta || !count || cap < 0) return SEVP_BAD_ARG;
+  *count = 0;
+  if (!ctx->hist) return SEVP_OK;
+  const int n = std::min(cap, ctx->hist_cap);
+  std::vector<double> h((size_t)2 * std::max(n, 1));
+  SEVP_CUDA_TRY(cudaMemcpyAsync(h.data(), ctx->hist, sizeof(double) * 2 * (size_t)n,
+                                cudaMemcpyDeviceToHost, ctx->stream));
+  SEVP_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  int last = 0;
+  for (int j = 0; j < n; ++j) {
+    alpha[j] = h[2 * j];
+    beta[j] = h[2 * j + 1];
+    if (alpha[j] != 0.0) last = j + 1;
+  }
+  *count = last;
+  return SEVP_OK;
+}
+
 extern "C" int sevp_schwarz_shift(const sevp_ctx *ctx) {
   return (ctx && schwarz_on(ctx)) ? ctx->tb.tg.xs : 0;
 }
@@ -1932,10 +2072,13 @@ static int launch_residual(sevp_ctx *ctx, const double *x, const float *d, doubl
   return launch_stencil(ctx, op, 2);
 }
 
-__global__ void k_state_init(SolveState *st, double tol2, int max_iter) {
+__global__ void k_state_init(SolveState *st, double tol2, int max_iter, double *hist = nullptr,
+                             int hist_cap = 0) {
   SolveState s{};
   s.tol2 = tol2;
   s.max_iter = max_iter;
+  s.hist = hist;
+  s.hist_cap = hist_cap;
   s.status = SEVP_OK;
   *st = s;
 }
@@ -2028,7 +2171,9 @@ static int solve_fp64(sevp_ctx *ctx, const double *b, double *x, const sevp_solv
   const double tol2 = o->tol * o->tol;
   int total = 0, status = SEVP_OK;
   for (int restart = 0; restart < 6; ++restart) {
-    k_state_init<<<1, 1, 0, ctx->stream>>>(ctx->st, tol2, std::max(o->max_iter - total, 0));
+    // the coefficients of the first PCG run are recorded when asked for
+    k_state_init<<<1, 1, 0, ctx->stream>>>(ctx->st, tol2, std::max(o->max_iter - total, 0),
+                                           restart == 0 ? ctx->hist : nullptr, ctx->hist_cap);
     ctx->launches++;
     // r = b - A x
     int s = launch_residual<double>(ctx, x, nullptr, nullptr, b, ctx->r64, 0, tol2);

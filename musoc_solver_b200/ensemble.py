@@ -34,7 +34,7 @@ def member_tile_height(ny: int, prefer=(8, 12, 6, 10, 16, 18, 20, 15, 24)) -> in
 
 class EnsembleSolver:
     def __init__(self, members, tile_m: int = 16, tile_h: int | None = None, growth_limit=1e10,
-                 device="cuda", stream=None):
+                 device="cuda", stream=None, schwarz=False):
         import torch
 
         self.torch = torch
@@ -46,7 +46,7 @@ class EnsembleSolver:
         if self.ny % th:
             raise ValueError("tile height must divide the member row count")
         self.solver = SevpSolver(self.problem, tile_m=tile_m, tile_h=th, growth_limit=growth_limit,
-                                 device=device, stream=stream)
+                                 device=device, stream=stream, schwarz=schwarz)
         self.device = self.solver.device
 
     def rhs(self):
@@ -56,12 +56,13 @@ class EnsembleSolver:
     def member_norms(self, v):
         return v.reshape(self.m, -1).norm(dim=1)
 
-    def solve(self, b, x=None, precision=1, tol=1e-12, max_iter=5000):
+    def solve(self, b, x=None, precision=1, tol=1e-12, max_iter=5000, inner_tol=1e-5):
         """Solves all members; returns (x, result, per-member relative
         residuals as a host array)."""
         bn = self.member_norms(b)
         tol_stack = tol * float(bn.min() / b.norm()) if float(b.norm()) > 0 else tol
-        x, res = self.solver.solve(b, x=x, precision=precision, tol=tol_stack, max_iter=max_iter)
+        x, res = self.solver.solve(b, x=x, precision=precision, tol=tol_stack, max_iter=max_iter,
+                                   inner_tol=inner_tol)
         return x, res, self.member_residuals(b, x)
 
     def member_residuals(self, b, x):

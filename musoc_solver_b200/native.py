@@ -87,6 +87,8 @@ _SIGS = {
     "sevp_set_graphs": ([P, C.c_int], C.c_int),
     "sevp_set_schwarz": ([P, C.c_int], C.c_int),
     "sevp_schwarz_shift": ([P], C.c_int),
+    "sevp_record_coefficients": ([P, C.c_int], C.c_int),
+    "sevp_read_coefficients": ([P, DP, DP, C.c_int, C.POINTER(C.c_int)], C.c_int),
     "sevp_schwarz_influence_bytes": ([P], C.c_longlong),
     "sevp_inprod_noalloc": ([P, P, C.c_int, C.c_int, P, P], C.c_int),
     "sevp_fs_mask": ([C.c_int, C.c_int, P, P, P, P, C.c_int, P], C.c_int),

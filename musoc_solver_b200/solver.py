@@ -193,6 +193,39 @@ class SevpSolver:
         """Column shift of the second tiling (0: block-Jacobi)."""
         return int(N.lib().sevp_schwarz_shift(self.h))
 
+    def condition_estimate(self, b, cap: int = 4000, tol: float = 1e-12):
+        """Extreme eigenvalues of the preconditioned operator M^-1 A (the
+        context's preconditioner): one FP64 PCG solve of ``b`` from zero
+        records its coefficients alpha_j, beta_j on the device; the Ritz
+        values of the CG-Lanczos tridiagonal (diagonal 1/alpha_j +
+        beta_{j-1}/alpha_{j-1}, off-diagonal sqrt(beta_j)/alpha_j) estimate
+        them from inside.  Returns dict(lambda_min, lambda_max, kappa,
+        iterations)."""
+        lib = N.lib()
+        N.check(lib.sevp_record_coefficients(self.h, int(cap)), "sevp_record_coefficients")
+        try:
+            x = self.torch.zeros_like(b)
+            self.solve(b, x=x, precision=0, tol=tol, max_iter=cap)
+            a = np.zeros(cap)
+            bt = np.zeros(cap)
+            cnt = C.c_int()
+            N.check(lib.sevp_read_coefficients(self.h, a.ctypes.data_as(N.DP),
+                                               bt.ctypes.data_as(N.DP), int(cap), C.byref(cnt)),
+                    "sevp_read_coefficients")
+        finally:
+            lib.sevp_record_coefficients(self.h, 0)
+        k = cnt.value
+        if k == 0:
+            raise RuntimeError("no PCG iterations were recorded")
+        a, bt = a[:k], bt[:k]
+        d = 1.0 / a
+        d[1:] += bt[:-1] / a[:-1]
+        e = np.sqrt(bt[:-1]) / a[:-1]
+        T = np.diag(d) + np.diag(e, 1) + np.diag(e, -1)
+        ev = np.linalg.eigvalsh(T)
+        return dict(lambda_min=float(ev[0]), lambda_max=float(ev[-1]),
+                    kappa=float(ev[-1] / ev[0]), iterations=k)
+
     def schwarz_influence_bytes(self) -> int:
         return int(N.lib().sevp_schwarz_influence_bytes(self.h))
 

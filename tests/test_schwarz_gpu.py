@@ -159,3 +159,32 @@ def test_schwarz_rejects_bad_shapes(torch_cuda):
         s2.set_schwarz(16)         # shift must be inside a tile
     s2.set_schwarz(5)
     assert s2.schwarz_shift == 5
+
+
+@pytest.mark.parametrize("schwarz", [False, True])
+def test_condition_estimate_matches_dense_spectrum(torch_cuda, oracle, schwarz):
+    """Ritz values from the recorded PCG coefficients against the dense
+    spectrum of M^-1 A built with the oracle's preconditioner (small grid)."""
+    torch = torch_cuda
+    from musoc_solver_b200.solver import SevpSolver, tile_sub_blocks
+
+    p = P.global_grid(48, 24, seed=13)
+    s = SevpSolver(p, tile_m=16, tile_h=6, growth_limit=GROWTH, schwarz=schwarz)
+    rng = np.random.default_rng(14)
+    b = rng.standard_normal((p.ny, p.nx))
+    est = s.condition_estimate(torch.from_numpy(b).cuda())
+    if schwarz:
+        pc = oracle.SchwarzPC(p, 16, 6, s.schwarz_shift, s.tile_nb,
+                              tile_sub_blocks(oracle.rolled_grid(p, s.schwarz_shift), 16, 6, GROWTH))
+    else:
+        pc = oracle.TilePC(p, 16, 6, tile_nb=s.tile_nb)
+    n = p.nx * p.ny
+    MA = np.zeros((n, n))
+    for j in range(n):
+        e = np.zeros(n)
+        e[j] = 1.0
+        MA[:, j] = pc.apply(oracle.apply(p, e.reshape(p.ny, p.nx))).ravel()
+    ev = np.sort(np.linalg.eigvals(MA).real)
+    assert abs(est["lambda_max"] - ev[-1]) <= 1e-3 * ev[-1]
+    assert abs(est["lambda_min"] - ev[0]) <= 1e-2 * ev[0]
+    assert est["iterations"] >= 2
