@@ -26,11 +26,14 @@ import numpy as np
 from . import native as N
 from .unet import UNet, lib as nnlib
 
+COARSE = (1, 2, 4, 8)
+
+
 def net_grid(nx: int, ny: int, coarse: int):
     """(H, W) of the network for a solver grid averaged over coarse x coarse
     cells, rounded up to multiples of 8."""
-    if coarse not in (1, 2, 4) or nx % coarse or ny % coarse:
-        raise ValueError("coarse must be 1, 2 or 4 and divide the grid")
+    if coarse not in COARSE or nx % coarse or ny % coarse:
+        raise ValueError("coarse must be 1, 2, 4 or 8 and divide the grid")
     r8 = lambda v: (v + 7) // 8 * 8
     return r8(ny // coarse), r8(nx // coarse)
 
@@ -50,10 +53,10 @@ class LearnedWarmStart:
         self.net = unet
         # the network grid: the solver grid averaged over coarse x coarse
         # cells, padded to multiples of 8
-        self.coarse = next((c for c in (1, 2, 4) if net_grid(solver.nx, solver.ny, c) ==
-                            (unet.H, unet.W)), None)
+        self.coarse = next((c for c in COARSE if solver.nx % c == 0 and solver.ny % c == 0
+                            and net_grid(solver.nx, solver.ny, c) == (unet.H, unet.W)), None)
         if self.coarse is None:
-            raise ValueError("network grid does not match the solver grid at coarse 1, 2 or 4")
+            raise ValueError("network grid does not match the solver grid at coarse 1, 2, 4 or 8")
         self._g = (self.coarse, unet.W, unet.H)
         n = unet.H * unet.W
         dev = solver.device
@@ -164,7 +167,7 @@ class LearnedWarmStart:
     @classmethod
     def create(cls, solver, seed=0, train=True, coarse=1):
         """A fresh network on the solver grid averaged over coarse x coarse
-        cells (coarse = 1, 2 or 4)."""
+        cells (coarse = 1, 2, 4 or 8)."""
         H, W = net_grid(solver.nx, solver.ny, coarse)
         net = UNet(H, W, device=solver.device, train=train, seed=seed, stream=solver.stream)
         return cls(solver, net, use_graph=not train)

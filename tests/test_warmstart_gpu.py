@@ -15,7 +15,7 @@ from musoc_solver_b200 import problems as P
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("coarse", [1, 2, 4])
+@pytest.mark.parametrize("coarse", [1, 2, 4, 8])
 def test_learned_warm_start_beats_no_network(torch_cuda_ws, coarse):
     torch = torch_cuda_ws
     from musoc_solver_b200 import native as N
