@@ -57,13 +57,15 @@ def test_fs_kernels_bit_exact(torch_cuda_b, oracle):
     bc.close()
 
 
-def test_fs_loop_matches_oracle_loop(torch_cuda_b, oracle):
+@pytest.mark.parametrize("schwarz", [False, True])
+def test_fs_loop_matches_oracle_loop(torch_cuda_b, oracle, schwarz):
     torch = torch_cuda_b
     from musoc_solver_b200.barotropic import BarotropicCorrection
     from musoc_solver_b200.solver import tile_sub_blocks
 
     st = P.fs_state(64, 32, 4, seed=6)
-    bc = BarotropicCorrection(st, tile_m=16, tile_h=8)
+    bc = BarotropicCorrection(st, tile_m=16, tile_h=8, schwarz=schwarz)
+    assert bool(bc.solver.schwarz_shift) == schwarz
     u, v, p0, scr = bc.upload()
     tolerance, mxmask = 1e-6, 5
     passes, vm, iters = bc.run(u, v, p0, scr, tolerance=tolerance, mxmask=mxmask, precision=0)

@@ -37,13 +37,15 @@ def test_graph_replay_matches_direct_launches(torch_cuda_e):
     assert r1.rel_residual <= 1e-12
 
 
-def test_ensemble_members_reach_tolerance_and_match_single_solves(torch_cuda_e, oracle):
+@pytest.mark.parametrize("schwarz", [False, True])
+def test_ensemble_members_reach_tolerance_and_match_single_solves(torch_cuda_e, oracle, schwarz):
     torch = torch_cuda_e
     from musoc_solver_b200.ensemble import EnsembleSolver
     from musoc_solver_b200.solver import SevpSolver
 
     members = P.ensemble(members=4, nx=96, ny=48, seed=9)
-    e = EnsembleSolver(members)
+    e = EnsembleSolver(members, schwarz=schwarz)
+    assert bool(e.solver.schwarz_shift) == schwarz
     b = e.rhs()
     x, res, rel = e.solve(b, precision=1)
     assert res.status == 0
