@@ -182,6 +182,8 @@ def make_sequence(nx, ny, nsteps):
 
 
 def dist_setup(args):
+    """One process per GPU (torchrun): NCCL on the GPU box; gloo on a host
+    without a GPU, where only the CPU reference arm runs."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -193,9 +195,22 @@ def dist_setup(args):
         import torch.distributed as dist
 
         os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
     return world, rank, local, dist
+
+
+def max_over_ranks(v, dist, device):
+    """The largest v over all ranks (the job's time is its slowest rank's)."""
+    if dist is None:
+        return v
+    import torch
+
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 # ------------------------------------------------------------ CPU oracle
@@ -427,12 +442,6 @@ def run_native(args, world, rank, local, dist):
             dist.barrier()
         torch.cuda.synchronize()
 
-    def max_over_ranks(v):
-        if dist is None:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
 
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     timed = range(T + W, T + W + K)
@@ -451,7 +460,7 @@ def run_native(args, world, rank, local, dist):
             reps.append(r)
         ev1.record(stream)
         torch.cuda.synchronize()
-        return max_over_ranks(ev0.elapsed_time(ev1) / 1e3), reps
+        return max_over_ranks(ev0.elapsed_time(ev1) / 1e3, dist, dev), reps
 
     # ---- value arm: mixed precision + warm start, device-resident inputs
     solver.profile(True)
@@ -489,7 +498,7 @@ def run_native(args, world, rank, local, dist):
             its.append(r.iterations)
         ev1.record(stream)
         torch.cuda.synchronize()
-        return max_over_ranks(ev0.elapsed_time(ev1) / 1e3), its
+        return max_over_ranks(ev0.elapsed_time(ev1) / 1e3, dist, dev), its
 
     if use_sw:
         solver.set_schwarz(0)
@@ -511,7 +520,7 @@ def run_native(args, world, rank, local, dist):
         itmz.append(r.iterations)
     ev1.record(stream)
     torch.cuda.synchronize()
-    t_mixed0 = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
+    t_mixed0 = max_over_ranks(ev0.elapsed_time(ev1) / 1e3, dist, dev)
 
     # ---- e2e: the same value arm through the C ABI with host buffers
     pin = lambda a: torch.from_numpy(a).pin_memory().numpy()
@@ -529,7 +538,7 @@ def run_native(args, world, rank, local, dist):
         solver.solve_step_host(b_host[k], eta_host[k - 1], eta_host[k - 2], eta_host[k],
                                guess=guess_mode, precision=1, inner_tol=itol)
     torch.cuda.synchronize()
-    t_e2e = max_over_ranks(time.perf_counter() - t0)
+    t_e2e = max_over_ranks(time.perf_counter() - t0, dist, dev)
     launches_e2e = solver.launches() - l1
     h2d = 8 * n * (3 if guess_mode in (N.GUESS_LINEAR, N.GUESS_LEARNED) else 2)
     d2h = 8 * n
