@@ -404,6 +404,12 @@ def run_native(args, world, rank, local, dist):
         tiles, use_sw, itol = (best["tile_m"], best["tile_h"]), best["schwarz"], best["inner_tol"]
     else:
         tiles, use_sw, itol = cands[0], sw_opts[0], itols[0]
+    if dist is not None:
+        # every rank runs the same arms (and so the same collectives): rank
+        # 0's choice holds for all
+        choice = [(tuple(tiles), bool(use_sw), float(itol))]
+        dist.broadcast_object_list(choice, src=0)
+        tiles, use_sw, itol = choice[0]
     if use_sw and tiles[1] > SCHWARZ_MAX_ROWS:
         raise SystemExit(f"the Schwarz preconditioner needs tiles of at most {SCHWARZ_MAX_ROWS} rows")
     solver = SevpSolver(p, tile_m=tiles[0], tile_h=tiles[1], growth_limit=GROWTH,
