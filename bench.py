@@ -528,26 +528,51 @@ def run_native(args, world, rank, local, dist):
     torch.cuda.synchronize()
     t_mixed0 = max_over_ranks(ev0.elapsed_time(ev1) / 1e3, dist, dev)
 
-    # ---- e2e: the same value arm through the C ABI with host buffers
+    # ---- e2e: the same value arm through the C ABI with host buffers.
+    #      The context keeps the last two solutions in device memory, so a
+    #      step copies b in and x out (pinned buffers).  Headline: the
+    #      asynchronous steps (step n+1's b prefetched during step n's
+    #      solve, x copied out on a copy stream); beside it the synchronous
+    #      step, and the steps with the history copied in every step.
     pin = lambda a: torch.from_numpy(a).pin_memory().numpy()
     b_host = {k: pin(rhs[k]) for k in range(T, T + W + K)}
     eta_host = {k: pin(np.zeros((p.ny, p.nx))) for k in range(T - 2, T + W + K)}
     for k in (T - 2, T - 1):
         eta_host[k][:] = eta[k].cpu().numpy()
+    solver.step_history(eta_host[T - 1], eta_host[T - 2])
     for k in range(T, T + W):
-        solver.solve_step_host(b_host[k], eta_host[k - 1], eta_host[k - 2], eta_host[k],
-                               guess=guess_mode, precision=1, inner_tol=itol)
+        solver.step_submit(b_host[k], eta_host[k], guess=guess_mode, precision=1, inner_tol=itol)
+    solver.step_wait()
     barrier()
     t0 = time.perf_counter()
     l1 = solver.launches()
+    solver.step_prefetch(b_host[timed[0]])
+    for k in timed:
+        if k + 1 in timed:
+            solver.step_prefetch(b_host[k + 1])
+        solver.step_submit(b_host[k], eta_host[k], guess=guess_mode, precision=1, inner_tol=itol)
+    solver.step_wait()
+    torch.cuda.synchronize()
+    t_e2e = max_over_ranks(time.perf_counter() - t0, dist, dev)
+    launches_e2e = solver.launches() - l1
+    h2d = 8 * n
+    d2h = 8 * n
+    # the synchronous step (history on the device, copies not overlapped)
+    solver.step_history(eta_host[timed[0] - 1], eta_host[timed[0] - 2])
+    barrier()
+    t0 = time.perf_counter()
+    for k in timed:
+        solver.step_host(b_host[k], eta_host[k], guess=guess_mode, precision=1, inner_tol=itol)
+    torch.cuda.synchronize()
+    t_e2e_sync = max_over_ranks(time.perf_counter() - t0, dist, dev)
+    barrier()
+    t0 = time.perf_counter()
     for k in timed:
         solver.solve_step_host(b_host[k], eta_host[k - 1], eta_host[k - 2], eta_host[k],
                                guess=guess_mode, precision=1, inner_tol=itol)
     torch.cuda.synchronize()
-    t_e2e = max_over_ranks(time.perf_counter() - t0, dist, dev)
-    launches_e2e = solver.launches() - l1
-    h2d = 8 * n * (3 if guess_mode in (N.GUESS_LINEAR, N.GUESS_LEARNED) else 2)
-    d2h = 8 * n
+    t_e2e_hist = max_over_ranks(time.perf_counter() - t0, dist, dev)
+    h2d_hist = 8 * n * (3 if guess_mode in (N.GUESS_LINEAR, N.GUESS_LEARNED) else 2)
 
     # ---- roofline of the dominant kernel (FP32 vectors): pass B with the
     #      block-Jacobi preconditioner, the Schwarz stage kernel otherwise
@@ -649,7 +674,15 @@ def run_native(args, world, rank, local, dist):
                       "max_rel_err_vs_fp64": float(max(errs))},
         "speedup_vs_fp64_plain": (K / t_value) / (K / t_fp64),
         "e2e": {"value": world * K / t_e2e, "unit": "solves/s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h},
+                "d2h_bytes_per_step": d2h,
+                "api": "sevp_step_prefetch / sevp_step_submit / sevp_step_wait (history of the "
+                       "two previous solutions held in HBM; copies overlapped with the solves)"},
+        "e2e_step_host": {"value": world * K / t_e2e_sync, "unit": "solves/s",
+                          "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                          "api": "sevp_step_host (history in HBM, copies not overlapped)"},
+        "e2e_history_from_host": {"value": world * K / t_e2e_hist, "unit": "solves/s",
+                                  "h2d_bytes_per_step": h2d_hist, "d2h_bytes_per_step": d2h,
+                                  "api": "sevp_solve_step_host (b, eta1, eta2 copied in)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                      "kernel": dom_name,

@@ -257,6 +257,28 @@ int sevp_set_warmstart(sevp_ctx *ctx, sevp_warmstart_fn fn, void *user, int laun
  * from that guess (device pointers; eta1/eta2 may be NULL when unused). */
 int sevp_solve_step(sevp_ctx *ctx, const double *b, const double *eta1, const double *eta2,
                     double *x, int guess_mode, const sevp_solve_opts *opts, sevp_report *report);
+/* Time stepping with the history held on the device (not part of the
+ * reference interface; the reference's FS_SOLVER passes the previous
+ * solution in X, M/fs_GLOBAL.f90:1852).  The context keeps the last two
+ * solutions in device memory, so a step copies only b in and x out:
+ * sevp_step_host solves A x = b from the guess of guess_mode built from
+ * that history (zero while it is empty, the previous solution while it holds
+ * one) and then makes x the newest solution.  sevp_step_history loads a
+ * history from host arrays (eta2 may be NULL; both NULL empties it). */
+int sevp_step_history(sevp_ctx *ctx, const double *eta1_host, const double *eta2_host);
+int sevp_step_host(sevp_ctx *ctx, const double *b_host, double *x_host, int guess_mode,
+                   const sevp_solve_opts *opts, sevp_report *report);
+/* Asynchronous stepping with the same device history.  sevp_step_submit
+ * stages b (or takes the copy that sevp_step_prefetch started), solves, and
+ * starts copying x out on a copy stream; it returns when the solve is done,
+ * before x has arrived.  sevp_step_wait waits for the submitted x copies.
+ * Prefetching step n+1's b before submitting step n overlaps that copy with
+ * the solve.  b_host and x_host must be pinned and left untouched until
+ * sevp_step_wait returns. */
+int sevp_step_prefetch(sevp_ctx *ctx, const double *b_host);
+int sevp_step_submit(sevp_ctx *ctx, const double *b_host, double *x_host, int guess_mode,
+                     const sevp_solve_opts *opts, sevp_report *report);
+int sevp_step_wait(sevp_ctx *ctx);
 /* Same with host buffers: copies b, eta1, eta2 in and x out inside the call. */
 int sevp_solve_step_host(sevp_ctx *ctx, const double *b_host, const double *eta1_host,
                          const double *eta2_host, double *x_host, int guess_mode,

@@ -1360,6 +1360,19 @@ struct sevp_ctx {
   double *bh = nullptr;  // device staging for host solves
   double *xh = nullptr;
   double *e1h = nullptr, *e2h = nullptr;
+  // time stepping with the history held on the device (sevp_step_host):
+  // three rotating buffers, the last two solutions and the next output
+  double *step_buf[3] = {nullptr, nullptr, nullptr};
+  int step_e1 = 0, step_e2 = 1, step_hist = 0;
+  // asynchronous stepping: b staged on a copy-in stream (two buffers), x
+  // copied out on a copy-out stream; events order the reuse of the buffers
+  cudaStream_t cp_in = nullptr, cp_out = nullptr;
+  double *bstage[2] = {nullptr, nullptr};
+  const double *bstage_src[2] = {nullptr, nullptr};
+  int bstage_next = 0;
+  cudaEvent_t ev_in[2] = {nullptr, nullptr}, ev_out[3] = {nullptr, nullptr, nullptr};
+  bool ev_out_set[3] = {false, false, false};
+  cudaEvent_t ev_solved = nullptr;
   // learned warm start (bound by the network module)
   sevp_warmstart_fn warm_fn = nullptr;
   void *warm_user = nullptr;
@@ -1654,12 +1667,19 @@ static void free_work(sevp_ctx *ctx) {
   void *ptrs[] = {ctx->r64, ctx->z64, ctx->p64[0], ctx->p64[1], ctx->q64, ctx->x64s, ctx->r32,
                   ctx->z32, ctx->p32[0], ctx->p32[1], ctx->q32, ctx->d32, ctx->bh, ctx->xh,
                   ctx->e1h, ctx->e2h, ctx->st, ctx->partials, ctx->tickets,
+                  ctx->step_buf[0], ctx->step_buf[1], ctx->step_buf[2], ctx->bstage[0],
+                  ctx->bstage[1],
                   ctx->s1_64, ctx->s2_64, ctx->s1_32, ctx->s2_32, ctx->hist};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   ctx->ta.release();
   ctx->tb.release();
   if (ctx->h_st) cudaFreeHost(ctx->h_st);
+  for (cudaEvent_t e : {ctx->ev_in[0], ctx->ev_in[1], ctx->ev_out[0], ctx->ev_out[1],
+                        ctx->ev_out[2], ctx->ev_solved})
+    if (e) cudaEventDestroy(e);
+  for (cudaStream_t st : {ctx->cp_in, ctx->cp_out})
+    if (st) cudaStreamDestroy(st);
   for (auto &pr : ctx->ev_pool) cudaEventDestroy(pr.first), cudaEventDestroy(pr.second);
   ctx->ev_pool.clear();
 }
@@ -2401,6 +2421,137 @@ extern "C" int sevp_solve_step_host(sevp_ctx *ctx, const double *bh, const doubl
   SEVP_CUDA_TRY(cudaMemcpyAsync(xh, ctx->xh, bytes, cudaMemcpyDeviceToHost, ctx->stream));
   SEVP_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   return s;
+}
+
+// ---------------------------------------------- stepping with device history
+static int ensure_step_buffers(sevp_ctx *ctx) {
+  for (double *&p : ctx->step_buf)
+    if (!p) SEVP_CUDA_TRY(cudaMalloc((void **)&p, ctx->n * 8));
+  if (!ctx->bh) SEVP_CUDA_TRY(cudaMalloc((void **)&ctx->bh, ctx->n * 8));
+  return SEVP_OK;
+}
+
+extern "C" int sevp_step_history(sevp_ctx *ctx, const double *eta1_host, const double *eta2_host) {
+  if (!ctx || (!eta1_host && eta2_host)) return SEVP_BAD_ARG;
+  int s = ensure_step_buffers(ctx);
+  if (s) return s;
+  // x copies of submitted steps may still read the buffers
+  if (ctx->cp_out) SEVP_CUDA_TRY(cudaStreamSynchronize(ctx->cp_out));
+  const size_t bytes = ctx->n * 8;
+  ctx->step_e1 = 0, ctx->step_e2 = 1, ctx->step_hist = 0;
+  if (eta1_host) {
+    SEVP_CUDA_TRY(cudaMemcpyAsync(ctx->step_buf[0], eta1_host, bytes, cudaMemcpyHostToDevice,
+                                  ctx->stream));
+    ctx->step_hist = 1;
+  }
+  if (eta2_host) {
+    SEVP_CUDA_TRY(cudaMemcpyAsync(ctx->step_buf[1], eta2_host, bytes, cudaMemcpyHostToDevice,
+                                  ctx->stream));
+    ctx->step_hist = 2;
+  }
+  SEVP_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return SEVP_OK;
+}
+
+extern "C" int sevp_step_host(sevp_ctx *ctx, const double *bh, double *xh, int guess_mode,
+                              const sevp_solve_opts *o, sevp_report *rep) {
+  if (!ctx || !ctx->have_op || !bh || !xh || !o || guess_mode < 0 || guess_mode > 3)
+    return SEVP_BAD_ARG;
+  int s = ensure_step_buffers(ctx);
+  if (s) return s;
+  const size_t bytes = ctx->n * 8;
+  SEVP_CUDA_TRY(cudaMemcpyAsync(ctx->bh, bh, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  // the guess needs as much history as there is
+  int mode = guess_mode;
+  if (ctx->step_hist == 0) mode = SEVP_GUESS_ZERO;
+  if (ctx->step_hist == 1 && mode > SEVP_GUESS_PREVIOUS) mode = SEVP_GUESS_PREVIOUS;
+  const int out = 3 - ctx->step_e1 - ctx->step_e2;  // the buffer holding neither
+  if (ctx->ev_out_set[out]) SEVP_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, ctx->ev_out[out], 0));
+  s = sevp_solve_step(ctx, ctx->bh, ctx->step_buf[ctx->step_e1], ctx->step_buf[ctx->step_e2],
+                      ctx->step_buf[out], mode, o, rep);
+  if (s != SEVP_OK && s != SEVP_MAXITER) return s;
+  SEVP_CUDA_TRY(cudaMemcpyAsync(xh, ctx->step_buf[out], bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  SEVP_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  ctx->step_e2 = ctx->step_e1;
+  ctx->step_e1 = out;
+  ctx->step_hist = std::min(ctx->step_hist + 1, 2);
+  return s;
+}
+
+static int ensure_async_step(sevp_ctx *ctx) {
+  int s = ensure_step_buffers(ctx);
+  if (s) return s;
+  if (ctx->cp_in) return SEVP_OK;
+  SEVP_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->cp_in, cudaStreamNonBlocking));
+  SEVP_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->cp_out, cudaStreamNonBlocking));
+  for (double *&p : ctx->bstage) SEVP_CUDA_TRY(cudaMalloc((void **)&p, ctx->n * 8));
+  for (cudaEvent_t &e : ctx->ev_in) SEVP_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  for (cudaEvent_t &e : ctx->ev_out) SEVP_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  SEVP_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_solved, cudaEventDisableTiming));
+  return SEVP_OK;
+}
+
+// Starts the copy of a step's b into the next staging buffer on the copy-in
+// stream.  A staging buffer is reused only after the solve that read it has
+// returned (the solves are synchronous), so two are enough.
+static int stage_b(sevp_ctx *ctx, const double *bh) {
+  const int k = ctx->bstage_next;
+  ctx->bstage_next ^= 1;
+  SEVP_CUDA_TRY(cudaMemcpyAsync(ctx->bstage[k], bh, ctx->n * 8, cudaMemcpyHostToDevice, ctx->cp_in));
+  SEVP_CUDA_TRY(cudaEventRecord(ctx->ev_in[k], ctx->cp_in));
+  ctx->bstage_src[k] = bh;
+  return SEVP_OK;
+}
+
+extern "C" int sevp_step_prefetch(sevp_ctx *ctx, const double *bh) {
+  if (!ctx || !bh) return SEVP_BAD_ARG;
+  int s = ensure_async_step(ctx);
+  return s ? s : stage_b(ctx, bh);
+}
+
+extern "C" int sevp_step_submit(sevp_ctx *ctx, const double *bh, double *xh, int guess_mode,
+                                const sevp_solve_opts *o, sevp_report *rep) {
+  if (!ctx || !ctx->have_op || !bh || !xh || !o || guess_mode < 0 || guess_mode > 3)
+    return SEVP_BAD_ARG;
+  int s = ensure_async_step(ctx);
+  if (s) return s;
+  // b: the staged copy when it was prefetched, else staged now
+  int k = -1;
+  for (int q = 0; q < 2; ++q)
+    if (ctx->bstage_src[q] == bh) k = q;
+  if (k < 0) {
+    k = ctx->bstage_next;
+    s = stage_b(ctx, bh);
+    if (s) return s;
+  }
+  ctx->bstage_src[k] = nullptr;  // consumed by this step
+  SEVP_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, ctx->ev_in[k], 0));
+  int mode = guess_mode;
+  if (ctx->step_hist == 0) mode = SEVP_GUESS_ZERO;
+  if (ctx->step_hist == 1 && mode > SEVP_GUESS_PREVIOUS) mode = SEVP_GUESS_PREVIOUS;
+  const int out = 3 - ctx->step_e1 - ctx->step_e2;
+  // the output buffer's previous contents must have left for the host
+  if (ctx->ev_out_set[out]) SEVP_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, ctx->ev_out[out], 0));
+  s = sevp_solve_step(ctx, ctx->bstage[k], ctx->step_buf[ctx->step_e1],
+                      ctx->step_buf[ctx->step_e2], ctx->step_buf[out], mode, o, rep);
+  if (s != SEVP_OK && s != SEVP_MAXITER) return s;
+  // x leaves on the copy-out stream while the caller goes on
+  SEVP_CUDA_TRY(cudaEventRecord(ctx->ev_solved, ctx->stream));
+  SEVP_CUDA_TRY(cudaStreamWaitEvent(ctx->cp_out, ctx->ev_solved, 0));
+  SEVP_CUDA_TRY(cudaMemcpyAsync(xh, ctx->step_buf[out], ctx->n * 8, cudaMemcpyDeviceToHost,
+                                ctx->cp_out));
+  SEVP_CUDA_TRY(cudaEventRecord(ctx->ev_out[out], ctx->cp_out));
+  ctx->ev_out_set[out] = true;
+  ctx->step_e2 = ctx->step_e1;
+  ctx->step_e1 = out;
+  ctx->step_hist = std::min(ctx->step_hist + 1, 2);
+  return s;
+}
+
+extern "C" int sevp_step_wait(sevp_ctx *ctx) {
+  if (!ctx) return SEVP_BAD_ARG;
+  if (ctx->cp_out) SEVP_CUDA_TRY(cudaStreamSynchronize(ctx->cp_out));
+  return SEVP_OK;
 }
 
 // ---------------------------------------------------- learned warm start

@@ -88,6 +88,11 @@ _SIGS = {
     "sevp_set_schwarz": ([P, C.c_int], C.c_int),
     "sevp_schwarz_shift": ([P], C.c_int),
     "sevp_record_coefficients": ([P, C.c_int], C.c_int),
+    "sevp_step_history": ([P, P, P], C.c_int),
+    "sevp_step_host": ([P, P, P, C.c_int, P, P], C.c_int),
+    "sevp_step_prefetch": ([P, P], C.c_int),
+    "sevp_step_submit": ([P, P, P, C.c_int, P, P], C.c_int),
+    "sevp_step_wait": ([P], C.c_int),
     "sevp_read_coefficients": ([P, DP, DP, C.c_int, C.POINTER(C.c_int)], C.c_int),
     "sevp_schwarz_influence_bytes": ([P], C.c_longlong),
     "sevp_inprod_noalloc": ([P, P, C.c_int, C.c_int, P, P], C.c_int),

@@ -294,6 +294,47 @@ class SevpSolver:
         return x, SolveResult(rep.status, rep.iterations, rep.refinements, rep.rel_residual,
                               rep.bnorm, rep.ms)
 
+    def step_history(self, eta1=None, eta2=None):
+        """Loads the device-held history of step_host from host arrays (eta1
+        the newest; both None empties it)."""
+        keep = [np.ascontiguousarray(a, np.float64) for a in (eta1, eta2) if a is not None]
+        N.check(N.lib().sevp_step_history(self.h, *(N.ptr(a) for a in keep),
+                                          *([None] * (2 - len(keep)))), "sevp_step_history")
+
+    def step_host(self, b, x, guess=N.GUESS_LINEAR, precision=1, tol=1e-12, max_iter=5000,
+                  inner_tol=1e-5, check_every=4):
+        """One time step with the history held on the device: copies b (host)
+        in and the solution into x (host) out; x becomes the newest solution
+        of the history."""
+        o = self.opts(precision, tol, max_iter, inner_tol, True, check_every)
+        rep = N.Report()
+        s = N.lib().sevp_step_host(self.h, N.ptr(b), N.ptr(x), int(guess), C.byref(o),
+                                   C.byref(rep))
+        if s not in (N.SEVP_OK, N.SEVP_MAXITER):
+            raise N.SevpError(s, "sevp_step_host")
+        return x, SolveResult(rep.status, rep.iterations, rep.refinements, rep.rel_residual,
+                              rep.bnorm, rep.ms)
+
+    def step_prefetch(self, b):
+        """Starts copying a later step's b (pinned host array) to the device."""
+        N.check(N.lib().sevp_step_prefetch(self.h, N.ptr(b)), "sevp_step_prefetch")
+
+    def step_submit(self, b, x, guess=N.GUESS_LINEAR, precision=1, tol=1e-12, max_iter=5000,
+                    inner_tol=1e-5, check_every=4):
+        """step_host without waiting for x: the copy of x (pinned host array)
+        completes by the next step_wait."""
+        o = self.opts(precision, tol, max_iter, inner_tol, True, check_every)
+        rep = N.Report()
+        s = N.lib().sevp_step_submit(self.h, N.ptr(b), N.ptr(x), int(guess), C.byref(o),
+                                     C.byref(rep))
+        if s not in (N.SEVP_OK, N.SEVP_MAXITER):
+            raise N.SevpError(s, "sevp_step_submit")
+        return SolveResult(rep.status, rep.iterations, rep.refinements, rep.rel_residual,
+                           rep.bnorm, rep.ms)
+
+    def step_wait(self):
+        N.check(N.lib().sevp_step_wait(self.h), "sevp_step_wait")
+
     def apply(self, x):
         y = self.torch.empty_like(x)
         N.check(N.lib().sevp_apply(self.h, N.ptr(x), N.ptr(y)), "sevp_apply")

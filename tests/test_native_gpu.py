@@ -205,3 +205,71 @@ def test_mixed_with_fp32_influence(torch_cuda):
     assert rep.status == 0 and rep.rel_residual <= 1e-12
     res = np.linalg.norm(p.b - P.apply_operator(p, x.cpu().numpy())) / np.linalg.norm(p.b)
     assert res <= 2e-12
+
+
+def test_step_host_keeps_history_on_device(torch_cuda):
+    """sevp_step_host (history in device memory, b in and x out per step)
+    gives the same solutions as device steps with the history passed in."""
+    torch = torch_cuda
+    from musoc_solver_b200 import native as N
+
+    p = P.global_grid(180, 90, seed=7)
+    rhs = [np.ascontiguousarray(b) for _, b in P.eddy_rhs(180, 90, range(6), seed=2)]
+    s1, s2 = _solver(p, 16, 6), _solver(p, 16, 6)
+    etas = []
+    for n, b in enumerate(rhs):
+        mode = N.GUESS_ZERO if n == 0 else (N.GUESS_PREVIOUS if n == 1 else N.GUESS_LINEAR)
+        x = torch.zeros((p.ny, p.nx), dtype=torch.float64, device="cuda")
+        s1.solve_step(torch.from_numpy(b).cuda(), etas[-1] if n >= 1 else None,
+                      etas[-2] if n >= 2 else None, x, guess=mode, precision=1)
+        etas.append(x)
+    for n, b in enumerate(rhs):
+        xh = np.zeros_like(b)
+        _, rep = s2.step_host(b, xh, guess=N.GUESS_LINEAR, precision=1)
+        assert rep.status == 0 and rep.rel_residual <= 1e-12
+        assert np.array_equal(xh, etas[n].cpu().numpy()), n
+    # a history loaded from the host
+    e1, e2 = etas[-1].cpu().numpy(), etas[-2].cpu().numpy()
+    s2.step_history(e1, e2)
+    xh = np.zeros_like(rhs[0])
+    s2.step_host(rhs[0], xh, guess=N.GUESS_LINEAR, precision=1)
+    x = torch.zeros_like(etas[0])
+    s1.solve_step(torch.from_numpy(rhs[0]).cuda(), etas[-1], etas[-2], x, guess=N.GUESS_LINEAR,
+                  precision=1)
+    assert np.array_equal(xh, x.cpu().numpy())
+
+
+def test_step_submit_overlapped_copies_match_step_host(torch_cuda):
+    """Asynchronous steps (next b prefetched before each submit, x copied out
+    on a copy stream) give the same solutions as synchronous steps."""
+    torch = torch_cuda
+    from musoc_solver_b200 import native as N
+
+    p = P.global_grid(180, 90, seed=8)
+    rhs = [np.ascontiguousarray(b) for _, b in P.eddy_rhs(180, 90, range(7), seed=5)]
+    pin = lambda a: torch.from_numpy(np.array(a)).pin_memory().numpy()
+    bs = [pin(b) for b in rhs]
+    xs = [pin(np.zeros_like(b)) for b in rhs]
+    s1, s2 = _solver(p, 16, 6), _solver(p, 16, 6)
+    ref = []
+    for b in rhs:
+        xh = np.zeros_like(b)
+        s1.step_host(b, xh, guess=N.GUESS_LINEAR, precision=1)
+        ref.append(xh)
+    s2.step_prefetch(bs[0])
+    for n in range(len(bs)):
+        if n + 1 < len(bs):
+            s2.step_prefetch(bs[n + 1])
+        rep = s2.step_submit(bs[n], xs[n], guess=N.GUESS_LINEAR, precision=1)
+        assert rep.status == 0 and rep.rel_residual <= 1e-12
+    s2.step_wait()
+    for n in range(len(bs)):
+        assert np.array_equal(xs[n], ref[n]), n
+    # a step submitted without a prefetch stages its own b
+    s2.step_history(ref[-1], ref[-2])
+    s1.step_history(ref[-1], ref[-2])
+    xa, xb = pin(np.zeros_like(rhs[0])), np.zeros_like(rhs[0])
+    s2.step_submit(bs[0], xa, guess=N.GUESS_LINEAR, precision=1)
+    s2.step_wait()
+    s1.step_host(rhs[0], xb, guess=N.GUESS_LINEAR, precision=1)
+    assert np.array_equal(xa, xb)
