@@ -459,6 +459,7 @@ def run_native(args, world, rank, local, dist):
                               inner_tol=itol)
         barrier()
         reps = []
+        l0 = solver.launches()
         ev0.record(stream)
         for k in timed:
             _, r = solver.solve_step(b_dev[k], hist[k - 1], hist[k - 2], hist[k], guess=mode,
@@ -466,22 +467,24 @@ def run_native(args, world, rank, local, dist):
             reps.append(r)
         ev1.record(stream)
         torch.cuda.synchronize()
-        return max_over_ranks(ev0.elapsed_time(ev1) / 1e3, dist, dev), reps
+        return max_over_ranks(ev0.elapsed_time(ev1) / 1e3, dist, dev), reps, solver.launches() - l0
 
     # ---- value arm: mixed precision + warm start, device-resident inputs
-    solver.profile(True)
-    l_value0 = solver.launches()
     with ClockSampler(local) as clk:
-        t_value, reps = run_arm(guess_mode, eta)
+        t_value, reps, launches_value = run_arm(guess_mode, eta)
+    # per-kernel device times of the same steps, from an untimed replay with
+    # CUDA events around every launch (the events and the direct launches
+    # they need would slow the timed arm)
+    solver.profile(True)
+    run_arm(guess_mode, eta)
     prof = solver.profile_read()
     solver.profile(False)
-    launches_value = solver.launches() - l_value0
     relres = [r.rel_residual for r in reps]
     status = [r.status for r in reps]
 
     # ---- the same sequence from linear extrapolation (no network)
     eta_lin = eta[:T] + [torch.zeros_like(eta[0]) for _ in range(W + K)]
-    t_lin, reps_lin = run_arm(N.GUESS_LINEAR, eta_lin)
+    t_lin, reps_lin, _ = run_arm(N.GUESS_LINEAR, eta_lin)
     del eta_lin
 
     # error of the value arm against an FP64 solve of the same steps
