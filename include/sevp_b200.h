@@ -296,7 +296,8 @@ int sevp_relative_residual(sevp_ctx *ctx, const double *b, const double *x, doub
 long long sevp_kernel_launches(const sevp_ctx *ctx);
 /* Per-kernel-class device timing with CUDA events on the context stream:
  * enable != 0 starts (and zeroes) it.  sevp_profile_read fills ms[4] and
- * count[4] for class 0 = tile pass B (update + precondition + dots),
+ * count[4] for class 0 = tile pass B (the x, r update and the first tile
+ * solve; with dot products unless the Schwarz sweep follows),
  * 1 = stencil passes (apply, pass A, residuals), 2 = tile precondition
  * without update, 3 = Schwarz stages on boundary couplings. */
 int sevp_profile(sevp_ctx *ctx, int enable);

@@ -1,6 +1,8 @@
-// Native SEVP-PCG solver for sm_100a: operator apply, block-Jacobi tile SEVP
-// preconditioner (precompute and apply), and the FP64 / mixed-precision
-// preconditioned conjugate-gradient drivers.
+// Native SEVP-PCG solver for sm_100a: operator apply, tile SEVP
+// preconditioners (block-Jacobi tiles, and the overlapping Schwarz sweep over
+// a second, shifted tiling; precompute and apply), the FP64 /
+// mixed-precision preconditioned conjugate-gradient drivers, and the time
+// stepping calls that keep the solution history on the device.
 //
 // The reference solves the barotropic pressure equation with SEVP marching
 // alone (M/sevp.f90:11-438) or with an unpreconditioned BiCGSTAB / Chebyshev
@@ -13,6 +15,9 @@
 //   pass A (stencil kernel):  p = z + beta p_old ; q = A p ; partial p.q
 //   pass B (tile kernel):     x += alpha p ; r -= alpha q ; z = M^{-1} r ;
 //                             partial r.z and r.r
+// (with the Schwarz preconditioner, pass B is three tile passes: the update
+// with the first tiling's solve, then k_tile_couple on the shifted tiling
+// and again on the first, the last one forming r.z and r.r)
 // Scalars (alpha, beta, convergence) are formed on the device by the last CTA
 // of each pass from the per-CTA partial sums, in a fixed order, so results
 // are deterministic and the host only polls a "done" flag between chunks of
