@@ -1378,6 +1378,9 @@ struct sevp_ctx {
   cudaEvent_t ev_in[2] = {nullptr, nullptr}, ev_out[3] = {nullptr, nullptr, nullptr};
   bool ev_out_set[3] = {false, false, false};
   cudaEvent_t ev_solved = nullptr;
+  // coarse-grid feature averages of the learned warm start (3 planes)
+  float *nn_avg = nullptr;
+  size_t nn_avg_n = 0;
   // learned warm start (bound by the network module)
   sevp_warmstart_fn warm_fn = nullptr;
   void *warm_user = nullptr;
@@ -1673,7 +1676,7 @@ static void free_work(sevp_ctx *ctx) {
                   ctx->z32, ctx->p32[0], ctx->p32[1], ctx->q32, ctx->d32, ctx->bh, ctx->xh,
                   ctx->e1h, ctx->e2h, ctx->st, ctx->partials, ctx->tickets,
                   ctx->step_buf[0], ctx->step_buf[1], ctx->step_buf[2], ctx->bstage[0],
-                  ctx->bstage[1],
+                  ctx->bstage[1], ctx->nn_avg,
                   ctx->s1_64, ctx->s2_64, ctx->s1_32, ctx->s2_32, ctx->hist};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -2364,7 +2367,6 @@ __global__ void k_guess(const double *eta1, const double *eta2, double *g, size_
     double v = 0.0;
     if (mode == 1) v = eta1[k];
     if (mode == 2) v = 2.0 * eta1[k] - eta2[k];
-    if (mode == 3) v = eta1[k] - eta2[k];
     g[k] = v;
   }
 }
@@ -2562,29 +2564,9 @@ extern "C" int sevp_step_wait(sevp_ctx *ctx) {
 // ---------------------------------------------------- learned warm start
 // Features of the network from (eta1, eta2, b): e = 2 eta1 - eta2 (the
 // linear extrapolation), r = b - A e, m = M^{-1} r (one tile-SEVP solve),
-// d = eta1 - eta2.  scales[0..2] = RMS of r, m, d; the packed input is
-// BF16 NHWC with 16 channels: r/s0, m/s1, d/s2, then zeros.
-__global__ void k_rms3(const double *a, const double *b, const double *c, size_t n,
-                       double *partials, unsigned *ticket, float *scales) {
-  double s[3] = {0.0, 0.0, 0.0};
-  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
-       k += (size_t)gridDim.x * blockDim.x) {
-    s[0] += a[k] * a[k];
-    s[1] += b[k] * b[k];
-    s[2] += c[k] * c[k];
-  }
-  struct Fin {
-    float *scales;
-    size_t n;
-    __device__ void operator()(double (&v)[3]) {
-      for (int q = 0; q < 3; ++q) {
-        double r = sqrt(v[q] / (double)n);
-        scales[q] = (float)(r > 0.0 ? r : 1.0);
-      }
-    }
-  } fin{scales, n};
-  reduce_and_finish<3>(s, partials, ticket, fin);
-}
+// d = eta1 - eta2, averaged over coarse x coarse cells.  scales[0..2] = RMS
+// of those averages; the packed input is BF16 NHWC with 16 channels: r/s0,
+// m/s1, d/s2, then zeros.
 
 // The network grid is the solver grid averaged over coarse x coarse cells
 // (coarse = 1, 2, 4 or 8), padded with zeros to wn x hn (multiples of 8).
@@ -2597,11 +2579,16 @@ __device__ __forceinline__ bool net_cell(size_t k, int wn, int cx, int cy, int c
   return ci < cx && cj < cy;
 }
 
-__global__ void k_pack_features(const double *r, const double *m, const double *d,
-                                const float *scales, __nv_bfloat16 *feat, int nx, int ny,
-                                int coarse, int wn, int hn) {
+// Coarse-cell averages of r, m and d into avg (3 planes of wn x hn, zero
+// on the padding), and their RMS over the network grid's cells as the
+// normalisation scales[0..2] (the last CTA finishes the sums).
+__global__ void k_pack_avg(const double *r, const double *m, const double *d, float *avg, int nx,
+                           int ny, int coarse, int wn, int hn, double *partials, unsigned *ticket,
+                           float *scales) {
   const int cx = nx / coarse, cy = ny / coarse;
   const size_t n = (size_t)wn * hn;
+  const double inv = 1.0 / (coarse * coarse);
+  double s[3] = {0.0, 0.0, 0.0};
   for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
        k += (size_t)gridDim.x * blockDim.x) {
     int i, j;
@@ -2615,11 +2602,37 @@ __global__ void k_pack_features(const double *r, const double *m, const double *
           c += d[q];
         }
     }
-    const double inv = 1.0 / (coarse * coarse);
+    a *= inv, bm *= inv, c *= inv;
+    avg[k] = (float)a;
+    avg[n + k] = (float)bm;
+    avg[2 * n + k] = (float)c;
+    s[0] += a * a;
+    s[1] += bm * bm;
+    s[2] += c * c;
+  }
+  struct Fin {
+    float *scales;
+    double cells;
+    __device__ void operator()(double (&v)[3]) {
+      for (int q = 0; q < 3; ++q) {
+        const double rms = sqrt(v[q] / cells);
+        scales[q] = (float)(rms > 0.0 ? rms : 1.0);
+      }
+    }
+  } fin{scales, (double)cx * cy};
+  reduce_and_finish<3>(s, partials, ticket, fin);
+}
+
+// The network input: BF16 NHWC with 16 channels, r/s0, m/s1, d/s2, then zeros.
+__global__ void k_pack_features(const float *avg, const float *scales, __nv_bfloat16 *feat,
+                                size_t n) {
+  const float i0 = 1.f / scales[0], i1 = 1.f / scales[1], i2 = 1.f / scales[2];
+  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += (size_t)gridDim.x * blockDim.x) {
     __nv_bfloat16 v[16];
-    v[0] = __float2bfloat16((float)(a * inv / scales[0]));
-    v[1] = __float2bfloat16((float)(bm * inv / scales[1]));
-    v[2] = __float2bfloat16((float)(c * inv / scales[2]));
+    v[0] = __float2bfloat16(avg[k] * i0);
+    v[1] = __float2bfloat16(avg[n + k] * i1);
+    v[2] = __float2bfloat16(avg[2 * n + k] * i2);
 #pragma unroll
     for (int q = 3; q < 16; ++q) v[q] = __float2bfloat16(0.f);
     uint4 *dst = reinterpret_cast<uint4 *>(feat + k * 16);
@@ -2684,26 +2697,51 @@ static bool net_grid_ok(const sevp_ctx *ctx, int coarse, int wn, int hn) {
   return wn % 8 == 0 && hn % 8 == 0 && wn >= ctx->nx / coarse && hn >= ctx->ny / coarse;
 }
 
+// One stencil pass for the features: e = 2 eta1 - eta2 (the linear
+// extrapolation) formed on the fly, d = eta1 - eta2, r = b - A e.
+struct OpFeatures {
+  using T = double;
+  static constexpr int NV = 1;
+  static constexpr bool kUsesState = false;
+  const double *eta1, *eta2, *b;
+  double *e, *d, *r;
+  __device__ void prepare(SolveState *) {}
+  __device__ double value(size_t idx) const { return 2.0 * eta1[idx] - eta2[idx]; }
+  __device__ void emit(size_t idx, double vc, double av, double (&)[NV]) const {
+    e[idx] = vc;
+    d[idx] = eta1[idx] - eta2[idx];
+    r[idx] = b[idx] - av;
+  }
+  __device__ void operator()(double (&)[NV]) {}
+};
+
 extern "C" int sevp_nn_features(sevp_ctx *ctx, const double *eta1, const double *eta2,
                                 const double *b, double *e, double *m, double *d, void *feat,
                                 float *scales, int coarse, int wn, int hn) {
   if (!ctx || !ctx->have_op || !eta1 || !eta2 || !b || !e || !m || !d || !feat || !scales ||
       !net_grid_ok(ctx, coarse, wn, hn))
     return SEVP_BAD_ARG;
-  int s = form_guess(ctx, eta1, eta2, e, 2);  // e = 2 eta1 - eta2
-  if (s) return s;
-  k_guess<<<grid_for(ctx->n), 256, 0, ctx->stream>>>(eta1, eta2, d, ctx->n, 3);
-  ctx->launches++;
-  s = launch_residual<double>(ctx, e, nullptr, nullptr, b, ctx->r64, 0, 0.0);
+  const size_t nn = (size_t)wn * hn;
+  if (ctx->nn_avg_n < nn) {
+    if (ctx->nn_avg) {
+      SEVP_CUDA_TRY(cudaFree(ctx->nn_avg));
+      ctx->nn_avg = nullptr;
+    }
+    SEVP_CUDA_TRY(cudaMalloc((void **)&ctx->nn_avg, 3 * nn * sizeof(float)));
+    ctx->nn_avg_n = nn;
+  }
+  OpFeatures op{eta1, eta2, b, e, d, ctx->r64};
+  int s = launch_stencil(ctx, op, 6);
   if (s) return s;
   // the feature is the block-Jacobi preconditioner's response (what the
   // network was trained on), whichever preconditioner the solves use
   s = launch_tile<double, false, false>(ctx, ctx->ta, nullptr, nullptr, ctx->r64, nullptr, m, 1);
   if (s) return s;
-  k_rms3<<<grid_for(ctx->n), 256, 0, ctx->stream>>>(ctx->r64, m, d, ctx->n, ctx->partials,
-                                                   ctx->tickets + 5, scales);
-  k_pack_features<<<grid_for((size_t)wn * hn), 256, 0, ctx->stream>>>(
-      ctx->r64, m, d, scales, (__nv_bfloat16 *)feat, ctx->nx, ctx->ny, coarse, wn, hn);
+  k_pack_avg<<<grid_for(nn), 256, 0, ctx->stream>>>(ctx->r64, m, d, ctx->nn_avg, ctx->nx, ctx->ny,
+                                                     coarse, wn, hn, ctx->partials,
+                                                     ctx->tickets + 5, scales);
+  k_pack_features<<<grid_for(nn), 256, 0, ctx->stream>>>(ctx->nn_avg, scales,
+                                                         (__nv_bfloat16 *)feat, nn);
   ctx->launches += 2;
   SEVP_CUDA_TRY(cudaGetLastError());
   return SEVP_OK;

@@ -63,3 +63,44 @@ def torch_cuda_ws():
 
     build.build()
     return torch
+
+
+@pytest.mark.parametrize("coarse", [1, 4])
+def test_features_match_numpy_restatement(torch_cuda_ws, oracle, coarse):
+    """sevp_nn_features against numpy with the oracle's operator and tile
+    preconditioner: e, d exact; m to the marching tolerance; scales (RMS of
+    the coarse-cell averages) and the BF16 network input to BF16 rounding."""
+    torch = torch_cuda_ws
+    from musoc_solver_b200.solver import SevpSolver
+    from musoc_solver_b200.warmstart import LearnedWarmStart
+
+    nx, ny = 96, 48
+    p = P.global_grid(nx, ny, seed=31)
+    s = SevpSolver(p, tile_m=16, tile_h=8, growth_limit=1e6)
+    rng = np.random.default_rng(32)
+    eta1, eta2 = rng.standard_normal((2, ny, nx))
+    b = p.b
+    w = LearnedWarmStart.create(s, seed=0, train=False, coarse=coarse)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    e1, e2, bb = t(eta1), t(eta2), t(b)
+    w.features(e1.data_ptr(), e2.data_ptr(), bb.data_ptr())
+    torch.cuda.synchronize()
+    e = 2.0 * eta1 - eta2
+    d = eta1 - eta2
+    assert np.array_equal(w.e.cpu().numpy(), e)
+    assert np.array_equal(w.d.cpu().numpy(), d)
+    r = b - oracle.apply(p, e)
+    m = oracle.TilePC(p, 16, 8, tile_nb=s.tile_nb).apply(r)
+    assert np.abs(w.m.cpu().numpy() - m).max() <= 1e-8 * np.abs(m).max()
+    avg = lambda a: a.reshape(ny // coarse, coarse, nx // coarse, coarse).mean(axis=(1, 3))
+    av = [avg(a) for a in (r, m, d)]
+    sc = np.array([np.sqrt((a * a).mean()) for a in av])
+    assert np.allclose(w.scales.cpu().numpy()[:3], sc, rtol=1e-5)
+    H, W = w.net.H, w.net.W
+    x = w.net.A["x"].float().cpu().numpy().reshape(H, W, -1)
+    cy, cx = ny // coarse, nx // coarse
+    for q in range(3):
+        ref = av[q] / sc[q]
+        got = x[:cy, :cx, q]
+        assert np.abs(got - ref).max() <= 8e-3 * np.abs(ref).max() + 1e-6
+        assert not x[cy:, :, q].any() and not x[:, cx:, q].any()
