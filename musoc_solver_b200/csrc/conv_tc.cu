@@ -304,12 +304,16 @@ template <int KC>
 __global__ void __launch_bounds__(kTcThreads)
     k_conv3x3_tma(const __grid_constant__ CUtensorMap tm_in, const __grid_constant__ CUtensorMap tm_w,
                   const float *__restrict__ bias, bf16 *__restrict__ out, int out_ld, int out_off,
-                  int cin, int cout, int H, int W, int relu, uint32_t tmem_cols) {
+                  int cin, int cout, int cout_total, int nsplit, int H, int W, int relu,
+                  uint32_t tmem_cols) {
   extern __shared__ __align__(1024) unsigned char sm_raw[];
   __shared__ __align__(8) uint64_t full[kTmStages], empty[kTmStages], done;
   __shared__ uint32_t s_tmem;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int x0 = blockIdx.x * kTcM, y = blockIdx.y, img = blockIdx.z;
+  // a CTA computes cout output channels (slice `slice` of cout_total) of
+  // 128 pixels of one image row
+  const int x0 = blockIdx.x * kTcM, y = blockIdx.y, img = blockIdx.z / nsplit;
+  const int slice = blockIdx.z - img * nsplit, n_base = slice * cout;
   const uint32_t raw = smem_u32(sm_raw);
   const uint32_t sbase = (raw + 1023u) & ~1023u;  // 1024-byte aligned stages
   const uint32_t a_bytes = (uint32_t)kTcM * KC * 2, b_bytes = (uint32_t)cout * KC * 2;
@@ -352,7 +356,7 @@ __global__ void __launch_bounds__(kTcThreads)
       const uint32_t a_s = sbase + st * stage_bytes, bar = smem_u32(&full[st]);
       mbar_expect_tx(bar, tx_bytes);
       tma_load_4d(a_s, &tm_in, c0, x0 + dx, y + dy, img, bar);
-      tma_load_2d(a_s + a_bytes, &tm_w, c0, tap * cout, bar);
+      tma_load_2d(a_s + a_bytes, &tm_w, c0, tap * cout_total + n_base, bar);
       issued = s + 1;
     }
   } else if (warp == 1 && lane == 0) {  // MMA issuer
@@ -385,7 +389,7 @@ __global__ void __launch_bounds__(kTcThreads)
   tc_fence_after();
   const int x = x0 + warp * 32 + lane;
   const uint32_t tl = tmem + ((uint32_t)(warp * 32) << 16);
-  bf16 *dst_row = out + (((long long)img * H + y) * W + x) * out_ld + out_off;
+  bf16 *dst_row = out + (((long long)img * H + y) * W + x) * out_ld + out_off + n_base;
   for (int n0 = 0; n0 < cout; n0 += 16) {
     uint32_t v[16];
     tmem_ld16(tl + (uint32_t)n0, v);
@@ -394,7 +398,7 @@ __global__ void __launch_bounds__(kTcThreads)
 #pragma unroll
       for (int q = 0; q < 16; ++q) {
         float f = __uint_as_float(v[q]);
-        if (bias) f += bias[n0 + q];
+        if (bias) f += bias[n_base + n0 + q];
         if (relu) f = fmaxf(f, 0.f);
         o[q] = __float2bfloat16(f);
       }
@@ -441,6 +445,13 @@ int launch_conv_tma(const void *in, int in_ld, int in_off, int cin, const void *
   const CUtensorMapSwizzle sw = KC == 64 ? CU_TENSOR_MAP_SWIZZLE_128B
                                          : (KC == 32 ? CU_TENSOR_MAP_SWIZZLE_64B
                                                      : CU_TENSOR_MAP_SWIZZLE_32B);
+  // small layers (the deep levels of the network) get more CTAs by
+  // splitting the output channels into slices of at least 64
+  const long long ctas = (long long)((W + kTcM - 1) / kTcM) * H * B;
+  int nsplit = 1;
+  while (ctas * nsplit < 148 && cout / (nsplit * 2) >= 64 && (cout / (nsplit * 2)) % 16 == 0)
+    nsplit *= 2;
+  const int ncta = cout / nsplit;
   CUtensorMap tm_in, tm_w;
   {
     // activations: (channel, x, y, image), KC channels x 128 pixels per box
@@ -455,10 +466,11 @@ int launch_conv_tma(const void *in, int in_ld, int in_off, int cin, const void *
       return SEVP_BAD_ARG;
   }
   {
-    // K-major weights (channel, tap * cout + n), KC channels x cout per box
+    // K-major weights (channel, tap * cout + n), KC channels x one slice of
+    // the output channels per box
     const cuuint64_t dims[2] = {(cuuint64_t)cin, (cuuint64_t)9 * cout};
     const cuuint64_t strides[1] = {(cuuint64_t)cin * 2};
-    const cuuint32_t box[2] = {(cuuint32_t)KC, (cuuint32_t)cout};
+    const cuuint32_t box[2] = {(cuuint32_t)KC, (cuuint32_t)ncta};
     const cuuint32_t es[2] = {1, 1};
     if (enc(&tm_w, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(wk), dims, strides, box, es,
             CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -466,8 +478,8 @@ int launch_conv_tma(const void *in, int in_ld, int in_off, int cin, const void *
       return SEVP_BAD_ARG;
   }
   uint32_t cols = 32;
-  while (cols < (uint32_t)cout) cols <<= 1;
-  const size_t stage = ((size_t)kTcM * KC * 2 + (size_t)cout * KC * 2 + 1023) & ~(size_t)1023;
+  while (cols < (uint32_t)ncta) cols <<= 1;
+  const size_t stage = ((size_t)kTcM * KC * 2 + (size_t)ncta * KC * 2 + 1023) & ~(size_t)1023;
   const size_t smem = (size_t)kTmStages * stage + 1024;
   static size_t set_smem = 0;
   if (smem > set_smem) {
@@ -475,9 +487,9 @@ int launch_conv_tma(const void *in, int in_ld, int in_off, int cin, const void *
                                        (int)smem));
     set_smem = smem;
   }
-  dim3 grid((unsigned)((W + kTcM - 1) / kTcM), (unsigned)H, (unsigned)B);
+  dim3 grid((unsigned)((W + kTcM - 1) / kTcM), (unsigned)H, (unsigned)(B * nsplit));
   k_conv3x3_tma<KC><<<grid, kTcThreads, smem, (cudaStream_t)stream>>>(
-      tm_in, tm_w, bias, (bf16 *)out, out_ld, out_off, cin, cout, H, W, relu, cols);
+      tm_in, tm_w, bias, (bf16 *)out, out_ld, out_off, cin, ncta, cout, nsplit, H, W, relu, cols);
   SEVP_CUDA_TRY(cudaGetLastError());
   return SEVP_OK;
 }
