@@ -638,15 +638,18 @@ __global__ void __launch_bounds__(kTileWarps * 32, SEVP_TILE_MINB)
 
 // The march of march_task_regs for a full-height task with one sub-block
 // (hh == HM, nb == 1, the common case): the same operations in straight-line
-// code, without the sub-block bookkeeping.
-template <typename MT, bool SYM, bool kChain, int HM, class Rhs, class Emit>
+// code, without the sub-block bookkeeping.  RCP: the FP32-vector march
+// keeps the reciprocals of AT from the forward sweep for the backward sweep
+// (the same rows) instead of forming them again; chosen per kernel, since
+// the registers it takes pay off in some and not in others.
+template <typename MT, bool SYM, bool kChain, int HM, bool RCP, class Rhs, class Emit>
 __device__ __forceinline__ void march_task_full(const float (&cc_)[HM], const float (&ce_)[HM],
                                                 const float (&cn_)[HM],
                                                 const float (&cw_)[SYM ? 1 : HM],
                                                 const float (&cs_)[SYM ? 1 : HM], int n, int mw,
                                                 bool active, int lane, int segbase, double *dv,
                                                 const MT *mt, Rhs &&rhs, Emit &&emit) {
-  double zs[HM];
+  double zs[HM], rcp[RCP ? HM : 1];
   double zb = 0.0, zc = 0.0, rho = 0.0;
   float cn_prev = 0.f;
 #pragma unroll
@@ -673,8 +676,12 @@ __device__ __forceinline__ void march_task_full(const float (&cc_)[HM], const fl
     const double res = (kChain && active) ? (part - cw * zw) - ce * ze : 0.0;
     if (k < HM - 1) {
       double zn;
-      if constexpr (kChain)
+      if constexpr (kChain && RCP) {
+        rcp[k] = march_rcp(cn);
+        zn = res * rcp[k];
+      } else if constexpr (kChain) {
         zn = res * march_rcp(cn);
+      }
       else
         zn = active ? ((((rk - cw * zw) - cs * zb) - cc * zc) - ce * ze) / cn : 0.0;
       zb = zc;
@@ -715,7 +722,7 @@ __device__ __forceinline__ void march_task_full(const float (&cc_)[HM], const fl
     if (n >= mw - 1) he = 0.0;
     double hn;
     if constexpr (kChain)
-      hn = active ? ((part - cw * hw) - ce * he) * march_rcp(cn) : 0.0;
+      hn = active ? ((part - cw * hw) - ce * he) * (RCP ? rcp[k] : march_rcp(cn)) : 0.0;
     else
       hn = active ? ((((-(cw * hw)) - cs * hb) - cc * hc) - ce * he) / cn : 0.0;
     zs[k + 1] += hn;
@@ -737,7 +744,7 @@ __device__ __forceinline__ void march_task_full(const float (&cc_)[HM], const fl
 // active lane as soon as its sub-block is final.  hh, nb and the sub-block bounds are the same for all
 // lanes of a warp, so the predicated rows keep the warp converged for the
 // shuffles and mat-vecs.
-template <typename MT, bool SYM, bool kChain, int HM, class Rhs, class Emit>
+template <typename MT, bool SYM, bool kChain, int HM, bool RCP, class Rhs, class Emit>
 __device__ __forceinline__ void march_task_regs(const float (&cc_)[HM], const float (&ce_)[HM],
                                                 const float (&cn_)[HM],
                                                 const float (&cw_)[SYM ? 1 : HM],
@@ -745,8 +752,8 @@ __device__ __forceinline__ void march_task_regs(const float (&cc_)[HM], const fl
                                                 int n, int mw, bool active, int lane, int segbase,
                                                 double *dv, const MT *mt, Rhs &&rhs, Emit &&emit) {
   if (nb == 1 && hh == HM) {
-    march_task_full<MT, SYM, kChain, HM>(cc_, ce_, cn_, cw_, cs_, n, mw, active, lane, segbase,
-                                         dv, mt, rhs, emit);
+    march_task_full<MT, SYM, kChain, HM, RCP>(cc_, ce_, cn_, cw_, cs_, n, mw, active, lane,
+                                              segbase, dv, mt, rhs, emit);
     return;
   }
   const size_t msz = (size_t)mw * mw;
@@ -982,8 +989,8 @@ __global__ void __launch_bounds__(kTileWarps * 32, 2)
       z[idx0 + (size_t)k * nx] = zv;
       if (DOTS) acc_rz += (double)rr[k] * (double)zv;
     };
-    march_task_regs<MT, SYM, kChain, HM>(cc_, ce_, cn_, cw_, cs_, hh, nb, n, mw, active, lane,
-                                         segbase, dv, mt, rhs, emit);
+    march_task_regs<MT, SYM, kChain, HM, UPDATE && !DOTS>(cc_, ce_, cn_, cw_, cs_, hh, nb, n, mw,
+                                                          active, lane, segbase, dv, mt, rhs, emit);
   }
   if (DOTS) {
     double v2[2] = {acc_rz, acc_rr};
@@ -1103,8 +1110,8 @@ __global__ void __launch_bounds__(kTileWarps * 32, 2)
         }
       }
     };
-    march_task_regs<MT, SYM, kChain, HM>(cc_, ce_, cn_, cw_, cs_, hh, nb, n, mw, active, lane,
-                                         segbase, dv, mt, rhs, emit);
+    march_task_regs<MT, SYM, kChain, HM, MODE == 0>(cc_, ce_, cn_, cw_, cs_, hh, nb, n, mw, active,
+                                                    lane, segbase, dv, mt, rhs, emit);
   }
   if constexpr (MODE == 2) {
     double v2[2] = {acc_rz, acc_rr};
