@@ -10,8 +10,9 @@ cuts the iterations by about three.  The mixed solve's inner tolerance sets
 how many FP64 refinements (each a PCG restart) the solve needs.  The best
 choice depends on the grid, so it is measured: every candidate shape gets a
 solver (its influence data precomputed on the GPU) for each preconditioner,
-one untimed solve and `repeats` timed solves of the same right-hand side
-from a zero guess per inner tolerance; the fastest wins.
+one untimed solve and `repeats` timed solves of the same right-hand side,
+from a zero guess or from the linear extrapolation of a given history, per
+inner tolerance; the fastest wins.
 """
 from __future__ import annotations
 
@@ -26,12 +27,25 @@ SCHWARZ_MAX_ROWS = 8
 
 
 def autotune(problem, b, candidates=CANDIDATES, precision=1, tol=1e-12, repeats=2,
-             growth_limit=1e10, device="cuda", schwarz=(False, True), inner_tols=(1e-5,)):
+             growth_limit=1e10, device="cuda", schwarz=(False, True), inner_tols=(1e-5,),
+             history=None):
     """Returns (best, table): best = dict(tile_m, tile_h, schwarz, inner_tol,
     ms, ...) of the fastest candidate, table = one such dict per candidate
     measured.  b is the right-hand side on the device (float64, shape
-    (ny, nx)).  inner_tols only matter for precision 1."""
+    (ny, nx)).  inner_tols only matter for precision 1.  history = (eta1,
+    eta2), the two previous solutions: each solve then starts from their
+    linear extrapolation (the warm start of a time sequence) instead of
+    zero."""
     import torch
+
+    from . import native as N
+
+    def run(s, x, itol):
+        if history is None:
+            x.zero_()
+            return s.solve(b, x=x, precision=precision, tol=tol, inner_tol=itol)[1]
+        return s.solve_step(b, history[0], history[1], x, guess=N.GUESS_LINEAR,
+                            precision=precision, tol=tol, inner_tol=itol)[1]
 
     table = []
     for tm, th in candidates:
@@ -47,11 +61,10 @@ def autotune(problem, b, candidates=CANDIDATES, precision=1, tol=1e-12, repeats=
             setup_s = time.perf_counter() - t0
             x = torch.zeros_like(b)
             for itol in (inner_tols if precision == 1 else inner_tols[:1]):
-                s.solve(b, x=x.zero_(), precision=precision, tol=tol, inner_tol=itol)
+                run(s, x, itol)
                 best_ms, res = None, None
                 for _ in range(repeats):
-                    x.zero_()
-                    _, res = s.solve(b, x=x, precision=precision, tol=tol, inner_tol=itol)
+                    res = run(s, x, itol)
                     best_ms = res.ms if best_ms is None else min(best_ms, res.ms)
                 table.append(dict(tile_m=tm, tile_h=th, schwarz=bool(sw), inner_tol=itol,
                                   ms=best_ms, iterations=res.iterations,
