@@ -44,6 +44,7 @@ extern "C" {
 #define SEVP_BAD_ARG 5     /* invalid size, pointer or option */
 #define SEVP_CUDA_ERROR 6  /* a CUDA runtime call failed (see sevp_last_error) */
 #define SEVP_SINGULAR 7    /* an influence matrix had a zero pivot */
+#define SEVP_NONSYMMETRIC 8 /* conjugate gradients asked of a nonsymmetric operator */
 
 const char *sevp_status_string(int status);
 /* Text of the last CUDA error seen by the library (empty if none). */
@@ -54,6 +55,15 @@ int sevp_last_status(void);
  * compiles it in with FLAG_PERIODIC_WE (M/sevp.f90:780-786).  Default 1. */
 void sevp_set_periodic_we(int periodic);
 int sevp_get_periodic_we(void);
+/* Device copies of the read-only inputs of rep1_, rep_, repbir_ and
+ * repbir_period_ (coefficients, RINV, RINV1, IE) kept between calls
+ * (enable != 0), keyed by host address and size: a model that reads the EVP
+ * file once and calls REP1 every step (M/fs_GLOBAL.f90:1852) then copies
+ * only F, X, H and the DUM workspaces per call.  The caller promises that
+ * those arrays keep their values while caching is on; sevp_dropin_cache(0)
+ * frees the copies and turns caching off (the default).  Not part of the
+ * reference interface. */
+int sevp_dropin_cache(int enable);
 
 /* ------------------------------------------- Fortran-compatible drop-ins */
 
@@ -175,13 +185,19 @@ typedef struct {
   int use_guess;     /* 1: x holds the initial guess on entry; 0: start from zero */
   int check_every;   /* PCG iterations between convergence reads by the host */
   int precond_fp32;  /* precision 1: FP32 copy of the influence matrices in the inner solve */
+  int tol_abs;       /* 1: stop on ||b - A x||_2 <= tol (absolute, the reference's rule,
+                        M/sevp.f90:482); 0: the relative test above */
+  int method;        /* SEVP_METHOD_*: the outer iteration */
 } sevp_solve_opts;
+/* Outer iterations of sevp_solve. */
+#define SEVP_METHOD_PCG 0     /* preconditioned CG, two grid passes per iteration */
 
 typedef struct {
   int status;          /* SEVP_* */
   int iterations;      /* total PCG iterations */
   int refinements;     /* FP64 residual evaluations (precision 1) */
   double rel_residual; /* final ||b - A x|| / ||b||, FP64 */
+  double abs_residual; /* final ||b - A x||, FP64 */
   double bnorm;        /* ||b||_2 */
   double ms;           /* device time of the solve */
 } sevp_report;
@@ -197,8 +213,21 @@ int sevp_destroy(sevp_ctx *ctx);
 int sevp_set_operator(sevp_ctx *ctx, const float *al, const float *ab, const float *ac,
                       const float *ar, const float *at, const sevp_tiling *tiling);
 /* 1 when the bound operator is exactly symmetric (AR(i,j) = AL(i+1,j),
- * AT(i,j) = AB(i,j+1)); the kernels then read only AC, AR and AT. */
+ * AT(i,j) = AB(i,j+1)); the kernels then read only AC, AR and AT.  A
+ * nonsymmetric operator can be applied and preconditioned, but sevp_solve
+ * refuses it with SEVP_NONSYMMETRIC (CG needs a symmetric operator). */
 int sevp_operator_symmetric(const sevp_ctx *ctx);
+/* Operator of the FP64 residual passes, when it is not the operator bound
+ * by sevp_set_operator (not part of the reference interface).  PREP's
+ * coefficients (P/prep_GLOBAL.f90:170-244) are symmetric only after each row
+ * J is scaled by 1 / (OCS(J+1) ODY(J+1)); p_sevp_pcg_ binds the scaled,
+ * symmetrised planes with sevp_set_operator and the caller's own planes
+ * here, with the row weights w (ny doubles, device; NULL: all 1).  Every
+ * residual pass then forms ru = b - A x with these planes, scales it by w_j
+ * for the PCG recursion, and tests ||ru|| (unscaled) against the tolerance,
+ * so the solve converges to the caller's operator.  al == NULL unbinds. */
+int sevp_set_residual_operator(sevp_ctx *ctx, const float *al, const float *ab, const float *ac,
+                               const float *ar, const float *at, const double *row_weight);
 /* force != 0: always read all five planes (call before sevp_set_operator). */
 /* CUDA graphs for the FP32 inner PCG iterations of mixed solves (default on):
  * one check interval (check_every iterations of the two passes) is captured
@@ -303,6 +332,58 @@ long long sevp_kernel_launches(const sevp_ctx *ctx);
 int sevp_profile(sevp_ctx *ctx, int enable);
 int sevp_profile_read(sevp_ctx *ctx, double *ms, long long *count);
 
+/* ------------------------- fast solver behind the reference's solver call */
+
+/* Options of p_sevp_pcg_ (process-wide; sevp_fs_default_options fills the
+ * defaults, which apply until sevp_fs_set_options is called). */
+typedef struct {
+  int precision;       /* 0: FP64 PCG; 1 (default): FP32 PCG inside FP64 refinement */
+  int tol_abs;         /* 0 (default): ||S - A X|| / ||S|| <= tol;
+                          1: ||S - A X|| <= tol, the reference's rule (M/sevp.f90:482) */
+  double tol;          /* default 1e-12 (the reference's absolute rule uses 1e-8) */
+  int max_iter;        /* default 5000 */
+  double inner_tol;    /* precision 1: reduction asked of each FP32 solve, default 1e-5 */
+  int tile_m, tile_h;  /* tile shape of the SEVP preconditioner, default 16 x 6 */
+  double growth_limit; /* marching growth bound per sub-block, default 1e10 */
+  int schwarz;         /* 1: overlapping Schwarz preconditioner (tiles <= 8 rows) */
+  int verify;          /* 1 (default): hash the coefficient planes on every call and
+                          rebuild the cached operator when they changed; 0: trust that
+                          the arrays at the same addresses still hold the same values */
+  int method;          /* SEVP_METHOD_* */
+} sevp_fs_options;
+void sevp_fs_default_options(sevp_fs_options *o);
+int sevp_fs_set_options(const sevp_fs_options *o);
+
+/* Same argument list as subroutine p_bicgstab_le, M/sevp.f90:443-552
+ * (called at M/fs_GLOBAL.f90:1853, 1968, 2024), so a Fortran caller swaps
+ * the call's name: al..at and cl..ct REAL*4 (i2, j2) PREP planes (not
+ * symmetric: row J carries OCS(J+1) ODY(J+1), P/prep_GLOBAL.f90:186-189),
+ * b REAL*4 (i2, j2), x REAL*8 (i2+2, j2+2) in/out with its ghost ring as
+ * boundary data.  Solves A x = b with the tile-SEVP preconditioned CG on
+ * the GPU: row weights that make the operator symmetric are found from the
+ * planes, the preconditioner and inner iterations use the symmetrised cl..ct,
+ * and the FP64 residual uses al..at unchanged.  Periodic in x per
+ * sevp_set_periodic_we (as the reference's FLAG_PERIODIC_WE).  The device
+ * operator is cached between calls (see sevp_fs_options.verify).  Status in
+ * sevp_last_status(): SEVP_NONSYMMETRIC when no row scaling symmetrises the
+ * operator (x untouched), SEVP_MAXITER with the last iterate in x. */
+void p_sevp_pcg_(const float *al, const float *ab, const float *ac, const float *ar,
+                 const float *at, const float *b, double *x, const float *cl, const float *cb,
+                 const float *cc, const float *cr, const float *ct, const int *i2, const int *j2);
+/* The row scaling p_sevp_pcg_ applies, on host arrays (no GPU needed): the
+ * weights w[j2] with w_{J+1} / w_J = AT(I,J) / AB(I,J+1) (the same for every
+ * I up to 1e-5), normalised so that max |w_J AC(I,J)| = 1, and the five
+ * planes of W A made exactly symmetric (each coupling the mean of its two
+ * scaled copies) into sym[5 i2 j2] (AL, AB, AC, AR, AT).  Couplings to points
+ * outside the grid are zero in sym.  SEVP_NONSYMMETRIC when no row scaling
+ * symmetrises the planes (message in sevp_last_error). */
+int sevp_row_symmetrize(const float *al, const float *ab, const float *ac, const float *ar,
+                        const float *at, int i2, int j2, int periodic, double *w, float *sym);
+/* Report of the last p_sevp_pcg_ call (iterations, residuals, device ms). */
+int sevp_fs_last_report(sevp_report *r);
+/* Frees the cached device operator of p_sevp_pcg_. */
+int sevp_fs_release(void);
+
 /* ------------------------------------------------- allocation-free entry */
 
 /* Interior dot product of two padded (i2+2, j2+2) FP64 fields, the sum that
@@ -316,8 +397,9 @@ int sevp_profile_read(sevp_ctx *ctx, double *ms, long long *count);
  * library holds until exit.  Limit: j2 <= 16384 (larger grids get
  * SEVP_BAD_ARG and a message in sevp_last_error).  The first call on a
  * device looks up the array's device address; make that first call before
- * any stream capture.  Calls share the array, so calls that overlap on the
- * GPU race; calls ordered in one stream do not. */
+ * any stream capture (a first call on a capturing stream returns
+ * SEVP_BAD_ARG with a message saying so).  Calls share the array, so calls
+ * that overlap on the GPU race; calls ordered in one stream do not. */
 int sevp_inprod_noalloc(const double *r, const double *p, int i2, int j2, double *result,
                         void *stream);
 

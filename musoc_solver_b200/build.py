@@ -47,9 +47,17 @@ def build(force: bool = False, verbose: bool = False) -> str:
     flags = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I",
                     os.path.join(ROOT, "include")]
     procs = []
+    # a source is recompiled when it, a shared header or the flags of this
+    # build changed since its object was made
+    headers = glob.glob(os.path.join(HERE, "csrc", "*.cuh")) + glob.glob(
+        os.path.join(ROOT, "include", "*.h")) + [os.path.abspath(__file__)]
+    newest_header = max(os.path.getmtime(h) for h in headers)
     for src in sources():
         obj = os.path.join(objdir, os.path.basename(src).replace(".cu", ".o"))
         objs.append(obj)
+        if (not force and os.path.exists(obj) and os.path.getmtime(obj) > os.path.getmtime(src)
+                and os.path.getmtime(obj) > newest_header):
+            continue
         cmd = [nvcc()] + flags + ["-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd))

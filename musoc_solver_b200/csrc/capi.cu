@@ -7,6 +7,7 @@
 // (sevp_last_status) and leave the outputs unchanged when they fail.
 #include <algorithm>
 #include <cstring>
+#include <memory>
 #include <vector>
 
 #include "common.cuh"
@@ -40,6 +41,53 @@ struct DBuf {
   }
   DBuf(const DBuf &) = delete;
   DBuf &operator=(const DBuf &) = delete;
+};
+
+// Device copies of read-only drop-in inputs (coefficients, RINV, RINV1, IE)
+// kept between calls when the caller opts in (sevp_dropin_cache): keyed by
+// the host address, the byte count and the device.  The caller promises that
+// the arrays at those addresses keep their values until it calls
+// sevp_dropin_cache(0), which frees the copies.
+struct CacheEntry {
+  const void *host;
+  size_t bytes;
+  int device;
+  void *dev;
+};
+std::vector<CacheEntry> g_cache;
+bool g_cache_on = false;
+
+const void *cached_upload(const void *host, size_t bytes, int *err) {
+  int device = 0;
+  if (cudaGetDevice(&device) != cudaSuccess) return *err = 1, nullptr;
+  for (const CacheEntry &e : g_cache)
+    if (e.host == host && e.bytes == bytes && e.device == device) return e.dev;
+  void *d = nullptr;
+  if (cudaMalloc(&d, bytes) != cudaSuccess) return *err = 1, nullptr;
+  if (cudaMemcpy(d, host, bytes, cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaFree(d);
+    return *err = 1, nullptr;
+  }
+  g_cache.push_back(CacheEntry{host, bytes, device, d});
+  return d;
+}
+
+// A read-only input: the cached device copy when caching is on, else a copy
+// owned by this call.
+template <typename T>
+struct RoBuf {
+  std::unique_ptr<DBuf<T>> own;
+  const T *d = nullptr;
+  int err = 0;
+  RoBuf(const T *h, size_t n) {
+    if (g_cache_on && h && n) {
+      d = static_cast<const T *>(cached_upload(h, n * sizeof(T), &err));
+    } else {
+      own.reset(new DBuf<T>(h, n));
+      d = own->d;
+      err = own->err;
+    }
+  }
 };
 
 // elements of a column-major (ld, rows) array accessed for `cols` columns
@@ -94,12 +142,13 @@ void march_dropin(const float *ax, const float *ay, const float *bb, const float
   }
   const int crows = je - 1;  // equation rows 1..IE(NBLK)-1
   const size_t msz = (size_t)m2 * m2;
-  DBuf<float> dax(ax, span(i2, crows, m2)), day(ay, span(i2, crows, m2)), dbb(bb, span(i2, crows, m2)),
-      dcx(cx, span(i2, crows, m2)), dcy(cy, span(i2, crows, m2)), df(f, span(ldf, crows, m2));
-  DBuf<double> dr(rinv, msz * nblk), dr1(rinv1, msz * std::max(nblk - 1, 0));
+  RoBuf<float> dax(ax, span(i2, crows, m2)), day(ay, span(i2, crows, m2)), dbb(bb, span(i2, crows, m2)),
+      dcx(cx, span(i2, crows, m2)), dcy(cy, span(i2, crows, m2));
+  DBuf<float> df(f, span(ldf, crows, m2));
+  RoBuf<double> dr(rinv, msz * nblk), dr1(rinv1, msz * std::max(nblk - 1, 0));
   DBuf<double> d0(dum0, (size_t)m2 * std::max(nblk - 1, 1)), d1(dum1, m2), d2(dum2, m2);
   DBuf<double> dh(h, span(ldh, je, hzero)), dx(x, span(i0, je + 1, m2 + 2));
-  DBuf<int> die(ie, nblk);
+  RoBuf<int> die(ie, nblk);
   if (ANYERR(dax.err, day.err, dbb.err, dcx.err, dcy.err, df.err, dr.err, dr1.err, d0.err, d1.err,
              d2.err, dh.err, dx.err, die.err)) {
     finish(SEVP_CUDA_ERROR);
@@ -156,9 +205,18 @@ void pre_dropin(const float *ax, const float *ay, const float *bb, const float *
 
 }  // namespace
 
+void sevp_internal_set_status(int s) { g_status = s; }
+
 extern "C" {
 
 int sevp_last_status(void) { return g_status; }
+
+int sevp_dropin_cache(int enable) {
+  for (const CacheEntry &e : g_cache) cudaFree(e.dev);
+  g_cache.clear();
+  g_cache_on = enable != 0;
+  return SEVP_OK;
+}
 void sevp_set_periodic_we(int p) { g_periodic_we = p ? 1 : 0; }
 int sevp_get_periodic_we(void) { return g_periodic_we; }
 

@@ -17,6 +17,8 @@
 
 void sevp_internal_set_error(cudaError_t e, const char *what, const char *file, int line);
 void sevp_internal_set_message(const char *msg);
+// Status that sevp_last_status() reports for the Fortran-compatible calls.
+void sevp_internal_set_status(int status);
 
 namespace sevp {
 

@@ -36,7 +36,9 @@ std::mutex g_scratch_mu;
 
 // Warp w of CTA b sums row j = b*8 + w of the interior (lanes stride over i,
 // then a fixed-order shuffle tree) into scratch[j].  The last CTA to arrive
-// adds scratch[0..j2-1] in row order on one thread and writes *result.
+// adds scratch[0..j2-1]: thread t sums rows t, t + 256, ... in order, then a
+// fixed-order shuffle and shared-memory tree combines the 256 sums, so the
+// result does not depend on which CTA arrives last.
 __global__ void __launch_bounds__(32 * kRowsPerBlock)
     k_inprod_rows(const double *r, const double *p, int i2, int j2, double *scratch,
                   double *result) {
@@ -58,11 +60,19 @@ __global__ void __launch_bounds__(32 * kRowsPerBlock)
     last = (atomicAdd(count, 1u) == gridDim.x - 1);
   }
   __syncthreads();
-  if (last && threadIdx.x == 0) {
+  if (last) {
     __threadfence();
     double t = 0.0;
-    for (int k = 0; k < j2; ++k) t += __ldcg(scratch + k);
-    *result = t;
+    for (int k = threadIdx.x; k < j2; k += blockDim.x) t += __ldcg(scratch + k);
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    __shared__ double warp_sums[kRowsPerBlock];
+    if (lane == 0) warp_sums[w] = t;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double s = 0.0;
+      for (int k = 0; k < kRowsPerBlock; ++k) s += warp_sums[k];
+      *result = s;
+    }
   }
 }
 
@@ -82,12 +92,25 @@ extern "C" int sevp_inprod_noalloc(const double *r, const double *p, int i2, int
     sevp_internal_set_error(e, "cudaGetDevice", __FILE__, __LINE__);
     return SEVP_CUDA_ERROR;
   }
-  if (dev < 0 || dev >= kNoAllocMaxDevices) return SEVP_BAD_ARG;
+  if (dev < 0 || dev >= kNoAllocMaxDevices) {
+    sevp_internal_set_message("sevp_inprod_noalloc: device index is 64 or more");
+    return SEVP_BAD_ARG;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
   double *scratch = nullptr;
   {
-    // first call on this device: look up the array's device address
+    // first call on this device: look up the array's device address (a
+    // runtime call that is not allowed while the stream is being captured)
     std::lock_guard<std::mutex> lock(g_scratch_mu);
     if (!g_scratch_ptr[dev]) {
+      cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+      e = cudaStreamIsCapturing(st, &cap);
+      if (e == cudaSuccess && cap != cudaStreamCaptureStatusNone) {
+        sevp_internal_set_message(
+            "sevp_inprod_noalloc: the first call on a device must come before any stream "
+            "capture (it looks up the scratch array's device address)");
+        return SEVP_BAD_ARG;
+      }
       e = cudaGetSymbolAddress((void **)&g_scratch_ptr[dev], g_noalloc_scratch);
       if (e != cudaSuccess) {
         g_scratch_ptr[dev] = nullptr;
@@ -97,7 +120,6 @@ extern "C" int sevp_inprod_noalloc(const double *r, const double *p, int i2, int
     }
     scratch = g_scratch_ptr[dev];
   }
-  cudaStream_t st = (cudaStream_t)stream;
   // the arrival counter must start at zero; the partial sums are overwritten
   e = cudaMemsetAsync(scratch + kNoAllocMaxRows, 0, sizeof(double), st);
   if (e != cudaSuccess) {

@@ -46,6 +46,10 @@ struct SolveState {
   double tol2;    // stop when rr <= tol2 * bb
   double rr64;    // FP64 true residual ||b - A x||^2 (residual kernel)
   double bb64;    // ||b||^2 (residual kernel)
+  // the same with every row scaled by the residual operator's row weight
+  // (equal to rr64, bb64 when the context has no row weights); the PCG
+  // recursion works on the scaled residual
+  double rr64w, bb64w;
   int iter, max_iter, done, status;
   unsigned ticket[4];
   // optional record of the PCG coefficients: alpha_j at hist[2 (j-1)],
@@ -192,7 +196,7 @@ __global__ void __launch_bounds__(kStencilThreads, SEVP_STENCIL_MINB)
           av += T(ccn[u]) * vc;
           av += T(ce[u]) * ve;
           av += T(cn[u]) * va[u];
-          op.emit((size_t)j * nx + i, vc, av, acc);
+          op.emit((size_t)j * nx + i, j, vc, av, acc);
         }
         vb = vc;
         vc = va[u];
@@ -229,7 +233,7 @@ struct OpApply {
   T *y;
   __device__ void prepare(SolveState *) {}
   __device__ T value(size_t idx) const { return x[idx]; }
-  __device__ void emit(size_t idx, T, T av, double (&acc)[NV]) const { y[idx] = av; }
+  __device__ void emit(size_t idx, int, T, T av, double (&acc)[NV]) const { y[idx] = av; }
   __device__ void operator()(double (&)[NV]) {}
 };
 
@@ -252,7 +256,7 @@ struct OpPassA {
     V zv = z[idx];
     return first ? zv : zv + beta * pold[idx];
   }
-  __device__ void emit(size_t idx, V vc, V av, double (&acc)[NV]) const {
+  __device__ void emit(size_t idx, int, V vc, V av, double (&acc)[NV]) const {
     pnew[idx] = vc;
     q[idx] = av;
     acc[0] += (double)vc * (double)av;
@@ -273,12 +277,15 @@ struct OpPassA {
   }
 };
 
-// FP64 residual: x_out = x + d (d optional, FP32 correction); r = b - A x_out
-// written as R (double or float, optional); sums ||r||^2 and ||b||^2.
+// FP64 residual: x_out = x + d (d optional, FP32 correction); ru = b - A x_out
+// with the residual operator; r = w_j ru (w_j the row weight of row j, 1
+// without weights) written as R (double or float, optional).  Sums ||r||^2,
+// ||w b||^2 (the scaled system the PCG recursion works on) and ||ru||^2,
+// ||b||^2 (the stopping test).
 template <typename R>
 struct OpResidual {
   using T = double;
-  static constexpr int NV = 2;
+  static constexpr int NV = 4;
   static constexpr bool kUsesState = false;
   const double *x;
   const float *d;
@@ -287,37 +294,52 @@ struct OpResidual {
   R *r;
   SolveState *st;
   double tol2;
-  double outer2;  // (safety * outer tolerance)^2: the inner solve need not go below it
+  // (safety * outer tolerance)^2: the inner solve need not go below it; a
+  // relative tolerance (of ||b||) unless abs_mode
+  double outer2;
   int set_inner;  // 1: also initialise the inner FP32 solve state
+  const double *roww;  // row weights (ny) or null
+  int abs_mode;        // the outer test is absolute: ||b - A x|| <= tol
   __device__ void prepare(SolveState *) {}
   __device__ double value(size_t idx) const {
     double v = x[idx];
     if (d) v += (double)d[idx];
     return v;
   }
-  __device__ void emit(size_t idx, double vc, double av, double (&acc)[NV]) const {
+  __device__ void emit(size_t idx, int j, double vc, double av, double (&acc)[NV]) const {
     if (xout) xout[idx] = vc;
-    double bv = b[idx];
-    double rv = bv - av;
+    const double bv = b[idx];
+    const double ru = bv - av;
+    double rv = ru, bw = bv;
+    if (roww) {
+      const double w = roww[j];
+      rv = w * ru;
+      bw = w * bv;
+    }
     if (r) r[idx] = (R)rv;
     acc[0] += rv * rv;
-    acc[1] += bv * bv;
+    acc[1] += bw * bw;
+    acc[2] += ru * ru;
+    acc[3] += bv * bv;
   }
   __device__ void operator()(double (&s)[NV]) {
-    st->rr64 = s[0];
-    st->bb64 = s[1];
+    st->rr64w = s[0];
+    st->bb64w = s[1];
+    st->rr64 = s[2];
+    st->bb64 = s[3];
     if (set_inner) {
       // inner solve starts from zero: its reference norm is ||r||^2
       st->bb = s[0];
       st->rr = s[0];
       // reduce ||r|| by inner_tol, or only as far as the outer test needs
-      st->tol2 = s[0] > 0.0 ? fmax(tol2, fmin(outer2 * s[1] / s[0], 0.25)) : tol2;
+      const double target = abs_mode ? outer2 : outer2 * s[3];
+      st->tol2 = s[2] > 0.0 ? fmax(tol2, fmin(target / s[2], 0.25)) : tol2;
       st->iter = 0;
       st->done = 0;
       st->beta = 0.0;
       st->status = SEVP_OK;
     }
-    if (!isfinite(s[0]) || !isfinite(s[1])) st->status = SEVP_NONFINITE;
+    if (!isfinite(s[0]) || !isfinite(s[2]) || !isfinite(s[3])) st->status = SEVP_NONFINITE;
   }
 };
 
@@ -1350,7 +1372,15 @@ struct sevp_ctx {
   // the overlapping Schwarz preconditioner (built when schwarz_req != 0)
   Tiling ta, tb;
   int sym = 0;                  // operator exactly symmetric: 3-plane kernels
+  int asym = 0;                 // the operator is not symmetric: CG solves are refused
   int force_full = 0;           // use the 5-plane kernels regardless
+  // operator of the FP64 residual passes when it is not the PCG operator c
+  // (sevp_set_residual_operator): the caller's planes, with row weights w_j
+  // such that c is (up to FP32 rounding) the symmetric W A
+  Coeffs cres{};
+  int res_sym = 0;
+  bool have_res = false;
+  const double *roww = nullptr;
   bool infl32_active = false;   // current solve uses the FP32 influence copies
   // the tiling request of the last sevp_set_operator (the second tiling is
   // built from it)
@@ -1463,6 +1493,7 @@ extern "C" const char *sevp_status_string(int s) {
     case SEVP_BAD_ARG: return "bad argument";
     case SEVP_CUDA_ERROR: return "CUDA error";
     case SEVP_SINGULAR: return "singular influence matrix";
+    case SEVP_NONSYMMETRIC: return "operator is not symmetric";
     default: return "unknown status";
   }
 }
@@ -1496,20 +1527,25 @@ static dim3 stencil_grid(const sevp_ctx *ctx, int rpw) {
 static size_t tile_warps(const TileGeom &tg) { return (size_t)tg.ty * tg.txg; }
 
 template <class Op>
-static int launch_stencil(sevp_ctx *ctx, const Op &op, int ticket_slot) {
+static int launch_stencil_c(sevp_ctx *ctx, const Op &op, int ticket_slot, const Coeffs &c,
+                            int sym) {
   int rpw = stencil_rpw(ctx);
   dim3 grid = stencil_grid(ctx, rpw);
   GridDims gd{ctx->nx, ctx->ny, ctx->periodic};
   ProfScope ps(ctx, 1);
-  if (ctx->sym)
+  if (sym)
     k_stencil<Op, true><<<grid, kStencilThreads, 0, ctx->stream>>>(
-        gd, ctx->c, op, rpw, ctx->partials, ctx->tickets + ticket_slot, ctx->st);
+        gd, c, op, rpw, ctx->partials, ctx->tickets + ticket_slot, ctx->st);
   else
     k_stencil<Op, false><<<grid, kStencilThreads, 0, ctx->stream>>>(
-        gd, ctx->c, op, rpw, ctx->partials, ctx->tickets + ticket_slot, ctx->st);
+        gd, c, op, rpw, ctx->partials, ctx->tickets + ticket_slot, ctx->st);
   ctx->launches++;
   SEVP_CUDA_TRY(cudaGetLastError());
   return SEVP_OK;
+}
+template <class Op>
+static int launch_stencil(sevp_ctx *ctx, const Op &op, int ticket_slot) {
+  return launch_stencil_c(ctx, op, ticket_slot, ctx->c, ctx->sym);
 }
 
 // Resident CTAs of a kernel on the current device at the given shared
@@ -1976,6 +2012,45 @@ static int build_schwarz(sevp_ctx *ctx) {
   return s;
 }
 
+// Exact symmetry test of five planes on the device (k_check_symmetry).
+static int check_symmetry(sevp_ctx *ctx, const Coeffs &c, int *asym) {
+  int *d_asym = nullptr;
+  SEVP_CUDA_TRY(cudaMalloc((void **)&d_asym, sizeof(int)));
+  SEVP_CUDA_TRY(cudaMemsetAsync(d_asym, 0, sizeof(int), ctx->stream));
+  const size_t n = (size_t)ctx->nx * ctx->ny;
+  k_check_symmetry<<<(unsigned)std::min<size_t>((n + 255) / 256, 148 * 32), 256, 0, ctx->stream>>>(
+      c, ctx->nx, ctx->ny, ctx->periodic, d_asym);
+  ctx->launches++;
+  *asym = 1;
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(asym, d_asym, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  cudaFree(d_asym);
+  if (e != cudaSuccess) {
+    sevp_internal_set_error(e, "symmetry check", __FILE__, __LINE__);
+    return SEVP_CUDA_ERROR;
+  }
+  return SEVP_OK;
+}
+
+extern "C" int sevp_set_residual_operator(sevp_ctx *ctx, const float *al, const float *ab,
+                                          const float *ac, const float *ar, const float *at,
+                                          const double *row_weight) {
+  if (!ctx) return SEVP_BAD_ARG;
+  ctx->have_res = false;
+  ctx->roww = nullptr;
+  if (!al) return SEVP_OK;
+  if (!ab || !ac || !ar || !at) return SEVP_BAD_ARG;
+  ctx->cres = Coeffs{al, ab, ac, ar, at};
+  int asym = 1;
+  int s = check_symmetry(ctx, ctx->cres, &asym);
+  if (s) return s;
+  ctx->res_sym = asym ? 0 : 1;
+  ctx->roww = row_weight;
+  ctx->have_res = true;
+  return SEVP_OK;
+}
+
 extern "C" int sevp_set_operator(sevp_ctx *ctx, const float *al, const float *ab, const float *ac,
                                  const float *ar, const float *at, const sevp_tiling *tl) {
   if (!ctx || !al || !ab || !ac || !ar || !at || !tl) return SEVP_BAD_ARG;
@@ -1985,24 +2060,15 @@ extern "C" int sevp_set_operator(sevp_ctx *ctx, const float *al, const float *ab
   ctx->have_op = false;
   ctx->c = Coeffs{al, ab, ac, ar, at};
   {
-    int *d_asym = nullptr;
-    SEVP_CUDA_TRY(cudaMalloc((void **)&d_asym, sizeof(int)));
-    SEVP_CUDA_TRY(cudaMemsetAsync(d_asym, 0, sizeof(int), ctx->stream));
-    const size_t n = (size_t)ctx->nx * ctx->ny;
-    k_check_symmetry<<<(unsigned)std::min<size_t>((n + 255) / 256, 148 * 32), 256, 0, ctx->stream>>>(
-        ctx->c, ctx->nx, ctx->ny, ctx->periodic, d_asym);
-    ctx->launches++;
     int h_asym = 1;
-    cudaError_t e = cudaGetLastError();
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(&h_asym, d_asym, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-    cudaFree(d_asym);
-    if (e != cudaSuccess) {
-      sevp_internal_set_error(e, "symmetry check", __FILE__, __LINE__);
-      return SEVP_CUDA_ERROR;
-    }
+    int s = check_symmetry(ctx, ctx->c, &h_asym);
+    if (s) return s;
     ctx->sym = (!h_asym && !ctx->force_full) ? 1 : 0;
+    ctx->asym = h_asym ? 1 : 0;
+    if (h_asym)
+      sevp_internal_set_message(
+          "sevp_set_operator: the operator is not symmetric; apply and precondition work, "
+          "sevp_solve returns SEVP_NONSYMMETRIC");
   }
   // keep the request (the second tiling is built from it later too)
   ctx->treq = *tl;
@@ -2098,12 +2164,15 @@ static int read_state(sevp_ctx *ctx) {
   return SEVP_OK;
 }
 
-// Residual pass: xout = x + d; r = b - A xout; ||r||^2, ||b||^2 into state.
+// Residual pass: xout = x + d; r = W (b - A xout) with the residual
+// operator and its row weights; the norms into the state (OpResidual).
 template <typename R>
 static int launch_residual(sevp_ctx *ctx, const double *x, const float *d, double *xout,
                            const double *b, R *r, int set_inner, double tol2,
-                           double outer2 = 0.0) {
-  OpResidual<R> op{x, d, xout, b, r, ctx->st, tol2, outer2, set_inner};
+                           double outer2 = 0.0, int abs_mode = 0) {
+  OpResidual<R> op{x, d, xout, b, r, ctx->st, tol2, outer2, set_inner,
+                   ctx->have_res ? ctx->roww : nullptr, abs_mode};
+  if (ctx->have_res) return launch_stencil_c(ctx, op, 2, ctx->cres, ctx->res_sym);
   return launch_stencil(ctx, op, 2);
 }
 
@@ -2118,13 +2187,24 @@ __global__ void k_state_init(SolveState *st, double tol2, int max_iter, double *
   *st = s;
 }
 
-// Copies the residual-pass norms into the PCG stopping reference.
-__global__ void k_state_from_residual(SolveState *st) {
-  st->bb = st->bb64;
-  st->rr = st->rr64;
+// Starts an FP64 PCG run from the residual pass's norms: the recursive
+// (row-scaled) residual must fall by the factor the outer test still needs,
+// target / ||b - A x||^2 with target = tol^2 ||b||^2 (relative test) or
+// tol^2 (absolute test).
+__global__ void k_state_from_residual(SolveState *st, double tol2, int abs_mode) {
+  const double target = abs_mode ? tol2 : tol2 * st->bb64;
+  st->tol2 = st->rr64 > 0.0 ? target / st->rr64 : tol2;
+  st->bb = st->rr64w;
+  st->rr = st->rr64w;
   st->iter = 0;
   st->done = 0;
   st->beta = 0.0;
+}
+
+// The outer stopping test on the FP64 residual pass's norms.
+static bool outer_converged(const SolveState *h, const sevp_solve_opts *o) {
+  if (o->tol_abs) return sqrt(h->rr64) <= o->tol;
+  return h->bb64 == 0.0 || sqrt(h->rr64 / h->bb64) <= o->tol;
 }
 
 // Runs PCG iterations on vectors of type V until the device state says done.
@@ -2213,7 +2293,7 @@ static int solve_fp64(sevp_ctx *ctx, const double *b, double *x, const sevp_solv
     // r = b - A x
     int s = launch_residual<double>(ctx, x, nullptr, nullptr, b, ctx->r64, 0, tol2);
     if (s) return s;
-    k_state_from_residual<<<1, 1, 0, ctx->stream>>>(ctx->st);
+    k_state_from_residual<<<1, 1, 0, ctx->stream>>>(ctx->st, tol2, o->tol_abs);
     ctx->launches++;
     s = read_state(ctx);
     if (s) return s;
@@ -2221,8 +2301,9 @@ static int solve_fp64(sevp_ctx *ctx, const double *b, double *x, const sevp_solv
     double rel = ctx->h_st->bb64 > 0 ? sqrt(ctx->h_st->rr64 / ctx->h_st->bb64) : 0.0;
     rep->bnorm = sqrt(ctx->h_st->bb64);
     rep->rel_residual = rel;
+    rep->abs_residual = sqrt(ctx->h_st->rr64);
     rep->refinements++;
-    if (rel <= o->tol || ctx->h_st->bb64 == 0.0) {
+    if (outer_converged(ctx->h_st, o)) {
       status = SEVP_OK;
       break;
     }
@@ -2275,7 +2356,7 @@ static int solve_mixed(sevp_ctx *ctx, const double *b, double *x, const sevp_sol
   const double inner2 = o->inner_tol * o->inner_tol;
   // the last inner solve stops at half the outer tolerance instead of
   // overshooting it by up to a factor inner_tol
-  const double outer2 = 0.25 * o->tol * o->tol;
+  const double outer2 = 0.25 * o->tol * o->tol;  // relative or absolute (o->tol_abs)
   int total = 0, status = SEVP_MAXITER;
   double *xa = x, *xb = ctx->x64s;  // ping-pong: the residual kernel reads xa, writes xb
   bool have_d = false;
@@ -2284,9 +2365,10 @@ static int solve_mixed(sevp_ctx *ctx, const double *b, double *x, const sevp_sol
     ctx->launches++;
     int s;
     if (have_d)
-      s = launch_residual<float>(ctx, xa, ctx->d32, xb, b, ctx->r32, 1, inner2, outer2);
+      s = launch_residual<float>(ctx, xa, ctx->d32, xb, b, ctx->r32, 1, inner2, outer2, o->tol_abs);
     else
-      s = launch_residual<float>(ctx, xa, nullptr, nullptr, b, ctx->r32, 1, inner2, outer2);
+      s = launch_residual<float>(ctx, xa, nullptr, nullptr, b, ctx->r32, 1, inner2, outer2,
+                                 o->tol_abs);
     if (s) return s;
     if (have_d) std::swap(xa, xb);
     s = read_state(ctx);
@@ -2298,8 +2380,9 @@ static int solve_mixed(sevp_ctx *ctx, const double *b, double *x, const sevp_sol
     double rel = ctx->h_st->bb64 > 0 ? sqrt(ctx->h_st->rr64 / ctx->h_st->bb64) : 0.0;
     rep->bnorm = sqrt(ctx->h_st->bb64);
     rep->rel_residual = rel;
+    rep->abs_residual = sqrt(ctx->h_st->rr64);
     rep->refinements++;
-    if (rel <= o->tol || ctx->h_st->bb64 == 0.0) {
+    if (outer_converged(ctx->h_st, o)) {
       status = SEVP_OK;
       break;
     }
@@ -2331,6 +2414,14 @@ static int solve_mixed(sevp_ctx *ctx, const double *b, double *x, const sevp_sol
 extern "C" int sevp_solve(sevp_ctx *ctx, const double *b, double *x, const sevp_solve_opts *o,
                           sevp_report *rep) {
   if (!ctx || !ctx->have_op || !b || !x || !o) return SEVP_BAD_ARG;
+  if (ctx->asym) {
+    sevp_internal_set_message(
+        "sevp_solve: the operator is not symmetric (AR(i,j) != AL(i+1,j) or AT(i,j) != "
+        "AB(i,j+1)), so conjugate gradients has no convergence guarantee; scale its rows "
+        "(p_sevp_pcg_ does this for PREP's coefficients) or use p_bicgstab_le_");
+    if (rep) *rep = sevp_report{}, rep->status = SEVP_NONSYMMETRIC;
+    return SEVP_NONSYMMETRIC;
+  }
   if (!(o->tol > 0.0) || o->max_iter < 0 || (o->precision != 0 && o->precision != 1))
     return SEVP_BAD_ARG;
   if (o->precision == 1 && !(o->inner_tol > 0.0 && o->inner_tol < 1.0)) return SEVP_BAD_ARG;
@@ -2714,7 +2805,7 @@ struct OpFeatures {
   double *e, *d, *r;
   __device__ void prepare(SolveState *) {}
   __device__ double value(size_t idx) const { return 2.0 * eta1[idx] - eta2[idx]; }
-  __device__ void emit(size_t idx, double vc, double av, double (&)[NV]) const {
+  __device__ void emit(size_t idx, int, double vc, double av, double (&)[NV]) const {
     e[idx] = vc;
     d[idx] = eta1[idx] - eta2[idx];
     r[idx] = b[idx] - av;

@@ -22,6 +22,9 @@ SEVP_TIMEOUT = 4
 SEVP_BAD_ARG = 5
 SEVP_CUDA_ERROR = 6
 SEVP_SINGULAR = 7
+SEVP_NONSYMMETRIC = 8
+
+METHOD_PCG = 0
 
 GUESS_ZERO, GUESS_PREVIOUS, GUESS_LINEAR, GUESS_LEARNED = 0, 1, 2, 3
 
@@ -45,12 +48,21 @@ class Tiling(C.Structure):
 class SolveOpts(C.Structure):
     _fields_ = [("precision", C.c_int), ("tol", C.c_double), ("max_iter", C.c_int),
                 ("inner_tol", C.c_double), ("use_guess", C.c_int), ("check_every", C.c_int),
-                ("precond_fp32", C.c_int)]
+                ("precond_fp32", C.c_int), ("tol_abs", C.c_int), ("method", C.c_int)]
+
+
+class FsOptions(C.Structure):
+    """sevp_fs_options: the options of p_sevp_pcg_."""
+    _fields_ = [("precision", C.c_int), ("tol_abs", C.c_int), ("tol", C.c_double),
+                ("max_iter", C.c_int), ("inner_tol", C.c_double), ("tile_m", C.c_int),
+                ("tile_h", C.c_int), ("growth_limit", C.c_double), ("schwarz", C.c_int),
+                ("verify", C.c_int), ("method", C.c_int)]
 
 
 class Report(C.Structure):
     _fields_ = [("status", C.c_int), ("iterations", C.c_int), ("refinements", C.c_int),
-                ("rel_residual", C.c_double), ("bnorm", C.c_double), ("ms", C.c_double)]
+                ("rel_residual", C.c_double), ("abs_residual", C.c_double), ("bnorm", C.c_double),
+                ("ms", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -70,9 +82,16 @@ _SIGS = {
     "sevp_last_status": ([], C.c_int),
     "sevp_set_periodic_we": ([C.c_int], None),
     "sevp_get_periodic_we": ([], C.c_int),
+    "sevp_dropin_cache": ([C.c_int], C.c_int),
+    "sevp_fs_default_options": ([P], None),
+    "sevp_fs_set_options": ([P], C.c_int),
+    "sevp_fs_last_report": ([P], C.c_int),
+    "sevp_fs_release": ([], C.c_int),
+    "sevp_row_symmetrize": ([P] * 5 + [C.c_int, C.c_int, C.c_int, P, P], C.c_int),
     "sevp_create": ([C.POINTER(P), C.c_int, C.c_int, C.c_int, P], C.c_int),
     "sevp_destroy": ([P], C.c_int),
     "sevp_set_operator": ([P, P, P, P, P, P, C.POINTER(Tiling)], C.c_int),
+    "sevp_set_residual_operator": ([P, P, P, P, P, P, P], C.c_int),
     "sevp_influence_bytes": ([P], C.c_longlong),
     "sevp_solve": ([P, P, P, C.POINTER(SolveOpts), C.POINTER(Report)], C.c_int),
     "sevp_solve_host": ([P, P, P, C.POINTER(SolveOpts), C.POINTER(Report)], C.c_int),
@@ -129,6 +148,7 @@ _SIGS = {
     "p_inprod_": ([P] * 5, None),
     "solver_boundary_update_": ([P] * 3, None),
     "p_bicgstab_le_": ([P] * 14, None),
+    "p_sevp_pcg_": ([P] * 14, None),
     "p_csi_": ([P] * 16, None),
     "lanczos_": ([P] * 9, None),
     "sevp_bir_sweeps_": ([P] * 17, None),

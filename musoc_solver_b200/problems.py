@@ -392,6 +392,106 @@ def idealised(i2: int = 180, j2: int = 90) -> Problem:
     return Problem(al, ab, ac, ar, at, b, periodic=True, name=f"idealised{i2}x{j2}")
 
 
+def prep_assemble(i2, j2, k1, odx, ody, csv, ocs, odyv, odz, iu, iv, nbir, gamma):
+    """PREP's coefficient assembly (``P/prep_GLOBAL.f90:170-244``, the 3-D
+    branch, without the idealised override of :246-261), in float32 with the
+    reference's order of operations.
+
+    Metric arrays are indexed by the Fortran row J = 1..J0 at position J-1;
+    ``iu``, ``iv`` are integer masks of shape (K0, J0, I0) (C order of the
+    Fortran (I0, J0, K0) arrays).  Returns AL, AB, AC, AR, AT of shape
+    (J2, I2).  Row J of AB and AT carries OCS(J+1) ODY(J+1), so the operator
+    is symmetric only after each row is divided by that factor.
+    """
+    f = np.float32
+    odx, ody, csv, ocs, odyv, odz = (np.asarray(a, f) for a in (odx, ody, csv, ocs, odyv, odz))
+    J = np.arange(1, j2 + 1)  # Fortran rows 1..J2
+    al = np.zeros((j2, i2), f)
+    ar = np.zeros((j2, i2), f)
+    ab = np.zeros((j2, i2), f)
+    at = np.zeros((j2, i2), f)
+    for k in range(1, k1 + 1):
+        tmp = f(1.0) / odz[k - 1]
+        dzx = (odx[J] * odx[J]) * tmp
+        dzyb = (((csv[J - 1] * ocs[J]) * odyv[J - 1]) * ody[J]) * tmp
+        dzyt = (((csv[J] * ocs[J]) * odyv[J]) * ody[J]) * tmp
+        if k == 1:  # top layer all water (:184-196)
+            al[:] = dzx[:, None]
+            ar[:] = dzx[:, None]
+            ab[:] = dzyb[:, None]
+            at[:] = dzyt[:, None]
+            continue
+        uk = iu[k - 1].astype(f)
+        vk = iv[k - 1].astype(f)
+        al += dzx[:, None] * uk[1:j2 + 1, 0:i2]
+        ar += dzx[:, None] * uk[1:j2 + 1, 1:i2 + 1]
+        ab += dzyb[:, None] * vk[0:j2, 1:i2 + 1]
+        at += dzyt[:, None] * vk[1:j2 + 1, 1:i2 + 1]
+    if nbir == 1:
+        al[:, 0] = 0.0
+        ar[:, i2 - 1] = 0.0
+    ab[0, :] = 0.0
+    at[j2 - 1, :] = 0.0
+    if nbir == 1 and j2 >= 2:
+        ab[0, i2 // 2 - 1] = ab[1, i2 // 2 - 1]  # pin down pressure (:228-230)
+    ac = (((-al - ar) - ab) - at) - f(gamma)
+    return al, ab, ac, ar, at
+
+
+def prep_grid(i2: int = 180, j2: int = 90, k1: int = 6, seed: int = 0, periodic: bool = True,
+              dt: float = 900.0, lat_max: float = 78.0) -> Problem:
+    """PREP-layout problem in the reference's CGS units: spherical metrics of
+    a global grid (R = 6.4e8 cm, lat in [-lat_max, lat_max]), k1 layers with
+    seeded land masks below the all-water top layer, FLAG_FS free surface
+    (GAMMA = 1 / (0.5 DT^2 G), G = 980), assembled by ``prep_assemble``
+    (nonsymmetric, as PREP writes it).  NBIR = 2 keeps the rows periodic in x;
+    periodic=False uses NBIR = 1 (closed side walls and the pressure pin).
+    The right-hand side is REAL*4 noise of the size of the coefficients."""
+    rng = np.random.default_rng(seed)
+    i0, j0 = i2 + 2, j2 + 2
+    r0 = 6.4e8
+    dlat = np.deg2rad(2.0 * lat_max / j2)
+    lat_t = np.deg2rad(-lat_max) + (np.arange(j0) - 0.5) * dlat  # T rows, J = 1..J0
+    lat_v = lat_t + 0.5 * dlat                                    # V rows
+    dlon = 2.0 * np.pi / i2
+    cs = np.cos(lat_t)
+    csv = np.cos(lat_v)
+    odx = 1.0 / (r0 * cs * dlon)
+    ody = np.full(j0, 1.0 / (r0 * dlat))
+    ocs = 1.0 / cs
+    odyv = ody.copy()
+    dz = np.sort(rng.uniform(1e3, 5e4, k1))
+    odz = 1.0 / dz
+    # wet layers per column from a smooth random field; masks of the deeper
+    # layers (the top layer is all water in PREP's assembly)
+    kb = np.clip(np.rint(k1 * (0.6 + 0.5 * smooth_field(j0, i0, 6.0, rng))), 1, k1)
+    if periodic:
+        kb[:, 0] = kb[:, i2]
+        kb[:, i2 + 1] = kb[:, 1]
+    iu = np.zeros((k1 + 1, j0, i0), np.int32)
+    iv = np.zeros((k1 + 1, j0, i0), np.int32)
+    for k in range(1, k1 + 1):
+        wet = kb >= k
+        iu[k - 1, :, 1:] = wet[:, 1:] & wet[:, :-1]
+        iu[k - 1, :, 0] = wet[:, 0]
+        iv[k - 1, 1:, :] = wet[1:, :] & wet[:-1, :]
+        iv[k - 1, 0, :] = wet[0, :]
+        if periodic:
+            iu[k - 1, :, 0] = iu[k - 1, :, i2]
+    gamma = 1.0 / (0.5 * dt * dt * 980.0)
+    nbir = 2 if periodic else 1
+    metrics = dict(odx=odx.astype(np.float32), ody=ody.astype(np.float32),
+                   csv=csv.astype(np.float32), ocs=ocs.astype(np.float32),
+                   odyv=odyv.astype(np.float32), odz=odz.astype(np.float32))
+    al, ab, ac, ar, at = prep_assemble(i2, j2, k1, metrics["odx"], metrics["ody"], metrics["csv"],
+                                       metrics["ocs"], metrics["odyv"], metrics["odz"], iu, iv,
+                                       nbir, gamma)
+    scale = float(np.abs(ac).mean())
+    b = (rng.standard_normal((j2, i2)) * scale).astype(np.float32).astype(np.float64)
+    return Problem(al, ab, ac, ar, at, b, periodic=periodic, name=f"prep{i2}x{j2}",
+                   meta=dict(k1=k1, iu=iu, iv=iv, gamma=np.float32(gamma), nbir=nbir, **metrics))
+
+
 def apply_operator(p: Problem, x: np.ndarray) -> np.ndarray:
     """y = A x in float64 on the unpadded grid (zero outside, periodic in x)."""
     xs = np.zeros_like(x)

@@ -92,6 +92,12 @@ class SolveResult:
     rel_residual: float
     bnorm: float
     ms: float
+    abs_residual: float = 0.0
+
+    @classmethod
+    def of(cls, rep) -> "SolveResult":
+        return cls(rep.status, rep.iterations, rep.refinements, rep.rel_residual, rep.bnorm,
+                   rep.ms, rep.abs_residual)
 
 
 class SevpSolver:
@@ -104,6 +110,7 @@ class SevpSolver:
         import torch
 
         self.precond_fp32 = bool(precond_fp32)
+        self.method = N.METHOD_PCG
 
         self.torch = torch
         self.p = problem
@@ -175,11 +182,14 @@ class SevpSolver:
                 "couple": (ms[3], n[3])}
 
     def opts(self, precision=0, tol=1e-12, max_iter=5000, inner_tol=1e-5, use_guess=False,
-             check_every=4, precond_fp32=None):
+             check_every=4, precond_fp32=None, tol_abs=False, method=None):
         if precond_fp32 is None:
             precond_fp32 = self.precond_fp32
+        if method is None:
+            method = self.method
         return N.SolveOpts(int(precision), float(tol), int(max_iter), float(inner_tol),
-                           int(use_guess), int(check_every), int(precond_fp32))
+                           int(use_guess), int(check_every), int(precond_fp32), int(bool(tol_abs)),
+                           int(method))
 
     def set_schwarz(self, shift: int = -1):
         """Overlapping Schwarz preconditioner: a second tiling rolled west by
@@ -250,8 +260,7 @@ class SevpSolver:
         s = N.lib().sevp_solve(self.h, N.ptr(b), N.ptr(x), C.byref(o), C.byref(rep))
         if s not in (N.SEVP_OK, N.SEVP_MAXITER):
             raise N.SevpError(s, "sevp_solve")
-        return x, SolveResult(rep.status, rep.iterations, rep.refinements, rep.rel_residual,
-                              rep.bnorm, rep.ms)
+        return x, SolveResult.of(rep)
 
     def solve_host(self, b: np.ndarray, x: np.ndarray | None = None, precision=0, tol=1e-12,
                    max_iter=5000, inner_tol=1e-5, check_every=4):
@@ -264,8 +273,7 @@ class SevpSolver:
         s = N.lib().sevp_solve_host(self.h, N.ptr(b), N.ptr(out), C.byref(o), C.byref(rep))
         if s not in (N.SEVP_OK, N.SEVP_MAXITER):
             raise N.SevpError(s, "sevp_solve_host")
-        return out, SolveResult(rep.status, rep.iterations, rep.refinements, rep.rel_residual,
-                                rep.bnorm, rep.ms)
+        return out, SolveResult.of(rep)
 
     def solve_step(self, b, eta1, eta2, x, guess=N.GUESS_LINEAR, precision=1, tol=1e-12,
                    max_iter=5000, inner_tol=1e-5, check_every=4):
@@ -278,8 +286,7 @@ class SevpSolver:
                                     C.byref(o), C.byref(rep))
         if s not in (N.SEVP_OK, N.SEVP_MAXITER):
             raise N.SevpError(s, "sevp_solve_step")
-        return x, SolveResult(rep.status, rep.iterations, rep.refinements, rep.rel_residual,
-                              rep.bnorm, rep.ms)
+        return x, SolveResult.of(rep)
 
     def solve_step_host(self, b, eta1, eta2, x, guess=N.GUESS_LINEAR, precision=1, tol=1e-12,
                         max_iter=5000, inner_tol=1e-5, check_every=4):
@@ -291,8 +298,7 @@ class SevpSolver:
                                          int(guess), C.byref(o), C.byref(rep))
         if s not in (N.SEVP_OK, N.SEVP_MAXITER):
             raise N.SevpError(s, "sevp_solve_step_host")
-        return x, SolveResult(rep.status, rep.iterations, rep.refinements, rep.rel_residual,
-                              rep.bnorm, rep.ms)
+        return x, SolveResult.of(rep)
 
     def step_history(self, eta1=None, eta2=None):
         """Loads the device-held history of step_host from host arrays (eta1
@@ -312,8 +318,7 @@ class SevpSolver:
                                    C.byref(rep))
         if s not in (N.SEVP_OK, N.SEVP_MAXITER):
             raise N.SevpError(s, "sevp_step_host")
-        return x, SolveResult(rep.status, rep.iterations, rep.refinements, rep.rel_residual,
-                              rep.bnorm, rep.ms)
+        return x, SolveResult.of(rep)
 
     def step_prefetch(self, b):
         """Starts copying a later step's b (pinned host array) to the device."""
@@ -329,8 +334,7 @@ class SevpSolver:
                                      C.byref(rep))
         if s not in (N.SEVP_OK, N.SEVP_MAXITER):
             raise N.SevpError(s, "sevp_step_submit")
-        return SolveResult(rep.status, rep.iterations, rep.refinements, rep.rel_residual,
-                           rep.bnorm, rep.ms)
+        return SolveResult.of(rep)
 
     def step_wait(self):
         N.check(N.lib().sevp_step_wait(self.h), "sevp_step_wait")
