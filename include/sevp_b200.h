@@ -191,6 +191,16 @@ typedef struct {
 } sevp_solve_opts;
 /* Outer iterations of sevp_solve. */
 #define SEVP_METHOD_PCG 0     /* preconditioned CG, two grid passes per iteration */
+/* Fused one-launch iterations (precision 1, block-Jacobi tiles of at most 8
+ * rows): each iteration is ONE kernel launch that applies the operator to
+ * the previous launch's direction inside the tile kernel (halo values read
+ * from global memory) and then runs the tile SEVP solve. */
+#define SEVP_METHOD_CG 1      /* CG with the recursion z_{k+1} = z_k - alpha M^-1 A p_k;
+                                 the three dot products of an iteration in one pass */
+#define SEVP_METHOD_CHEB 2    /* Chebyshev iteration on [lmin, lmax] of M^-1 A (no dot
+                                 product feeds the next launch); needs
+                                 sevp_set_chebyshev_bounds.  The reference's P-CSI
+                                 (M/sevp.f90:553-616) is the unpreconditioned form */
 
 typedef struct {
   int status;          /* SEVP_* */
@@ -266,6 +276,15 @@ int sevp_read_coefficients(sevp_ctx *ctx, double *alpha, double *beta, int cap, 
 int sevp_schwarz_shift(const sevp_ctx *ctx);
 /* Device bytes held by the second tiling's influence data. */
 long long sevp_schwarz_influence_bytes(const sevp_ctx *ctx);
+/* Spectrum bounds of the preconditioned operator M^-1 A used by
+ * SEVP_METHOD_CHEB (0 < lmin < lmax).  sevp_estimate_bounds runs one FP64
+ * PCG solve of b (to 1e-10, not changing any caller buffer) and returns the
+ * extreme Ritz values of its CG-Lanczos tridiagonal (the reference gets its
+ * bounds from a 10-step Lanczos run and RATQR, M/sevp.f90:618-694); they
+ * lie inside the spectrum, so widen them a little before setting them. */
+int sevp_set_chebyshev_bounds(sevp_ctx *ctx, double lmin, double lmax);
+int sevp_estimate_bounds(sevp_ctx *ctx, const double *b, double *lmin, double *lmax,
+                         int *iterations);
 /* Solves A x = b (device pointers, (nx, ny) column-major FP64). */
 int sevp_solve(sevp_ctx *ctx, const double *b, double *x, const sevp_solve_opts *opts,
                sevp_report *report);

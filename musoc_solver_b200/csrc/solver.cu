@@ -31,77 +31,9 @@
 
 #include <cuda_bf16.h>
 
-#include "common.cuh"
-#include "tile_sevp.cuh"
+#include "solver_core.cuh"
 
 namespace sevp {
-
-// ------------------------------------------------------------------ state
-struct SolveState {
-  double rz;      // current r.z
-  double pq;      // current p.(A p)
-  double rr;      // current ||r||^2 (recursive residual)
-  double bb;      // reference norm^2 for the stopping test
-  double alpha, beta;
-  double tol2;    // stop when rr <= tol2 * bb
-  double rr64;    // FP64 true residual ||b - A x||^2 (residual kernel)
-  double bb64;    // ||b||^2 (residual kernel)
-  // the same with every row scaled by the residual operator's row weight
-  // (equal to rr64, bb64 when the context has no row weights); the PCG
-  // recursion works on the scaled residual
-  double rr64w, bb64w;
-  int iter, max_iter, done, status;
-  unsigned ticket[4];
-  // optional record of the PCG coefficients: alpha_j at hist[2 (j-1)],
-  // beta_j at hist[2 (j-1) + 1] for iterations j = 1..hist_cap
-  double *hist;
-  int hist_cap;
-};
-
-struct Coeffs {
-  const float *al, *ab, *ac, *ar, *at;
-};
-
-struct GridDims {
-  int nx, ny, periodic;
-};
-
-// ------------------------------------------------- reductions / finisher
-// Writes this CTA's NV partial sums, and lets the last CTA to arrive sum all
-// partials in block order and call fin(sums) once.
-template <int NV, class Fin>
-__device__ __forceinline__ void reduce_and_finish(double (&v)[NV], double *partials,
-                                                  unsigned *ticket, Fin &fin) {
-  __shared__ double red[NV * 32];
-  __shared__ int s_last;
-  const int nblk = gridDim.x * gridDim.y;
-  const int bid = blockIdx.y * gridDim.x + blockIdx.x;
-  block_sum<NV>(v, red);
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int k = 0; k < NV; ++k) partials[(size_t)bid * NV + k] = v[k];
-    __threadfence();
-    unsigned t = atomicAdd(ticket, 1u);
-    s_last = (t == (unsigned)nblk - 1u);
-  }
-  __syncthreads();
-  if (s_last) {
-    __threadfence();
-    double acc[NV];
-#pragma unroll
-    for (int k = 0; k < NV; ++k) acc[k] = 0.0;
-    for (int b = threadIdx.x; b < nblk; b += blockDim.x)
-#pragma unroll
-      for (int k = 0; k < NV; ++k) acc[k] += __ldcg(&partials[(size_t)b * NV + k]);
-    __syncthreads();
-    block_sum<NV>(acc, red);
-    if (threadIdx.x == 0) {
-      fin(acc);
-      *ticket = 0u;
-      __threadfence();
-    }
-  }
-}
 
 // ------------------------------------------------------ stencil kernels
 // Column-walking 5-point stencil.  A CTA of 256 threads covers 32 columns;
@@ -300,10 +232,18 @@ struct OpResidual {
   int set_inner;  // 1: also initialise the inner FP32 solve state
   const double *roww;  // row weights (ny) or null
   int abs_mode;        // the outer test is absolute: ||b - A x|| <= tol
+  // the fused CG leaves its last step out of d: d + dalpha dsel (dsel
+  // null otherwise)
+  const float *dsel;
+  double dalpha;
   __device__ void prepare(SolveState *) {}
   __device__ double value(size_t idx) const {
     double v = x[idx];
-    if (d) v += (double)d[idx];
+    if (d) {
+      double dv = (double)d[idx];
+      if (dsel) dv += dalpha * (double)dsel[idx];
+      v += dv;
+    }
     return v;
   }
   __device__ void emit(size_t idx, int j, double vc, double av, double (&acc)[NV]) const {
@@ -344,50 +284,6 @@ struct OpResidual {
 };
 
 // --------------------------------------------------- tile apply kernel
-constexpr int kTileWarps = 8;
-// FP32-vector tiles up to this height use k_tile_short (measured faster
-// there; the FP64 kernel and taller tiles keep k_tile_apply)
-constexpr int kShortTileRows = 6;
-
-
-// Shared memory per warp: the tile's rows of z (FP64 marching state, 32
-// lanes per row), the last-equation residual of each sub-block (stored at
-// the sub-block's last row), and the mat-vec broadcast vector.
-__host__ __device__ inline size_t tile_smem_per_warp(int hmax) {
-  return (size_t)hmax * 32 * 8 * 2 + 32 * 8;
-}
-
-// out(n) = sum_k dv[seg + k] * M[k * mw + n].  All loads of the column are
-// issued before the first multiply-add, so a mat-vec costs one memory round
-// trip instead of one per group of rows.  MT is the stored matrix type.
-template <int WMAX, typename MT>
-__device__ __forceinline__ double seg_matvec_w(const double *dv, int segbase, const MT *M, int mw,
-                                               int n) {
-  MT m[WMAX];
-#pragma unroll
-  for (int k = 0; k < WMAX; ++k) m[k] = (k < mw) ? __ldg(M + (size_t)k * mw + n) : MT(0);
-  if (sizeof(MT) == 4) {
-    // FP32 influence data: multiply-add in FP32 (the mixed-precision mode)
-    float s = 0.f;
-#pragma unroll
-    for (int k = 0; k < WMAX; ++k)
-      if (k < mw) s += (float)dv[segbase + k] * (float)m[k];
-    return (double)s;
-  }
-  double s = 0.0;
-#pragma unroll
-  for (int k = 0; k < WMAX; ++k)
-    if (k < mw) s += dv[segbase + k] * (double)m[k];
-  return s;
-}
-template <typename MT>
-__device__ __forceinline__ double seg_matvec(const double *dv, int segbase, const MT *M, int mw,
-                                             int n) {
-  if (mw <= 8) return seg_matvec_w<8, MT>(dv, segbase, M, mw, n);
-  if (mw <= 16) return seg_matvec_w<16, MT>(dv, segbase, M, mw, n);
-  return seg_matvec_w<32, MT>(dv, segbase, M, mw, n);
-}
-
 // Inputs of one tile row for one lane (prefetched one row ahead).
 template <typename V>
 struct RowIn {
@@ -412,55 +308,6 @@ __device__ __forceinline__ void load_row(RowIn<V> &in, const Coeffs &c, const V 
   in.ce = __ldg(c.ar + idx);
   in.cn = __ldg(c.at + idx);
 }
-
-// 1/a for the marching rows: the hardware's approximate FP64 reciprocal
-// refined by two Newton-Raphson steps r <- r + r (1 - a r), each of which
-// squares the relative error (a few ulp at most from the rounded quotient).
-// It is formed off the row recurrence's dependency chain.
-__device__ __forceinline__ double march_rcp(double a) {
-  double r;
-  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(a));
-  double e = fma(-a, r, 1.0);
-  r = fma(r, e, r);
-  e = fma(-a, r, 1.0);
-  return fma(r, e, r);
-}
-
-// Finishes a PCG iteration after pass B: r.z and r.r are complete.
-struct TileFin {
-  SolveState *st;
-  __device__ void operator()(double (&s)[2]) {
-    double rz = s[0], rr = s[1];
-    int first = (st->beta == 0.0 && st->iter == 0);
-    st->rr = rr;
-    if (!isfinite(rz) || !isfinite(rr)) {
-      st->status = SEVP_NONFINITE;
-      st->done = 1;
-      return;
-    }
-    if (rr <= st->tol2 * st->bb) {
-      st->done = 1;
-      st->status = SEVP_OK;
-      st->rz = rz;
-      return;
-    }
-    if (st->iter >= st->max_iter) {
-      st->done = 1;
-      st->status = SEVP_MAXITER;
-      st->rz = rz;
-      return;
-    }
-    if (rz == 0.0) {
-      st->status = SEVP_BREAKDOWN;
-      st->done = 1;
-      return;
-    }
-    st->beta = first ? 0.0 : rz / st->rz;
-    if (st->hist && st->iter >= 1 && st->iter <= st->hist_cap)
-      st->hist[2 * (st->iter - 1) + 1] = st->beta;
-    st->rz = rz;
-  }
-};
 
 // UPDATE: fused x += alpha p, r -= alpha q before preconditioning (pass B).
 // DOTS:   accumulate r.z and r.r and finish the iteration on the device.
@@ -655,292 +502,6 @@ __global__ void __launch_bounds__(kTileWarps * 32, SEVP_TILE_MINB)
     double v2[2] = {acc_rz, acc_rr};
     TileFin fin{st};
     reduce_and_finish<2>(v2, partials, ticket, fin);
-  }
-}
-
-// The march of march_task_regs for a full-height task with one sub-block
-// (hh == HM, nb == 1, the common case): the same operations in straight-line
-// code, without the sub-block bookkeeping.  RCP: the FP32-vector march
-// keeps the reciprocals of AT from the forward sweep for the backward sweep
-// (the same rows) instead of forming them again; chosen per kernel, since
-// the registers it takes pay off in some and not in others.
-template <typename MT, bool SYM, bool kChain, int HM, bool RCP, class Rhs, class Emit>
-__device__ __forceinline__ void march_task_full(const float (&cc_)[HM], const float (&ce_)[HM],
-                                                const float (&cn_)[HM],
-                                                const float (&cw_)[SYM ? 1 : HM],
-                                                const float (&cs_)[SYM ? 1 : HM], int n, int mw,
-                                                bool active, int lane, int segbase, double *dv,
-                                                const MT *mt, Rhs &&rhs, Emit &&emit) {
-  double zs[HM], rcp[RCP ? HM : 1];
-  double zb = 0.0, zc = 0.0, rho = 0.0;
-  float cn_prev = 0.f;
-#pragma unroll
-  for (int k = 0; k < HM; ++k) {
-    double cw, cs;
-    if (SYM) {
-      const float arw = __shfl_up_sync(0xffffffffu, ce_[k], 1);
-      cw = (n == 0) ? 0.0 : (double)arw;
-      cs = (double)cn_prev;
-      cn_prev = cn_[k];
-    } else {
-      cw = cw_[k];
-      cs = cs_[k];
-    }
-    const double cc = cc_[k], ce = ce_[k];
-    const double cn = active ? (double)cn_[k] : 1.0;
-    const double rk = rhs(k);
-    const double part = (kChain && active) ? (rk - cs * zb) - cc * zc : 0.0;
-    double zw = __shfl_up_sync(0xffffffffu, zc, 1);
-    double ze = __shfl_down_sync(0xffffffffu, zc, 1);
-    if (n == 0) zw = 0.0;
-    if (n >= mw - 1) ze = 0.0;
-    zs[k] = zc;
-    const double res = (kChain && active) ? (part - cw * zw) - ce * ze : 0.0;
-    if (k < HM - 1) {
-      double zn;
-      if constexpr (kChain && RCP) {
-        rcp[k] = march_rcp(cn);
-        zn = res * rcp[k];
-      } else if constexpr (kChain) {
-        zn = res * march_rcp(cn);
-      }
-      else
-        zn = active ? ((((rk - cw * zw) - cs * zb) - cc * zc) - ce * ze) / cn : 0.0;
-      zb = zc;
-      zc = zn;
-    } else {
-      if constexpr (kChain)
-        rho = res;
-      else
-        rho = active ? (((rk - cw * zw) - cs * zb) - cc * zc) - ce * ze : 0.0;
-    }
-  }
-  dv[lane] = rho;
-  __syncwarp();
-  const double v = active ? seg_matvec<MT>(dv, segbase, mt, mw, n) : 0.0;
-  __syncwarp();
-  zs[0] += v;
-  double hb = 0.0, hc = v;
-  float cn_prev_b = 0.f;
-#pragma unroll
-  for (int k = 0; k < HM - 1; ++k) {
-    const float ncc = active ? cc_[k] : 0.f, nce = active ? ce_[k] : 0.f;
-    const float ncn = active ? cn_[k] : 1.f;
-    double cw, cs;
-    if (SYM) {
-      const float arw = __shfl_up_sync(0xffffffffu, nce, 1);
-      cw = (n == 0) ? 0.0 : (double)arw;
-      cs = (double)cn_prev_b;
-      cn_prev_b = ncn;
-    } else {
-      cw = active ? cw_[k] : 0.f;
-      cs = active ? cs_[k] : 0.f;
-    }
-    const double cc = ncc, ce = nce, cn = ncn;
-    const double part = kChain ? -(cs * hb) - cc * hc : 0.0;
-    double hw = __shfl_up_sync(0xffffffffu, hc, 1);
-    double he = __shfl_down_sync(0xffffffffu, hc, 1);
-    if (n == 0) hw = 0.0;
-    if (n >= mw - 1) he = 0.0;
-    double hn;
-    if constexpr (kChain)
-      hn = active ? ((part - cw * hw) - ce * he) * (RCP ? rcp[k] : march_rcp(cn)) : 0.0;
-    else
-      hn = active ? ((((-(cw * hw)) - cs * hb) - cc * hc) - ce * he) / cn : 0.0;
-    zs[k + 1] += hn;
-    hb = hc;
-    hc = hn;
-  }
-  if (active) {
-#pragma unroll
-    for (int k = 0; k < HM; ++k) emit(k, zs[k]);
-  }
-}
-
-// SEVP march of one task with every row in registers: the forward sweep
-// (particular solution with zero guess rows and block-top corrections) and
-// the backward sweep (guess-row values and homogeneous corrections) of
-// k_tile_apply, operation for operation.  rhs(k) gives row k's right-hand
-// side (0 for inactive lanes; called once per row k < hh, in order, by all
-// lanes of the warp); emit(k, z) receives the solution of row k of an
-// active lane as soon as its sub-block is final.  hh, nb and the sub-block bounds are the same for all
-// lanes of a warp, so the predicated rows keep the warp converged for the
-// shuffles and mat-vecs.
-template <typename MT, bool SYM, bool kChain, int HM, bool RCP, class Rhs, class Emit>
-__device__ __forceinline__ void march_task_regs(const float (&cc_)[HM], const float (&ce_)[HM],
-                                                const float (&cn_)[HM],
-                                                const float (&cw_)[SYM ? 1 : HM],
-                                                const float (&cs_)[SYM ? 1 : HM], int hh, int nb,
-                                                int n, int mw, bool active, int lane, int segbase,
-                                                double *dv, const MT *mt, Rhs &&rhs, Emit &&emit) {
-  if (nb == 1 && hh == HM) {
-    march_task_full<MT, SYM, kChain, HM, RCP>(cc_, ce_, cn_, cw_, cs_, n, mw, active, lane,
-                                              segbase, dv, mt, rhs, emit);
-    return;
-  }
-  const size_t msz = (size_t)mw * mw;
-  // ---- forward sweep
-  double zs[HM], rho[HM];
-  double zb = 0.0, zc = 0.0;
-  float cn_prev = 0.f;
-  int t = 0, kb = 0, ke = sub_start(1, hh, nb) - 1;
-#pragma unroll
-  for (int k = 0; k < HM; ++k) {
-    zs[k] = 0.0;
-    rho[k] = 0.0;
-    if (k < hh) {
-      double cw, cs;
-      if (SYM) {
-        const float arw = __shfl_up_sync(0xffffffffu, ce_[k], 1);
-        cw = (n == 0) ? 0.0 : (double)arw;
-        cs = (double)cn_prev;
-        cn_prev = cn_[k];
-      } else {
-        cw = cw_[k];
-        cs = cs_[k];
-      }
-      const double cc = cc_[k], ce = ce_[k];
-      const double cn = active ? (double)cn_[k] : 1.0;
-      const double rcp_k = kChain ? march_rcp(cn) : 0.0;
-      const double rk = rhs(k);
-      if (k == kb) zc = 0.0;
-      const double part = (kChain && active) ? (rk - cs * zb) - cc * zc : 0.0;
-      double zw = __shfl_up_sync(0xffffffffu, zc, 1);
-      double ze = __shfl_down_sync(0xffffffffu, zc, 1);
-      if (n == 0) zw = 0.0;
-      if (n >= mw - 1) ze = 0.0;
-      zs[k] = zc;
-      const double res = (kChain && active) ? (part - cw * zw) - ce * ze : 0.0;
-      if (k < ke) {
-        double zn;
-        if constexpr (kChain)
-          zn = res * rcp_k;
-        else
-          zn = active ? ((((rk - cw * zw) - cs * zb) - cc * zc) - ce * ze) / cn : 0.0;
-        zb = zc;
-        zc = zn;
-      } else {
-        double rh;
-        if constexpr (kChain)
-          rh = res;
-        else
-          rh = active ? (((rk - cw * zw) - cs * zb) - cc * zc) - ce * ze : 0.0;
-        rho[k] = rh;
-        if (t < nb - 1) {
-          dv[lane] = rh;
-          __syncwarp();
-          double sc = active ? seg_matvec<MT>(dv, segbase, mt + (size_t)(nb + t) * msz, mw, n) : 0.0;
-          __syncwarp();
-          zc = zc - sc;
-        }
-        zb = zc;
-        ++t;
-        kb = k + 1;
-        ke = sub_start(t + 1, hh, nb) - 1;
-      }
-    }
-  }
-  // ---- backward sweep
-  double vnext = 0.0;
-  for (t = nb - 1; t >= 0; --t) {
-    kb = sub_start(t, hh, nb);
-    ke = sub_start(t + 1, hh, nb) - 1;
-    double rho_ke = 0.0;
-    float cn_ke = 0.f, cnb = 0.f;
-#pragma unroll
-    for (int k = 0; k < HM; ++k) {
-      if (k == ke) rho_ke = rho[k], cn_ke = cn_[k];
-      if (k == kb - 1) cnb = cn_[k];
-    }
-    const double cnk = active ? (double)cn_ke : 0.0;
-    dv[lane] = rho_ke - cnk * vnext;
-    __syncwarp();
-    double v = active ? seg_matvec<MT>(dv, segbase, mt + (size_t)t * msz, mw, n) : 0.0;
-    __syncwarp();
-#pragma unroll
-    for (int k = 0; k < HM; ++k)
-      if (k == kb) zs[k] += v;
-    double hb = 0.0, hc = v;
-    if (!active) cnb = 0.f;
-    if (t > 0) {
-      dv[lane] = v * (double)cnb;
-      __syncwarp();
-      hb = active ? seg_matvec<MT>(dv, segbase, mt + (size_t)(nb + t - 1) * msz, mw, n) : 0.0;
-      __syncwarp();
-    }
-    float cn_prev_b = cnb;
-#pragma unroll
-    for (int k = 0; k < HM - 1; ++k) {
-      if (k >= kb && k < ke) {
-        const float ncc = active ? cc_[k] : 0.f, nce = active ? ce_[k] : 0.f;
-        const float ncn = active ? cn_[k] : 1.f;
-        double cw, cs;
-        if (SYM) {
-          const float arw = __shfl_up_sync(0xffffffffu, nce, 1);
-          cw = (n == 0) ? 0.0 : (double)arw;
-          cs = (double)cn_prev_b;
-          cn_prev_b = ncn;
-        } else {
-          cw = active ? cw_[k] : 0.f;
-          cs = active ? cs_[k] : 0.f;
-        }
-        const double cc = ncc, ce = nce, cn = ncn;
-        const double rcp_k = kChain ? march_rcp(cn) : 0.0;
-        const double part = kChain ? -(cs * hb) - cc * hc : 0.0;
-        double hw = __shfl_up_sync(0xffffffffu, hc, 1);
-        double he = __shfl_down_sync(0xffffffffu, hc, 1);
-        if (n == 0) hw = 0.0;
-        if (n >= mw - 1) he = 0.0;
-        double hn;
-        if constexpr (kChain)
-          hn = active ? ((part - cw * hw) - ce * he) * rcp_k : 0.0;
-        else
-          hn = active ? ((((-(cw * hw)) - cs * hb) - cc * hc) - ce * he) / cn : 0.0;
-        zs[k + 1] += hn;
-        hb = hc;
-        hc = hn;
-      }
-    }
-    if (active) {
-#pragma unroll
-      for (int k = 0; k < HM; ++k)
-        if (k >= kb && k <= ke) emit(k, zs[k]);
-    }
-    vnext = v;
-  }
-}
-
-// Asynchronous copy of one 4- or 8-byte element from global to shared
-// memory (zero-filled, with no global read, when pred is false).
-template <int BYTES>
-__device__ __forceinline__ void cp_async_elem(void *smem, const void *gmem, bool pred) {
-  const unsigned dst = (unsigned)__cvta_generic_to_shared(smem);
-  const int n = pred ? BYTES : 0;
-  if constexpr (BYTES == 4)
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(dst), "l"(gmem), "r"(n)
-                 : "memory");
-  else
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dst), "l"(gmem), "r"(n)
-                 : "memory");
-}
-
-// Coefficient rows of one task into registers.
-template <bool SYM, int HM>
-__device__ __forceinline__ void load_task_coeffs(const Coeffs &c, size_t idx0, int nx, int hh,
-                                                 bool active, float (&cc_)[HM], float (&ce_)[HM],
-                                                 float (&cn_)[HM], float (&cw_)[SYM ? 1 : HM],
-                                                 float (&cs_)[SYM ? 1 : HM]) {
-#pragma unroll
-  for (int k = 0; k < HM; ++k) {
-    const bool ok = active && k < hh;
-    const size_t id = ok ? idx0 + (size_t)k * nx : 0;
-    cc_[k] = ok ? __ldg(c.ac + id) : 0.f;
-    ce_[k] = ok ? __ldg(c.ar + id) : 0.f;
-    cn_[k] = ok ? __ldg(c.at + id) : 0.f;
-    if (!SYM) {
-      cw_[k] = ok ? __ldg(c.al + id) : 0.f;
-      cs_[k] = ok ? __ldg(c.ab + id) : 0.f;
-    }
   }
 }
 
@@ -1399,6 +960,10 @@ struct sevp_ctx {
   double *x64s = nullptr;  // ping-pong partner for the refinement update
   float *r32 = nullptr, *z32 = nullptr, *p32[2] = {nullptr, nullptr}, *q32 = nullptr,
         *d32 = nullptr;
+  // the fused CG's second pair of t buffers (allocated on first use)
+  float *t32[2] = {nullptr, nullptr};
+  // spectrum bounds of M^-1 A for the Chebyshev iteration (0: not set)
+  double cheb_lmin = 0.0, cheb_lmax = 0.0;
   double *bh = nullptr;  // device staging for host solves
   double *xh = nullptr;
   double *e1h = nullptr, *e2h = nullptr;
@@ -1439,7 +1004,7 @@ struct sevp_ctx {
   cudaStream_t cap_stream = nullptr;
   cudaGraphExec_t inner_graph = nullptr;
   int inner_graph_ce = 0;
-  const void *inner_graph_key[4] = {nullptr, nullptr, nullptr, nullptr};
+  const void *inner_graph_key[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   // optional per-kernel-class timing (CUDA events on the context stream)
   int prof = 0;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pool;
@@ -1720,7 +1285,8 @@ static void free_work(sevp_ctx *ctx) {
                   ctx->e1h, ctx->e2h, ctx->st, ctx->partials, ctx->tickets,
                   ctx->step_buf[0], ctx->step_buf[1], ctx->step_buf[2], ctx->bstage[0],
                   ctx->bstage[1], ctx->nn_avg,
-                  ctx->s1_64, ctx->s2_64, ctx->s1_32, ctx->s2_32, ctx->hist};
+                  ctx->s1_64, ctx->s2_64, ctx->s1_32, ctx->s2_32, ctx->hist, ctx->t32[0],
+                  ctx->t32[1]};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   ctx->ta.release();
@@ -2169,9 +1735,10 @@ static int read_state(sevp_ctx *ctx) {
 template <typename R>
 static int launch_residual(sevp_ctx *ctx, const double *x, const float *d, double *xout,
                            const double *b, R *r, int set_inner, double tol2,
-                           double outer2 = 0.0, int abs_mode = 0) {
+                           double outer2 = 0.0, int abs_mode = 0, const float *dsel = nullptr,
+                           double dalpha = 0.0) {
   OpResidual<R> op{x, d, xout, b, r, ctx->st, tol2, outer2, set_inner,
-                   ctx->have_res ? ctx->roww : nullptr, abs_mode};
+                   ctx->have_res ? ctx->roww : nullptr, abs_mode, dsel, dalpha};
   if (ctx->have_res) return launch_stencil_c(ctx, op, 2, ctx->cres, ctx->res_sym);
   return launch_stencil(ctx, op, 2);
 }
@@ -2207,33 +1774,19 @@ static bool outer_converged(const SolveState *h, const sevp_solve_opts *o) {
   return h->bb64 == 0.0 || sqrt(h->rr64 / h->bb64) <= o->tol;
 }
 
-// Runs PCG iterations on vectors of type V until the device state says done.
-// x, r hold the iterate and residual; the first z = M^{-1} r must already be
-// in place (with rz, beta = 0 set).  Returns iterations done.
-template <typename V>
-static int pcg_loop(sevp_ctx *ctx, V *x, V *r, V *z, V *p0, V *p1, V *q, int check_every,
-                    int *iters_out) {
-  V *pp[2] = {p0, p1};
-  auto interval = [&](int &cur) -> int {  // check_every iterations of passes A and B
-    for (int k = 0; k < check_every; ++k) {
-      OpPassA<V> op{z, pp[cur], pp[cur ^ 1], q, ctx->st};
-      int s = launch_stencil(ctx, op, 3);
-      if (s) return s;
-      s = precondition_pass<V, true, true>(ctx, x, pp[cur ^ 1], r, q, z);
-      if (s) return s;
-      cur ^= 1;
-    }
-    return SEVP_OK;
-  };
+// Runs check intervals of an inner iteration until the device state says
+// done.  interval(cur) issues one interval's launches with the ping-pong
+// buffer index cur (and flips it per iteration); with graphs on, one
+// interval is captured once per key (buffers, influence precision, method)
+// and replayed, which needs an even interval so that the buffers return to
+// the same roles.  launches: kernel launches per interval.
+template <class Interval>
+static int graph_loop(sevp_ctx *ctx, bool graph, const void *const (&key)[5], int check_every,
+                      int launches, Interval &&interval) {
   int cur = 0;
-  // FP32 inner loop: one graph replay per check interval (an even interval
-  // returns the p buffers to the same roles, so one capture serves all)
-  const bool graph = sizeof(V) == 4 && ctx->use_graphs && !ctx->prof && check_every % 2 == 0;
-  const void *key[4] = {(const void *)x, (const void *)p0,
-                        (const void *)(ctx->infl32_active ? ctx->ta.d_mats32 : nullptr),
-                        (const void *)(schwarz_on(ctx) ? ctx->tb.d_mats : nullptr)};
+  graph = graph && ctx->use_graphs && !ctx->prof && check_every % 2 == 0;
   if (graph && !(ctx->inner_graph && ctx->inner_graph_ce == check_every &&
-                 std::equal(key, key + 4, ctx->inner_graph_key))) {
+                 std::equal(key, key + 5, ctx->inner_graph_key))) {
     drop_inner_graph(ctx);
     if (!ctx->cap_stream)
       SEVP_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking));
@@ -2258,16 +1811,16 @@ static int pcg_loop(sevp_ctx *ctx, V *x, V *r, V *z, V *p0, V *p1, V *q, int che
     if (g) cudaGraphDestroy(g);
     if (e != cudaSuccess) {
       ctx->inner_graph = nullptr;
-      sevp_internal_set_error(e, "capture of the inner PCG loop", __FILE__, __LINE__);
+      sevp_internal_set_error(e, "capture of the inner iteration loop", __FILE__, __LINE__);
       return SEVP_CUDA_ERROR;
     }
     ctx->inner_graph_ce = check_every;
-    std::copy(key, key + 4, ctx->inner_graph_key);
+    std::copy(key, key + 5, ctx->inner_graph_key);
   }
   for (;;) {
     if (graph) {
       SEVP_CUDA_TRY(cudaGraphLaunch(ctx->inner_graph, ctx->stream));
-      ctx->launches += (schwarz_on(ctx) ? 4 : 2) * check_every;
+      ctx->launches += launches;
     } else {
       int s = interval(cur);
       if (s) return s;
@@ -2277,6 +1830,107 @@ static int pcg_loop(sevp_ctx *ctx, V *x, V *r, V *z, V *p0, V *p1, V *q, int che
     prof_collect(ctx);
     if (ctx->h_st->done) break;
   }
+  return SEVP_OK;
+}
+
+// Runs PCG iterations on vectors of type V until the device state says done.
+// x, r hold the iterate and residual; the first z = M^{-1} r must already be
+// in place (with rz, beta = 0 set).  Returns iterations done.
+template <typename V>
+static int pcg_loop(sevp_ctx *ctx, V *x, V *r, V *z, V *p0, V *p1, V *q, int check_every,
+                    int *iters_out) {
+  V *pp[2] = {p0, p1};
+  auto interval = [&](int &cur) -> int {  // check_every iterations of passes A and B
+    for (int k = 0; k < check_every; ++k) {
+      OpPassA<V> op{z, pp[cur], pp[cur ^ 1], q, ctx->st};
+      int s = launch_stencil(ctx, op, 3);
+      if (s) return s;
+      s = precondition_pass<V, true, true>(ctx, x, pp[cur ^ 1], r, q, z);
+      if (s) return s;
+      cur ^= 1;
+    }
+    return SEVP_OK;
+  };
+  // FP32 inner loop: one graph replay per check interval
+  const void *const key[5] = {(const void *)x, (const void *)p0,
+                              (const void *)(ctx->infl32_active ? ctx->ta.d_mats32 : nullptr),
+                              (const void *)(schwarz_on(ctx) ? ctx->tb.d_mats : nullptr),
+                              (const void *)(uintptr_t)SEVP_METHOD_PCG};
+  int s = graph_loop(ctx, sizeof(V) == 4, key, check_every,
+                     (schwarz_on(ctx) ? 4 : 2) * check_every, interval);
+  if (s) return s;
+  *iters_out = ctx->h_st->iter;
+  return SEVP_OK;
+}
+
+// One fused launch (fused.cu) on the block-Jacobi tiling.
+static int launch_fused_k(sevp_ctx *ctx, int mode, const float *zi, const float *ti,
+                          const float *pi, float *zo, float *to, float *po, float *x, float *r) {
+  const Tiling &T = ctx->ta;
+  const bool m32 = ctx->infl32_active && T.d_mats32;
+  FusedLaunch<float> L{mode, ctx->sym, m32 ? 1 : 0, T.tg, T.c, ctx->periodic,
+                       m32 ? (const void *)T.d_mats32 : (const void *)T.d_mats,
+                       zi, ti, pi, zo, to, po, x, r, ctx->st, ctx->partials, ctx->tickets + 7,
+                       ctx->stream};
+  ProfScope ps(ctx, 0);
+  int s = fused_launch<float>(L);
+  ctx->launches++;
+  return s;
+}
+
+// Inner FP32 solve A d = r32 with a fused one-launch iteration, from d = 0
+// (d32 zeroed by the caller).  CG: the first z = M^-1 r is made by a tile
+// pass; the buffers z = {z32, r32} (r is not needed after it), t = t32,
+// p = p32.  Chebyshev: d = {p32[0], p32[1]}, x = d32, r = r32 in place.
+__global__ void k_state_fused_cg(SolveState *st) {
+  st->bb = st->rz;  // stopping reference: (r_0, z_0)
+  st->alpha = 0.0;
+  st->beta = 0.0;
+  st->iter = 0;
+}
+__global__ void k_state_cheb(SolveState *st, double theta, double delta) {
+  st->cheb_theta = theta;
+  st->cheb_delta = delta;
+  st->cheb_sigma = theta / delta;
+  st->cheb_rho = delta / theta;
+}
+
+static int fused_inner(sevp_ctx *ctx, int method, int check_every, int *iters_out) {
+  const int mode = method == SEVP_METHOD_CHEB ? kFusedCheb : kFusedCG;
+  if (mode == kFusedCG) {
+    for (float *&t : ctx->t32)
+      if (!t) SEVP_CUDA_TRY(cudaMalloc((void **)&t, ctx->n * sizeof(float)));
+    int s = launch_tile<float, false, true>(ctx, ctx->ta, nullptr, nullptr, ctx->r32, nullptr,
+                                            ctx->z32, 4);
+    if (s) return s;
+    k_state_fused_cg<<<1, 1, 0, ctx->stream>>>(ctx->st);
+  } else {
+    const double lmin = ctx->cheb_lmin, lmax = ctx->cheb_lmax;
+    k_state_cheb<<<1, 1, 0, ctx->stream>>>(ctx->st, 0.5 * (lmax + lmin), 0.5 * (lmax - lmin));
+  }
+  ctx->launches++;
+  SEVP_CUDA_TRY(cudaGetLastError());
+  float *zb[2] = {ctx->z32, ctx->r32}, *tb[2] = {ctx->t32[0], ctx->t32[1]};
+  float *pb[2] = {ctx->p32[0], ctx->p32[1]};
+  auto interval = [&](int &cur) -> int {
+    for (int k = 0; k < check_every; ++k) {
+      int s;
+      if (mode == kFusedCG)
+        s = launch_fused_k(ctx, mode, zb[cur], tb[cur], pb[cur], zb[cur ^ 1], tb[cur ^ 1],
+                           pb[cur ^ 1], ctx->d32, nullptr);
+      else
+        s = launch_fused_k(ctx, mode, pb[cur], nullptr, nullptr, pb[cur ^ 1], nullptr, nullptr,
+                           ctx->d32, ctx->r32);
+      if (s) return s;
+      cur ^= 1;
+    }
+    return SEVP_OK;
+  };
+  const void *const key[5] = {(const void *)ctx->d32, (const void *)ctx->p32[0],
+                              (const void *)(ctx->infl32_active ? ctx->ta.d_mats32 : nullptr),
+                              nullptr, (const void *)(uintptr_t)method};
+  int s = graph_loop(ctx, true, key, check_every, check_every, interval);
+  if (s) return s;
   *iters_out = ctx->h_st->iter;
   return SEVP_OK;
 }
@@ -2360,12 +2014,16 @@ static int solve_mixed(sevp_ctx *ctx, const double *b, double *x, const sevp_sol
   int total = 0, status = SEVP_MAXITER;
   double *xa = x, *xb = ctx->x64s;  // ping-pong: the residual kernel reads xa, writes xb
   bool have_d = false;
+  const int method = o->method;
+  const float *dsel = nullptr;  // fused CG: the last step alpha_k p_k, left out of d32
+  double dalpha = 0.0;
   for (int refine = 0; refine < 64; ++refine) {
     k_state_init<<<1, 1, 0, ctx->stream>>>(ctx->st, inner2, std::max(o->max_iter - total, 0));
     ctx->launches++;
     int s;
     if (have_d)
-      s = launch_residual<float>(ctx, xa, ctx->d32, xb, b, ctx->r32, 1, inner2, outer2, o->tol_abs);
+      s = launch_residual<float>(ctx, xa, ctx->d32, xb, b, ctx->r32, 1, inner2, outer2, o->tol_abs,
+                                 dsel, dalpha);
     else
       s = launch_residual<float>(ctx, xa, nullptr, nullptr, b, ctx->r32, 1, inner2, outer2,
                                  o->tol_abs);
@@ -2392,11 +2050,22 @@ static int solve_mixed(sevp_ctx *ctx, const double *b, double *x, const sevp_sol
     }
     // inner solve A d = r32 from d = 0
     SEVP_CUDA_TRY(cudaMemsetAsync(ctx->d32, 0, ctx->n * 4, ctx->stream));
-    s = precondition_pass<float, false, true>(ctx, nullptr, nullptr, ctx->r32, nullptr, ctx->z32);
-    if (s) return s;
     int it = 0;
-    s = pcg_loop<float>(ctx, ctx->d32, ctx->r32, ctx->z32, ctx->p32[0], ctx->p32[1], ctx->q32,
-                        std::max(1, o->check_every), &it);
+    if (method == SEVP_METHOD_PCG) {
+      s = precondition_pass<float, false, true>(ctx, nullptr, nullptr, ctx->r32, nullptr, ctx->z32);
+      if (s) return s;
+      s = pcg_loop<float>(ctx, ctx->d32, ctx->r32, ctx->z32, ctx->p32[0], ctx->p32[1], ctx->q32,
+                          std::max(1, o->check_every), &it);
+    } else {
+      s = fused_inner(ctx, method, std::max(1, o->check_every), &it);
+      if (!s && method == SEVP_METHOD_CG && it > 0) {
+        dsel = ctx->p32[it & 1];
+        dalpha = ctx->h_st->alpha;
+      } else {
+        dsel = nullptr;
+        dalpha = 0.0;
+      }
+    }
     if (s) return s;
     total += it;
     have_d = true;
@@ -2424,6 +2093,20 @@ extern "C" int sevp_solve(sevp_ctx *ctx, const double *b, double *x, const sevp_
   }
   if (!(o->tol > 0.0) || o->max_iter < 0 || (o->precision != 0 && o->precision != 1))
     return SEVP_BAD_ARG;
+  if (o->method != SEVP_METHOD_PCG) {
+    const char *why = nullptr;
+    if (o->method != SEVP_METHOD_CG && o->method != SEVP_METHOD_CHEB) why = "unknown method";
+    else if (o->precision != 1) why = "the fused iterations run in the mixed-precision mode (precision 1)";
+    else if (schwarz_on(ctx)) why = "the fused iterations use the block-Jacobi tiles (no Schwarz)";
+    else if (ctx->ta.tg.hmax > kFusedMaxRows) why = "the fused iterations need tiles of at most 8 rows";
+    else if (o->method == SEVP_METHOD_CHEB && !(ctx->cheb_lmax > ctx->cheb_lmin && ctx->cheb_lmin > 0.0))
+      why = "Chebyshev needs spectrum bounds (sevp_set_chebyshev_bounds / sevp_estimate_bounds)";
+    if (why) {
+      std::string m = std::string("sevp_solve: ") + why;
+      sevp_internal_set_message(m.c_str());
+      return SEVP_BAD_ARG;
+    }
+  }
   if (o->precision == 1 && !(o->inner_tol > 0.0 && o->inner_tol < 1.0)) return SEVP_BAD_ARG;
   sevp_report local{};
   sevp_report *r = rep ? rep : &local;
@@ -2882,5 +2565,95 @@ extern "C" int sevp_relative_residual(sevp_ctx *ctx, const double *b, const doub
   s = read_state(ctx);
   if (s) return s;
   *relres = ctx->h_st->bb64 > 0 ? sqrt(ctx->h_st->rr64 / ctx->h_st->bb64) : 0.0;
+  return SEVP_OK;
+}
+
+// Extreme eigenvalues of the symmetric tridiagonal matrix (diagonal d,
+// off-diagonal e) by bisection on Sturm sequence counts.
+static void tridiag_extremes(const std::vector<double> &d, const std::vector<double> &e,
+                             double *lo, double *hi) {
+  const int n = (int)d.size();
+  double gl = d[0], gu = d[0];
+  for (int i = 0; i < n; ++i) {
+    const double r = (i > 0 ? std::fabs(e[i - 1]) : 0.0) + (i + 1 < n ? std::fabs(e[i]) : 0.0);
+    gl = std::min(gl, d[i] - r);
+    gu = std::max(gu, d[i] + r);
+  }
+  // eigenvalues below x
+  auto count = [&](double x) {
+    int c = 0;
+    double q = d[0] - x;
+    if (q < 0) ++c;
+    for (int i = 1; i < n; ++i) {
+      const double qq = q != 0.0 ? q : 1e-300;
+      q = d[i] - x - e[i - 1] * e[i - 1] / qq;
+      if (q < 0) ++c;
+    }
+    return c;
+  };
+  auto kth = [&](int k) {  // k-th smallest (0-based)
+    double a = gl, b = gu;
+    for (int it = 0; it < 200 && b - a > 1e-15 * std::max(std::fabs(a), std::fabs(b)); ++it) {
+      const double m = 0.5 * (a + b);
+      if (count(m) > k) b = m;
+      else a = m;
+    }
+    return 0.5 * (a + b);
+  };
+  *lo = kth(0);
+  *hi = kth(n - 1);
+}
+
+extern "C" int sevp_set_chebyshev_bounds(sevp_ctx *ctx, double lmin, double lmax) {
+  if (!ctx || !(lmin > 0.0) || !(lmax > lmin) || !std::isfinite(lmax)) return SEVP_BAD_ARG;
+  ctx->cheb_lmin = lmin;
+  ctx->cheb_lmax = lmax;
+  drop_inner_graph(ctx);
+  return SEVP_OK;
+}
+
+extern "C" int sevp_estimate_bounds(sevp_ctx *ctx, const double *b, double *lmin, double *lmax,
+                                    int *iterations) {
+  if (!ctx || !ctx->have_op || !b || !lmin || !lmax) return SEVP_BAD_ARG;
+  const int cap = 2000;
+  double *keep_hist = ctx->hist;
+  const int keep_cap = ctx->hist_cap;
+  double *hist = nullptr;
+  SEVP_CUDA_TRY(cudaMalloc((void **)&hist, sizeof(double) * 2 * cap));
+  SEVP_CUDA_TRY(cudaMemsetAsync(hist, 0, sizeof(double) * 2 * cap, ctx->stream));
+  if (!ctx->xh) SEVP_CUDA_TRY(cudaMalloc((void **)&ctx->xh, ctx->n * 8));
+  ctx->hist = hist;
+  ctx->hist_cap = cap;
+  sevp_solve_opts o{};
+  o.precision = 0;
+  o.tol = 1e-10;
+  o.max_iter = cap;
+  o.check_every = 4;
+  o.method = SEVP_METHOD_PCG;
+  sevp_report rep{};
+  int s = sevp_solve(ctx, b, ctx->xh, &o, &rep);
+  ctx->hist = keep_hist;
+  ctx->hist_cap = keep_cap;
+  std::vector<double> h((size_t)2 * cap);
+  cudaError_t e = cudaMemcpy(h.data(), hist, sizeof(double) * 2 * cap, cudaMemcpyDeviceToHost);
+  cudaFree(hist);
+  if (s != SEVP_OK && s != SEVP_MAXITER) return s;
+  if (e != cudaSuccess) {
+    sevp_internal_set_error(e, "copy of the PCG coefficients", __FILE__, __LINE__);
+    return SEVP_CUDA_ERROR;
+  }
+  int k = 0;
+  while (k < cap && h[2 * k] != 0.0) ++k;
+  if (k == 0) return SEVP_BREAKDOWN;
+  // CG-Lanczos tridiagonal: diagonal 1/alpha_j + beta_{j-1}/alpha_{j-1},
+  // off-diagonal sqrt(beta_j)/alpha_j
+  std::vector<double> d((size_t)k), off((size_t)std::max(k - 1, 1));
+  for (int j = 0; j < k; ++j) {
+    d[j] = 1.0 / h[2 * j];
+    if (j > 0) d[j] += h[2 * (j - 1) + 1] / h[2 * (j - 1)];
+    if (j + 1 < k) off[j] = std::sqrt(std::fabs(h[2 * j + 1])) / h[2 * j];
+  }
+  tridiag_extremes(d, off, lmin, lmax);
+  if (iterations) *iterations = k;
   return SEVP_OK;
 }

@@ -186,7 +186,8 @@ class SevpSolver:
         if precond_fp32 is None:
             precond_fp32 = self.precond_fp32
         if method is None:
-            method = self.method
+            # the fused iterations are mixed-precision methods
+            method = self.method if int(precision) == 1 else N.METHOD_PCG
         return N.SolveOpts(int(precision), float(tol), int(max_iter), float(inner_tol),
                            int(use_guess), int(check_every), int(precond_fp32), int(bool(tol_abs)),
                            int(method))
@@ -235,6 +236,31 @@ class SevpSolver:
         ev = np.linalg.eigvalsh(T)
         return dict(lambda_min=float(ev[0]), lambda_max=float(ev[-1]),
                     kappa=float(ev[-1] / ev[0]), iterations=k)
+
+    def set_method(self, method: int):
+        """Outer iteration of the mixed-precision solves: N.METHOD_PCG (two
+        passes per iteration), N.METHOD_CG or N.METHOD_CHEB (one fused launch
+        per iteration; Chebyshev needs bounds, see chebyshev_setup)."""
+        self.method = int(method)
+
+    def estimate_bounds(self, b):
+        """(lambda_min, lambda_max, iterations) of M^-1 A from the CG-Lanczos
+        tridiagonal of one FP64 PCG solve of b (computed in the library)."""
+        lo, hi, it = C.c_double(), C.c_double(), C.c_int()
+        N.check(N.lib().sevp_estimate_bounds(self.h, N.ptr(b), C.byref(lo), C.byref(hi),
+                                             C.byref(it)), "sevp_estimate_bounds")
+        return lo.value, hi.value, it.value
+
+    def set_chebyshev_bounds(self, lmin: float, lmax: float):
+        N.check(N.lib().sevp_set_chebyshev_bounds(self.h, float(lmin), float(lmax)),
+                "sevp_set_chebyshev_bounds")
+
+    def chebyshev_setup(self, b, widen: float = 0.02):
+        """Estimates the bounds from a solve of b, widens them by the factor
+        (1 -/+ widen) (Ritz values lie inside the spectrum) and sets them."""
+        lo, hi, _ = self.estimate_bounds(b)
+        self.set_chebyshev_bounds(lo * (1.0 - widen), hi * (1.0 + widen))
+        return lo, hi
 
     def schwarz_influence_bytes(self) -> int:
         return int(N.lib().sevp_schwarz_influence_bytes(self.h))

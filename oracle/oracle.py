@@ -87,6 +87,9 @@ def lib():
         L.or_pcg.argtypes = [C.c_void_p] + c5 + [C.c_int, f64p, f64p, C.c_double, C.c_int,
                                                  C.POINTER(C.c_double)]
         L.or_pcg.restype = C.c_int
+        L.or_cheb.argtypes = [C.c_void_p] + c5 + [C.c_int, f64p, f64p, C.c_double, C.c_double,
+                                                  C.c_double, C.c_int, C.POINTER(C.c_double)]
+        L.or_cheb.restype = C.c_int
         _lib = L
     return _lib
 
@@ -263,6 +266,15 @@ class TilePC:
         rel = C.c_double()
         it = lib().or_pcg(self.h, *self.c, int(self.p.periodic), _c(b, np.float64), x, tol, maxit,
                           C.byref(rel))
+        return x, it, rel.value
+
+
+    def cheb(self, b, lmin, lmax, x0=None, tol=1e-12, maxit=10000):
+        """Preconditioned Chebyshev iteration on [lmin, lmax] (or_cheb)."""
+        x = np.zeros(b.shape) if x0 is None else _c(x0, np.float64).copy()
+        rel = C.c_double()
+        it = lib().or_cheb(self.h, *self.c, int(self.p.periodic), _c(b, np.float64), x,
+                           float(lmin), float(lmax), tol, maxit, C.byref(rel))
         return x, it, rel.value
 
 

@@ -1176,6 +1176,63 @@ int or_pcg(const tile_pc_t *pc, const float *al, const float *ab, const float *a
   return it;
 }
 
+/* Preconditioned Chebyshev iteration: the new method's second outer
+ * iteration around the tile SEVP preconditioner (the reference's P-CSI,
+ * M/sevp.f90:553-616, is the unpreconditioned form with bounds from
+ * lanczos/ratqr).  Bounds lmin, lmax of the spectrum of M^-1 A:
+ *   theta = (lmax + lmin) / 2, delta = (lmax - lmin) / 2, sigma = theta / delta;
+ *   r = b - A x; d = M^-1 r / theta; rho = 1 / sigma;
+ *   repeat: x += d; r -= A d; rho' = 1 / (2 sigma - rho);
+ *           d = rho' rho d + (2 rho' / delta) M^-1 r; rho = rho'
+ * until ||r|| <= tol ||b|| on the recursive residual; the true residual is
+ * then recomputed and the iteration restarts from it if it is not yet
+ * below the tolerance.  Returns the x updates made; *relres gets the final
+ * true relative residual. */
+int or_cheb(const tile_pc_t *pc, const float *al, const float *ab, const float *ac,
+            const float *ar, const float *at, int periodic, const double *b, double *x,
+            double lmin, double lmax, double tol, int maxit, double *relres) {
+  int nx = pc->T.nx, ny = pc->T.ny;
+  size_t n = (size_t)nx * ny;
+  double *r = malloc(n * 8), *z = malloc(n * 8), *d = malloc(n * 8), *q = malloc(n * 8);
+  double bn = sqrt(or_dot(b, b, nx, ny));
+  if (bn == 0.0) bn = 1.0;
+  const double theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin);
+  const double sigma = theta / delta;
+  int it = 0;
+  double rel = 0.0;
+  for (int restart = 0; restart < 8; ++restart) {
+    or_apply(al, ab, ac, ar, at, nx, ny, periodic, x, q);
+    for (size_t k = 0; k < n; ++k) r[k] = b[k] - q[k];
+    rel = sqrt(or_dot(r, r, nx, ny)) / bn;
+    if (rel <= tol || it >= maxit || !isfinite(rel)) break;
+    or_tile_apply(pc, al, ab, ac, ar, at, r, z);
+    for (size_t k = 0; k < n; ++k) d[k] = z[k] / theta;
+    double rho = 1.0 / sigma;
+    while (it < maxit) {
+      or_apply(al, ab, ac, ar, at, nx, ny, periodic, d, q);
+      for (size_t k = 0; k < n; ++k) {
+        x[k] += d[k];
+        r[k] -= q[k];
+      }
+      ++it;
+      double rr = or_dot(r, r, nx, ny);
+      if (!isfinite(rr)) {
+        it = maxit;
+        break;
+      }
+      if (sqrt(rr) / bn <= tol) break;
+      or_tile_apply(pc, al, ab, ac, ar, at, r, z);
+      const double rho1 = 1.0 / (2.0 * sigma - rho);
+      const double c1 = rho1 * rho, c2 = 2.0 * rho1 / delta;
+      for (size_t k = 0; k < n; ++k) d[k] = c1 * d[k] + c2 * z[k];
+      rho = rho1;
+    }
+  }
+  if (relres) *relres = rel;
+  free(r), free(z), free(d), free(q);
+  return it;
+}
+
 /* ---------------------------------------------------------------------
  * Barotropic pressure correction of FS (M/fs_GLOBAL.f90:1156-1283), the
  * ITMASK loop around the elliptic solve.  Arrays column-major with the

@@ -1,0 +1,178 @@
+"""The fused one-launch iterations (SEVP_METHOD_CG, SEVP_METHOD_CHEB) against
+the CPU oracle.
+
+Each iteration is one kernel launch: the operator is applied inside the tile
+kernel to the previous launch's direction (its halo read from global
+memory), then the tile SEVP solve runs.  They are mixed-precision methods
+(FP32 vectors inside FP64 iterative refinement), so the bars are those of
+the two-pass mixed solve:
+  * ||b - A x|| / ||b|| <= 1e-12, recomputed on the host with the oracle's
+    operator apply;
+  * max|x - x_oracle| <= 1e-8 max|x_oracle| against the oracle's FP64 PCG
+    (and, for Chebyshev, against the oracle's own Chebyshev iteration on the
+    same bounds);
+  * the bounds from the library's CG-Lanczos estimate within 1e-3 of a numpy
+    CG-Lanczos run with the oracle preconditioner.
+"""
+import numpy as np
+import pytest
+
+from musoc_solver_b200 import problems as P
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from musoc_solver_b200 import build
+
+    build.build()
+    return torch
+
+
+CASES = [
+    ("global16x6", lambda: P.global_grid(240, 120, seed=7), 16, 6),
+    ("global16x8", lambda: P.global_grid(180, 90, seed=2), 16, 8),
+    ("basin_closed", lambda: P.basin(1), 16, 6),
+    ("ragged", lambda: P.global_grid(100, 70, seed=3), 12, 5),
+    ("narrow8", lambda: P.global_grid(96, 64, seed=8), 8, 8),
+    ("wide32", lambda: P.global_grid(150, 77, seed=4), 32, 6),
+]
+
+
+def _residual(p, x):
+    return np.linalg.norm(p.b - P.apply_operator(p, x)) / np.linalg.norm(p.b)
+
+
+def _solve(torch, s, p, method, **kw):
+    from musoc_solver_b200 import native as N
+
+    s.set_method(method)
+    b = torch.from_numpy(p.b).cuda()
+    x, rep = s.solve(b, precision=1, **kw)
+    assert rep.status == 0, rep
+    return x.cpu().numpy(), rep
+
+
+@pytest.mark.parametrize("name,mk,tm,th", CASES)
+def test_fused_cg_matches_oracle(torch_cuda, oracle, name, mk, tm, th):
+    from musoc_solver_b200 import native as N
+    from musoc_solver_b200.solver import SevpSolver
+
+    torch = torch_cuda
+    p = mk()
+    s = SevpSolver(p, tile_m=tm, tile_h=th, growth_limit=1e6)
+    pc = oracle.TilePC(p, tm, th, tile_nb=s.tile_nb)
+    xo, _, _ = pc.pcg(p.b, tol=1e-12)
+    x, rep = _solve(torch, s, p, N.METHOD_CG)
+    assert rep.rel_residual <= 1e-12 and _residual(p, x) <= 2e-12
+    assert np.abs(x - xo).max() <= 1e-8 * np.abs(xo).max()
+    # about the iterations of the two-pass PCG (same Krylov recursion, other
+    # rounding)
+    _, rep2 = _solve(torch, s, p, N.METHOD_PCG)
+    assert rep.iterations <= rep2.iterations + 2 * rep2.refinements + 2, (rep, rep2)
+    s.close()
+
+
+@pytest.mark.parametrize("name,mk,tm,th", CASES)
+def test_fused_chebyshev_matches_oracle(torch_cuda, oracle, name, mk, tm, th):
+    from musoc_solver_b200 import native as N
+    from musoc_solver_b200.solver import SevpSolver
+
+    torch = torch_cuda
+    p = mk()
+    s = SevpSolver(p, tile_m=tm, tile_h=th, growth_limit=1e6)
+    b = torch.from_numpy(p.b).cuda()
+    lo, hi = s.chebyshev_setup(b)
+    assert 0 < lo < hi
+    x, rep = _solve(torch, s, p, N.METHOD_CHEB)
+    assert rep.rel_residual <= 1e-12 and _residual(p, x) <= 2e-12
+    pc = oracle.TilePC(p, tm, th, tile_nb=s.tile_nb)
+    xc, itc, relc = pc.cheb(p.b, lo * 0.98, hi * 1.02, tol=1e-12)
+    assert relc <= 1e-12
+    assert np.abs(x - xc).max() <= 1e-8 * np.abs(xc).max()
+    s.close()
+
+
+def test_bounds_match_numpy_lanczos(torch_cuda, oracle):
+    from musoc_solver_b200.solver import SevpSolver
+
+    from test_oracle_cpu import _lanczos_bounds
+
+    torch = torch_cuda
+    p = P.global_grid(160, 80, seed=3)
+    s = SevpSolver(p, tile_m=16, tile_h=6, growth_limit=1e6)
+    lo, hi, it = s.estimate_bounds(torch.from_numpy(p.b).cuda())
+    pc = oracle.TilePC(p, 16, 6, tile_nb=s.tile_nb)
+    lo2, hi2 = _lanczos_bounds(p, pc)
+    assert abs(lo - lo2) <= 1e-3 * lo2 and abs(hi - hi2) <= 1e-3 * hi2, (lo, hi, lo2, hi2)
+    s.close()
+
+
+@pytest.mark.parametrize("method", [1, 2])
+def test_fused_graph_replay_is_bit_identical(torch_cuda, method):
+    from musoc_solver_b200.solver import SevpSolver
+
+    torch = torch_cuda
+    p = P.global_grid(240, 120, seed=9)
+    s = SevpSolver(p, tile_m=16, tile_h=6, growth_limit=1e10)
+    b = torch.from_numpy(p.b).cuda()
+    if method == 2:
+        s.chebyshev_setup(b)
+    s.set_method(method)
+    xg, rg = s.solve(b, precision=1)
+    s.graphs(False)
+    xd, rd = s.solve(b, precision=1)
+    assert rg.iterations == rd.iterations
+    assert torch.equal(xg, xd)
+    s.close()
+
+
+def test_fused_five_plane_and_fp32_influence(torch_cuda, oracle):
+    """The 5-plane (non-symmetric-storage) kernels and the FP32 influence
+    data, on a small grid where FP32 influence data is accurate enough."""
+    from musoc_solver_b200 import native as N
+    from musoc_solver_b200.solver import SevpSolver
+
+    torch = torch_cuda
+    p = P.global_grid(180, 90, seed=2)
+    for kw in (dict(full_coefficients=True), dict(precond_fp32=True)):
+        s = SevpSolver(p, tile_m=16, tile_h=6, growth_limit=1e4, **kw)
+        b = torch.from_numpy(p.b).cuda()
+        s.chebyshev_setup(b)
+        for m in (N.METHOD_CG, N.METHOD_CHEB):
+            x, rep = _solve(torch, s, p, m)
+            assert rep.rel_residual <= 1e-12 and _residual(p, x) <= 2e-12, (kw, m)
+        s.close()
+
+
+def test_fused_methods_refuse_unsupported_settings(torch_cuda):
+    from musoc_solver_b200 import native as N
+    from musoc_solver_b200.solver import SevpSolver
+
+    torch = torch_cuda
+    p = P.global_grid(96, 64, seed=1)
+    b = torch.from_numpy(p.b).cuda()
+    s = SevpSolver(p, tile_m=16, tile_h=6, growth_limit=1e6)
+    s.set_method(N.METHOD_CHEB)
+    with pytest.raises(N.SevpError, match="bounds"):
+        s.solve(b, precision=1)  # no bounds yet
+    o = s.opts(precision=0, method=N.METHOD_CG)
+    import ctypes as C
+
+    rep = N.Report()
+    x = torch.zeros_like(b)
+    assert N.lib().sevp_solve(s.h, N.ptr(b), N.ptr(x), C.byref(o), C.byref(rep)) == N.SEVP_BAD_ARG
+    s.set_schwarz(-1)
+    s.set_method(N.METHOD_CG)
+    with pytest.raises(N.SevpError, match="Schwarz"):
+        s.solve(b, precision=1)
+    s.close()
+    s = SevpSolver(p, tile_m=16, tile_h=12, growth_limit=1e6)
+    s.set_method(N.METHOD_CG)
+    with pytest.raises(N.SevpError, match="8 rows"):
+        s.solve(b, precision=1)
+    s.close()

@@ -245,3 +245,53 @@ def test_tile_preconditioner_is_exact_tile_inverse(oracle):
             idx = np.arange(p.nx * p.ny).reshape(p.ny, p.nx)[b * th:(b + 1) * th, a * tm:(a + 1) * tm].ravel()
             zt = np.linalg.solve(A[np.ix_(idx, idx)], r.ravel()[idx])
             assert np.abs(z.ravel()[idx] - zt).max() <= 1e-9 * np.abs(zt).max()
+
+
+def _lanczos_bounds(p, pc, tol=1e-12):
+    """Extreme Ritz values of M^-1 A from the CG-Lanczos tridiagonal of a
+    numpy PCG run with the oracle preconditioner."""
+    A = P.sparse_matrix(p)
+    b = p.b.ravel()
+    x = np.zeros_like(b)
+    r = b.copy()
+    z = pc.apply(r.reshape(p.ny, p.nx)).ravel()
+    pv = z.copy()
+    rz = r @ z
+    al, be = [], []
+    for _ in range(500):
+        q = A @ pv
+        a = rz / (pv @ q)
+        x += a * pv
+        r -= a * q
+        al.append(a)
+        if np.linalg.norm(r) <= tol * np.linalg.norm(b):
+            break
+        z = pc.apply(r.reshape(p.ny, p.nx)).ravel()
+        rz2 = r @ z
+        be.append(rz2 / rz)
+        rz = rz2
+        pv = z + be[-1] * pv
+    k = len(al)
+    d = np.array([1 / al[j] + (be[j - 1] / al[j - 1] if j else 0.0) for j in range(k)])
+    e = np.array([np.sqrt(be[j]) / al[j] for j in range(k - 1)])
+    ev = np.linalg.eigvalsh(np.diag(d) + np.diag(e, 1) + np.diag(e, -1))
+    return ev[0], ev[-1]
+
+
+@pytest.mark.parametrize("grid", ["global", "basin"])
+def test_tile_chebyshev_matches_scipy(oracle, grid):
+    """The oracle's preconditioned Chebyshev iteration (or_cheb) with bounds
+    from CG-Lanczos converges to the scipy direct solution."""
+    from musoc_solver_b200.solver import tile_sub_blocks
+
+    p = P.global_grid(160, 80, seed=3) if grid == "global" else P.basin(1)
+    pc = oracle.TilePC(p, 16, 6, tile_nb=tile_sub_blocks(p, 16, 6, 1e10))
+    lo, hi = _lanczos_bounds(p, pc)
+    assert 0 < lo < hi
+    x, it, rel = pc.cheb(p.b, lo * 0.98, hi * 1.02, tol=1e-12)
+    assert rel <= 1e-12, (it, rel)
+    xd = spla.spsolve(P.sparse_matrix(p).tocsc(), p.b.ravel()).reshape(p.b.shape)
+    assert np.abs(x - xd).max() <= 1e-9 * np.abs(xd).max()
+    # Chebyshev with exact bounds takes no more than about the CG bound
+    _, it_cg, _ = pc.pcg(p.b, tol=1e-12)
+    assert it <= 3 * it_cg + 10, (it, it_cg)
