@@ -191,16 +191,14 @@ typedef struct {
 } sevp_solve_opts;
 /* Outer iterations of sevp_solve. */
 #define SEVP_METHOD_PCG 0     /* preconditioned CG, two grid passes per iteration */
-/* Fused one-launch iterations (precision 1, block-Jacobi tiles of at most 8
- * rows): each iteration is ONE kernel launch that applies the operator to
- * the previous launch's direction inside the tile kernel (halo values read
- * from global memory) and then runs the tile SEVP solve. */
-#define SEVP_METHOD_CG 1      /* CG with the recursion z_{k+1} = z_k - alpha M^-1 A p_k;
-                                 the three dot products of an iteration in one pass */
-#define SEVP_METHOD_CHEB 2    /* Chebyshev iteration on [lmin, lmax] of M^-1 A (no dot
-                                 product feeds the next launch); needs
-                                 sevp_set_chebyshev_bounds.  The reference's P-CSI
-                                 (M/sevp.f90:553-616) is the unpreconditioned form */
+/* Chebyshev iteration on the spectrum bounds [lmin, lmax] of M^-1 A
+ * (precision 1, block-Jacobi tiles of at most 8 rows; needs
+ * sevp_set_chebyshev_bounds).  No dot product feeds its next update, so
+ * each iteration is ONE kernel launch that applies the operator to the
+ * previous launch's direction inside the tile kernel (halo values read from
+ * global memory) and then runs the tile SEVP solve.  The reference's P-CSI
+ * (M/sevp.f90:553-616) is the unpreconditioned form. */
+#define SEVP_METHOD_CHEB 1
 
 typedef struct {
   int status;          /* SEVP_* */
@@ -278,13 +276,21 @@ int sevp_schwarz_shift(const sevp_ctx *ctx);
 long long sevp_schwarz_influence_bytes(const sevp_ctx *ctx);
 /* Spectrum bounds of the preconditioned operator M^-1 A used by
  * SEVP_METHOD_CHEB (0 < lmin < lmax).  sevp_estimate_bounds runs one FP64
- * PCG solve of b (to 1e-10, not changing any caller buffer) and returns the
+ * PCG solve of b (to 1e-13, not changing any caller buffer) and returns the
  * extreme Ritz values of its CG-Lanczos tridiagonal (the reference gets its
  * bounds from a 10-step Lanczos run and RATQR, M/sevp.f90:618-694); they
  * lie inside the spectrum, so widen them a little before setting them. */
 int sevp_set_chebyshev_bounds(sevp_ctx *ctx, double lmin, double lmax);
 int sevp_estimate_bounds(sevp_ctx *ctx, const double *b, double *lmin, double *lmax,
                          int *iterations);
+/* One launch of the Chebyshev iteration on caller buffers (FP32 device
+ * vectors of the grid), for testing the kernel against a host restatement;
+ * not part of the reference interface.  iter = k (0: the first launch, which
+ * ignores din and forms d_0 = M^-1 r / theta); theta = (lmax + lmin) / 2,
+ * delta = (lmax - lmin) / 2, rho = rho_k.  din is d_k, dout receives d_{k+1};
+ * x += d_k and r -= A d_k in place.  *rr_out = ||r||^2 after the update. */
+int sevp_cheb_step(sevp_ctx *ctx, int iter, double theta, double delta, double rho,
+                   const float *din, float *dout, float *x, float *r, double *rr_out);
 /* Solves A x = b (device pointers, (nx, ny) column-major FP64). */
 int sevp_solve(sevp_ctx *ctx, const double *b, double *x, const sevp_solve_opts *opts,
                sevp_report *report);

@@ -1,39 +1,31 @@
-// Fused one-launch iterations of the tile-SEVP preconditioned solvers.
+// The one-launch Chebyshev iteration with the tile-SEVP preconditioner.
 //
-// The two-pass PCG of solver.cu makes two grid passes per iteration (the
-// stencil pass A and the tile pass B) because each of its two global dot
-// products must be complete before the next vector update.  The kernels
-// here make ONE grid pass per iteration: the operator apply is done inside
-// the tile kernel, on the direction vector of the previous launch, whose
-// values at the tile's halo (the rows above and below the tile, the columns
-// beside it) are read from global memory as the previous launch left them.
-// Each launch reads every vector once and writes every vector once, and the
-// coefficient planes are read once per iteration instead of twice.
+// The PCG of solver.cu makes two grid passes per iteration (the stencil
+// pass A and the tile pass B) because each of its two global dot products
+// must be complete before the next vector update.  A Chebyshev iteration
+// has no dot product that feeds the next update, so one launch does a whole
+// iteration: the operator is applied inside the tile kernel to the previous
+// launch's direction, whose values at the tile's halo (the rows above and
+// below the tile, the columns beside it) are read from global memory as the
+// previous launch left them.
 //
-// kCG: conjugate gradients with the preconditioned operator recursion.  With
-// q = A p and t = M^-1 q, z_{k+1} = M^-1 r_{k+1} = z_k - alpha_k t_k, and
-// (r_{k+1}, z_{k+1}) = (r,z)_k - 2 alpha_k (z_k, q_k) + alpha_k^2 (q_k, t_k)
-// (M symmetric), so all three dot products of an iteration come from one
-// pass and the residual r itself is never formed:
-//   launch k: z_k = z_{k-1} - alpha_{k-1} t_{k-1}; p_k = z_k + beta_{k-1} p_{k-1}
-//             (own points and halo); x_k = x_{k-1} + alpha_{k-1} p_{k-1};
-//             q_k = A p_k; t_k = M^-1 q_k (tile SEVP march);
-//             partial (p_k, q_k), (z_k, q_k), (q_k, t_k)
-//   finisher: alpha_k = rz_k / (p,q); rz_{k+1} from the expansion;
-//             beta_k = rz_{k+1} / rz_k.
-// The last update x += alpha_k p_k is folded into the FP64 residual pass
-// that follows the inner solve.
-//
-// kCheb: preconditioned Chebyshev iteration (the reference's P-CSI without
-// preconditioner is M/sevp.f90:553-616; bounds here come from CG-Lanczos):
+// Preconditioned Chebyshev on the spectrum bounds [lmin, lmax] of M^-1 A
+// (the reference's P-CSI, M/sevp.f90:553-616, is the unpreconditioned form
+// with bounds from lanczos/ratqr; here the bounds come from CG-Lanczos):
 //   theta = (lmax + lmin) / 2, delta = (lmax - lmin) / 2, sigma = theta/delta,
 //   rho_0 = 1/sigma, d_0 = M^-1 r_0 / theta;
 //   launch k+1: x += d_k; r -= A d_k; z = M^-1 r;
 //               rho_{k+1} = 1 / (2 sigma - rho_k);
 //               d_{k+1} = rho_{k+1} rho_k d_k + (2 rho_{k+1} / delta) z;
-//               partial (r, r).
-// No dot product feeds the next launch, so the iteration has no global
-// dependency besides the halo.
+//               partial (r, r) for the stopping test.
+// The first launch (state iter 0) only forms d_0.
+//
+// A one-launch CG is possible too (with t = M^-1 A p, z_{k+1} = z_k -
+// alpha t_k and the three dot products of an iteration from one pass), but
+// its residual is only implied through z, so the FP32 rounding of the
+// stored z and t enters the residual multiplied by the tile operator's
+// norm: measured on the bench grid, the recursion lost its accuracy after
+// a residual reduction of about 1e-4, short of what an inner solve needs.
 #include <algorithm>
 
 #include "solver_core.cuh"
@@ -42,46 +34,8 @@ namespace sevp {
 
 namespace {
 
-// Finishes a kCG launch: alpha_k, the next (r, z) and beta_k.
-struct FinCG {
-  SolveState *st;
-  __device__ void operator()(double (&s)[3]) {
-    const double pq = s[0], zq = s[1], qt = s[2];
-    st->iter += 1;
-    if (!isfinite(pq) || !isfinite(zq) || !isfinite(qt)) {
-      st->status = SEVP_NONFINITE;
-      st->done = 1;
-      return;
-    }
-    if (pq == 0.0) {
-      st->status = SEVP_BREAKDOWN;
-      st->done = 1;
-      return;
-    }
-    const double rz = st->rz, alpha = rz / pq;
-    const double rzn = (rz - 2.0 * alpha * zq) + alpha * alpha * qt;
-    st->alpha = alpha;
-    st->pq = pq;
-    st->rr = rzn;
-    // converged, or (r, z) changed sign: the recursion is at its rounding
-    // floor and the FP64 residual pass takes over
-    if (fabs(rzn) <= st->tol2 * fabs(st->bb) || rzn / rz <= 0.0) {
-      st->status = SEVP_OK;
-      st->done = 1;
-      return;
-    }
-    if (st->iter >= st->max_iter) {
-      st->status = SEVP_MAXITER;
-      st->done = 1;
-      return;
-    }
-    st->beta = rzn / rz;
-    st->rz = rzn;
-  }
-};
-
-// Finishes a kCheb launch: the Chebyshev scalar of this launch and the
-// stopping test on (r, r).
+// Finishes a launch: the Chebyshev scalar of this launch and the stopping
+// test on (r, r).
 struct FinCheb {
   SolveState *st;
   __device__ void operator()(double (&s)[1]) {
@@ -106,46 +60,29 @@ struct FinCheb {
   }
 };
 
-// One fused iteration (see the file comment).  Vector arguments:
-//   kCG:   zi, ti, pi: z_{k-1}, t_{k-1}, p_{k-1}; zo, to, po: z_k, t_k, p_k;
-//          x: x_{k-1} in, x_k out; r unused
-//   kCheb: zi: d_k; zo: d_{k+1}; x, r: in place; ti, pi, to, po unused
-template <typename V, typename MT, bool SYM, int HM, int MODE>
+// One Chebyshev iteration (see the file comment): din = d_k (read on the
+// task's rows and its halo), dout = d_{k+1}; x and r updated in place.
+template <typename V, typename MT, bool SYM, int HM>
 __global__ void __launch_bounds__(kTileWarps * 32, 2)
-    k_fused(TileGeom tg, Coeffs c, int periodic, const MT *__restrict__ mats, const V *zi,
-            const V *ti, const V *pi, V *zo, V *to, V *po, V *x, V *r, SolveState *st,
-            double *partials, unsigned *ticket) {
+    k_cheb(TileGeom tg, Coeffs c, int periodic, const MT *__restrict__ mats, const V *din,
+           V *dout, V *x, V *r, SolveState *st, double *partials, unsigned *ticket) {
   if (st->done) return;
   constexpr bool kChain = sizeof(V) == 4;
-  constexpr int NV = MODE == kFusedCG ? 3 : 1;
   __shared__ double dv_all[kTileWarps * 32];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   double *dv = dv_all + wib * 32;
   const bool first = st->iter == 0;
-  V a_prev = V(0), b_prev = V(0), c1 = V(0), c2 = V(0);
-  if constexpr (MODE == kFusedCG) {
-    if (!first) a_prev = (V)st->alpha, b_prev = (V)st->beta;
+  V c1 = V(0), c2;
+  if (first) {
+    c2 = (V)(1.0 / st->cheb_theta);
   } else {
-    if (first) {
-      c2 = (V)(1.0 / st->cheb_theta);
-    } else {
-      const double rho1 = 1.0 / (2.0 * st->cheb_sigma - st->cheb_rho);
-      c1 = (V)(rho1 * st->cheb_rho);
-      c2 = (V)(2.0 * rho1 / st->cheb_delta);
-    }
+    const double rho1 = 1.0 / (2.0 * st->cheb_sigma - st->cheb_rho);
+    c1 = (V)(rho1 * st->cheb_rho);
+    c2 = (V)(2.0 * rho1 / st->cheb_delta);
   }
-  // the direction at grid index g: p_k (kCG) or d_k (kCheb)
-  auto dir = [&](size_t g) -> V {
-    if constexpr (MODE == kFusedCG) {
-      if (first) return zi[g];
-      return (zi[g] - a_prev * ti[g]) + b_prev * pi[g];
-    } else {
-      return first ? V(0) : zi[g];
-    }
-  };
-  double acc[NV];
-#pragma unroll
-  for (int v = 0; v < NV; ++v) acc[v] = 0.0;
+  // d_k at grid index g (zero before the first launch)
+  auto dir = [&](size_t g) -> V { return first ? V(0) : din[g]; };
+  double acc[1] = {0.0};
   const int nx = tg.nx, ny = tg.ny;
   const int ntasks = tg.ty * tg.txg;
   for (int gw = blockIdx.x * kTileWarps + wib; gw < ntasks; gw += gridDim.x * kTileWarps) {
@@ -174,119 +111,76 @@ __global__ void __launch_bounds__(kTileWarps * 32, 2)
     }
 
     // ---- loads of the task's rows
-    V pv[HM], zc[MODE == kFusedCG ? HM : 1], xr[HM], rv[MODE == kFusedCheb ? HM : 1];
+    V dk[HM], xr[HM], rv[HM];
 #pragma unroll
     for (int k = 0; k < HM; ++k) {
       const bool ok = active && k < hh;
       const size_t g = ok ? idx0 + (size_t)k * nx : 0;
-      if constexpr (MODE == kFusedCG) {
-        V zz = ok ? zi[g] : V(0), xx = ok ? x[g] : V(0);
-        V pp = zz;
-        if (!first && ok) {
-          const V tv = ti[g], po_ = pi[g];
-          zz = zz - a_prev * tv;
-          pp = zz + b_prev * po_;
-          xx = xx + a_prev * po_;
-        }
-        zc[k] = zz;
-        pv[k] = pp;
-        xr[k] = xx;
-      } else {
-        pv[k] = (ok && !first) ? zi[g] : V(0);
-        xr[k] = ok ? x[g] : V(0);
-        rv[k] = ok ? r[g] : V(0);
-      }
+      dk[k] = ok ? dir(g) : V(0);
+      xr[k] = ok ? x[g] : V(0);
+      rv[k] = ok ? r[g] : V(0);
     }
     float cc_[HM], ce_[HM], cn_[HM], cw_[SYM ? 1 : HM], cs_[SYM ? 1 : HM];
     load_task_coeffs<SYM, HM>(c, idx0, nx, hh, active, cc_, ce_, cn_, cw_, cs_);
     const bool has_s = active && j0 > 0, has_n = active && j0 + hh < ny;
-    const V ps = has_s ? dir(idx0 - nx) : V(0);
-    const V pn = has_n ? dir(idx0 + (size_t)hh * nx) : V(0);
+    const V ds = has_s ? dir(idx0 - nx) : V(0);
+    const V dn = has_n ? dir(idx0 + (size_t)hh * nx) : V(0);
     float ab0 = 0.f;
     if constexpr (SYM) ab0 = has_s ? __ldg(c.at + idx0 - nx) : 0.f;
 
-    // ---- q = A p on the task's rows (the full operator, across tile edges)
-    V q[HM];
+    // ---- r -= A d on the task's rows (the full operator, across tile
+    //      edges; in FP64 from the FP32 values, rounded once) and x += d
 #pragma unroll
     for (int k = 0; k < HM; ++k) {
-      V pw = __shfl_sync(0xffffffffu, pv[k], src_w);
-      V pe = __shfl_sync(0xffffffffu, pv[k], src_e);
+      V dw = __shfl_sync(0xffffffffu, dk[k], src_w);
+      V de = __shfl_sync(0xffffffffu, dk[k], src_e);
       float cw = SYM ? __shfl_sync(0xffffffffu, ce_[k], src_w) : cw_[SYM ? 0 : k];
       const bool ok = active && k < hh;
       if (ld_w) {
         const bool okw = ok && iw >= 0;
         const size_t gwi = okw ? (size_t)(j0 + k) * nx + iw : 0;
-        pw = okw ? dir(gwi) : V(0);
+        dw = okw ? dir(gwi) : V(0);
         if constexpr (SYM) cw = okw ? __ldg(c.ar + gwi) : 0.f;
       }
       if (ld_e) {
         const bool oke = ok && ie >= 0;
-        pe = oke ? dir((size_t)(j0 + k) * nx + ie) : V(0);
+        de = oke ? dir((size_t)(j0 + k) * nx + ie) : V(0);
       }
       const float cb = SYM ? (k == 0 ? ab0 : cn_[k > 0 ? k - 1 : 0]) : cs_[SYM ? 0 : k];
-      const V vb = k == 0 ? ps : pv[k > 0 ? k - 1 : 0];
-      const V va = (k + 1 < hh) ? pv[k + 1 < HM ? k + 1 : k] : pn;
-      V av = V(cb) * vb;
-      av += V(cw) * pw;
-      av += V(cc_[k]) * pv[k];
-      av += V(ce_[k]) * pe;
-      av += V(cn_[k]) * va;
-      q[k] = ok ? av : V(0);
-    }
-
-    // ---- elementwise updates and stores of the own rows
-#pragma unroll
-    for (int k = 0; k < HM; ++k) {
-      const bool ok = active && k < hh;
-      if (!ok) continue;
-      const size_t g = idx0 + (size_t)k * nx;
-      if constexpr (MODE == kFusedCG) {
-        zo[g] = zc[k];
-        po[g] = pv[k];
-        x[g] = xr[k];
-        acc[0] += (double)pv[k] * (double)q[k];
-        acc[1] += (double)zc[k] * (double)q[k];
-      } else {
-        const V rn = rv[k] - q[k];
+      const V vb = k == 0 ? ds : dk[k > 0 ? k - 1 : 0];
+      const V va = (k + 1 < hh) ? dk[k + 1 < HM ? k + 1 : k] : dn;
+      double av = (double)cb * (double)vb;
+      av += (double)cw * (double)dw;
+      av += (double)cc_[k] * (double)dk[k];
+      av += (double)ce_[k] * (double)de;
+      av += (double)cn_[k] * (double)va;
+      if (ok) {
+        const size_t g = idx0 + (size_t)k * nx;
+        const V rn = (V)((double)rv[k] - av);
         rv[k] = rn;
         r[g] = rn;
-        x[g] = xr[k] + pv[k];
+        x[g] = xr[k] + dk[k];
         acc[0] += (double)rn * (double)rn;
+      } else {
+        rv[k] = V(0);
       }
     }
 
-    // ---- tile SEVP solve: t = M^-1 q (kCG) or z = M^-1 r (kCheb)
-    auto rhs = [&](int k) -> double {
-      if constexpr (MODE == kFusedCG)
-        return (double)q[k];
-      else
-        return (double)rv[k];
-    };
+    // ---- z = M^-1 r (tile SEVP march) and d_{k+1} = c1 d_k + c2 z
+    auto rhs = [&](int k) -> double { return (double)rv[k]; };
     auto emit = [&](int k, double zk) {
-      const size_t g = idx0 + (size_t)k * nx;
-      if constexpr (MODE == kFusedCG) {
-        const V tv = (V)zk;
-        to[g] = tv;
-        acc[2] += (double)q[k] * (double)tv;
-      } else {
-        zo[g] = c1 * pv[k] + c2 * (V)zk;
-      }
+      dout[idx0 + (size_t)k * nx] = c1 * dk[k] + c2 * (V)zk;
     };
     march_task_regs<MT, SYM, kChain, HM, false>(cc_, ce_, cn_, cw_, cs_, hh, nb, n, mw, active,
                                                 lane, segbase, dv, mt, rhs, emit);
   }
-  if constexpr (MODE == kFusedCG) {
-    FinCG fin{st};
-    reduce_and_finish<NV>(acc, partials, ticket, fin);
-  } else {
-    FinCheb fin{st};
-    reduce_and_finish<NV>(acc, partials, ticket, fin);
-  }
+  FinCheb fin{st};
+  reduce_and_finish<1>(acc, partials, ticket, fin);
 }
 
-template <typename V, typename MT, bool SYM, int HM, int MODE>
-int launch_k(const FusedLaunch<V> &L) {
-  auto kern = k_fused<V, MT, SYM, HM, MODE>;
+template <typename V, typename MT, bool SYM, int HM>
+int launch_k(const ChebLaunch<V> &L) {
+  auto kern = k_cheb<V, MT, SYM, HM>;
   static int slots = 0;
   if (!slots) {
     int per_sm = 0, dev = 0, sms = 0;
@@ -298,33 +192,27 @@ int launch_k(const FusedLaunch<V> &L) {
   const size_t warps = (size_t)L.tg.ty * L.tg.txg;
   const unsigned blocks =
       (unsigned)std::min<size_t>((warps + kTileWarps - 1) / kTileWarps, (size_t)slots);
-  kern<<<blocks, kTileWarps * 32, 0, L.stream>>>(L.tg, L.c, L.periodic, (const MT *)L.mats, L.zi,
-                                                L.ti, L.pi, L.zo, L.to, L.po, L.x, L.r, L.st,
-                                                L.partials, L.ticket);
+  kern<<<blocks, kTileWarps * 32, 0, L.stream>>>(L.tg, L.c, L.periodic, (const MT *)L.mats, L.din,
+                                                L.dout, L.x, L.r, L.st, L.partials, L.ticket);
   SEVP_CUDA_TRY(cudaGetLastError());
   return SEVP_OK;
 }
 
-template <typename V, typename MT, bool SYM, int MODE>
-int launch_h(const FusedLaunch<V> &L) {
-  if (L.tg.hmax <= 6) return launch_k<V, MT, SYM, 6, MODE>(L);
-  return launch_k<V, MT, SYM, kFusedMaxRows, MODE>(L);
-}
-
-template <typename V, int MODE>
-int launch_m(const FusedLaunch<V> &L) {
-  if (L.mats_fp32)
-    return L.sym ? launch_h<V, float, true, MODE>(L) : launch_h<V, float, false, MODE>(L);
-  return L.sym ? launch_h<V, double, true, MODE>(L) : launch_h<V, double, false, MODE>(L);
+template <typename V, typename MT, bool SYM>
+int launch_h(const ChebLaunch<V> &L) {
+  if (L.tg.hmax <= 6) return launch_k<V, MT, SYM, 6>(L);
+  return launch_k<V, MT, SYM, kChebMaxRows>(L);
 }
 
 }  // namespace
 
 template <typename V>
-int fused_launch(const FusedLaunch<V> &L) {
-  if (L.tg.hmax > kFusedMaxRows) return SEVP_BAD_ARG;
-  return L.mode == kFusedCG ? launch_m<V, kFusedCG>(L) : launch_m<V, kFusedCheb>(L);
+int cheb_launch(const ChebLaunch<V> &L) {
+  if (L.tg.hmax > kChebMaxRows) return SEVP_BAD_ARG;
+  if (L.mats_fp32)
+    return L.sym ? launch_h<V, float, true>(L) : launch_h<V, float, false>(L);
+  return L.sym ? launch_h<V, double, true>(L) : launch_h<V, double, false>(L);
 }
-template int fused_launch<float>(const FusedLaunch<float> &);
+template int cheb_launch<float>(const ChebLaunch<float> &);
 
 }  // namespace sevp

@@ -232,18 +232,10 @@ struct OpResidual {
   int set_inner;  // 1: also initialise the inner FP32 solve state
   const double *roww;  // row weights (ny) or null
   int abs_mode;        // the outer test is absolute: ||b - A x|| <= tol
-  // the fused CG leaves its last step out of d: d + dalpha dsel (dsel
-  // null otherwise)
-  const float *dsel;
-  double dalpha;
   __device__ void prepare(SolveState *) {}
   __device__ double value(size_t idx) const {
     double v = x[idx];
-    if (d) {
-      double dv = (double)d[idx];
-      if (dsel) dv += dalpha * (double)dsel[idx];
-      v += dv;
-    }
+    if (d) v += (double)d[idx];
     return v;
   }
   __device__ void emit(size_t idx, int j, double vc, double av, double (&acc)[NV]) const {
@@ -960,8 +952,6 @@ struct sevp_ctx {
   double *x64s = nullptr;  // ping-pong partner for the refinement update
   float *r32 = nullptr, *z32 = nullptr, *p32[2] = {nullptr, nullptr}, *q32 = nullptr,
         *d32 = nullptr;
-  // the fused CG's second pair of t buffers (allocated on first use)
-  float *t32[2] = {nullptr, nullptr};
   // spectrum bounds of M^-1 A for the Chebyshev iteration (0: not set)
   double cheb_lmin = 0.0, cheb_lmax = 0.0;
   double *bh = nullptr;  // device staging for host solves
@@ -1285,8 +1275,7 @@ static void free_work(sevp_ctx *ctx) {
                   ctx->e1h, ctx->e2h, ctx->st, ctx->partials, ctx->tickets,
                   ctx->step_buf[0], ctx->step_buf[1], ctx->step_buf[2], ctx->bstage[0],
                   ctx->bstage[1], ctx->nn_avg,
-                  ctx->s1_64, ctx->s2_64, ctx->s1_32, ctx->s2_32, ctx->hist, ctx->t32[0],
-                  ctx->t32[1]};
+                  ctx->s1_64, ctx->s2_64, ctx->s1_32, ctx->s2_32, ctx->hist};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   ctx->ta.release();
@@ -1735,10 +1724,9 @@ static int read_state(sevp_ctx *ctx) {
 template <typename R>
 static int launch_residual(sevp_ctx *ctx, const double *x, const float *d, double *xout,
                            const double *b, R *r, int set_inner, double tol2,
-                           double outer2 = 0.0, int abs_mode = 0, const float *dsel = nullptr,
-                           double dalpha = 0.0) {
+                           double outer2 = 0.0, int abs_mode = 0) {
   OpResidual<R> op{x, d, xout, b, r, ctx->st, tol2, outer2, set_inner,
-                   ctx->have_res ? ctx->roww : nullptr, abs_mode, dsel, dalpha};
+                   ctx->have_res ? ctx->roww : nullptr, abs_mode};
   if (ctx->have_res) return launch_stencil_c(ctx, op, 2, ctx->cres, ctx->res_sym);
   return launch_stencil(ctx, op, 2);
 }
@@ -1863,31 +1851,19 @@ static int pcg_loop(sevp_ctx *ctx, V *x, V *r, V *z, V *p0, V *p1, V *q, int che
   return SEVP_OK;
 }
 
-// One fused launch (fused.cu) on the block-Jacobi tiling.
-static int launch_fused_k(sevp_ctx *ctx, int mode, const float *zi, const float *ti,
-                          const float *pi, float *zo, float *to, float *po, float *x, float *r) {
+// One Chebyshev launch (fused.cu) on the block-Jacobi tiling.
+static int launch_cheb_k(sevp_ctx *ctx, const float *din, float *dout, float *x, float *r) {
   const Tiling &T = ctx->ta;
   const bool m32 = ctx->infl32_active && T.d_mats32;
-  FusedLaunch<float> L{mode, ctx->sym, m32 ? 1 : 0, T.tg, T.c, ctx->periodic,
-                       m32 ? (const void *)T.d_mats32 : (const void *)T.d_mats,
-                       zi, ti, pi, zo, to, po, x, r, ctx->st, ctx->partials, ctx->tickets + 7,
-                       ctx->stream};
+  ChebLaunch<float> L{ctx->sym, m32 ? 1 : 0, T.tg, T.c, ctx->periodic,
+                      m32 ? (const void *)T.d_mats32 : (const void *)T.d_mats, din, dout, x, r,
+                      ctx->st, ctx->partials, ctx->tickets + 7, ctx->stream};
   ProfScope ps(ctx, 0);
-  int s = fused_launch<float>(L);
+  int s = cheb_launch<float>(L);
   ctx->launches++;
   return s;
 }
 
-// Inner FP32 solve A d = r32 with a fused one-launch iteration, from d = 0
-// (d32 zeroed by the caller).  CG: the first z = M^-1 r is made by a tile
-// pass; the buffers z = {z32, r32} (r is not needed after it), t = t32,
-// p = p32.  Chebyshev: d = {p32[0], p32[1]}, x = d32, r = r32 in place.
-__global__ void k_state_fused_cg(SolveState *st) {
-  st->bb = st->rz;  // stopping reference: (r_0, z_0)
-  st->alpha = 0.0;
-  st->beta = 0.0;
-  st->iter = 0;
-}
 __global__ void k_state_cheb(SolveState *st, double theta, double delta) {
   st->cheb_theta = theta;
   st->cheb_delta = delta;
@@ -1895,32 +1871,18 @@ __global__ void k_state_cheb(SolveState *st, double theta, double delta) {
   st->cheb_rho = delta / theta;
 }
 
-static int fused_inner(sevp_ctx *ctx, int method, int check_every, int *iters_out) {
-  const int mode = method == SEVP_METHOD_CHEB ? kFusedCheb : kFusedCG;
-  if (mode == kFusedCG) {
-    for (float *&t : ctx->t32)
-      if (!t) SEVP_CUDA_TRY(cudaMalloc((void **)&t, ctx->n * sizeof(float)));
-    int s = launch_tile<float, false, true>(ctx, ctx->ta, nullptr, nullptr, ctx->r32, nullptr,
-                                            ctx->z32, 4);
-    if (s) return s;
-    k_state_fused_cg<<<1, 1, 0, ctx->stream>>>(ctx->st);
-  } else {
-    const double lmin = ctx->cheb_lmin, lmax = ctx->cheb_lmax;
-    k_state_cheb<<<1, 1, 0, ctx->stream>>>(ctx->st, 0.5 * (lmax + lmin), 0.5 * (lmax - lmin));
-  }
+// Inner FP32 solve A d = r32 from d = 0 (d32 zeroed by the caller) with the
+// one-launch Chebyshev iteration: directions in p32[0], p32[1], x = d32, r =
+// r32 in place.
+static int cheb_inner(sevp_ctx *ctx, int check_every, int *iters_out) {
+  const double lmin = ctx->cheb_lmin, lmax = ctx->cheb_lmax;
+  k_state_cheb<<<1, 1, 0, ctx->stream>>>(ctx->st, 0.5 * (lmax + lmin), 0.5 * (lmax - lmin));
   ctx->launches++;
   SEVP_CUDA_TRY(cudaGetLastError());
-  float *zb[2] = {ctx->z32, ctx->r32}, *tb[2] = {ctx->t32[0], ctx->t32[1]};
-  float *pb[2] = {ctx->p32[0], ctx->p32[1]};
+  float *db[2] = {ctx->p32[0], ctx->p32[1]};
   auto interval = [&](int &cur) -> int {
     for (int k = 0; k < check_every; ++k) {
-      int s;
-      if (mode == kFusedCG)
-        s = launch_fused_k(ctx, mode, zb[cur], tb[cur], pb[cur], zb[cur ^ 1], tb[cur ^ 1],
-                           pb[cur ^ 1], ctx->d32, nullptr);
-      else
-        s = launch_fused_k(ctx, mode, pb[cur], nullptr, nullptr, pb[cur ^ 1], nullptr, nullptr,
-                           ctx->d32, ctx->r32);
+      int s = launch_cheb_k(ctx, db[cur], db[cur ^ 1], ctx->d32, ctx->r32);
       if (s) return s;
       cur ^= 1;
     }
@@ -1928,7 +1890,7 @@ static int fused_inner(sevp_ctx *ctx, int method, int check_every, int *iters_ou
   };
   const void *const key[5] = {(const void *)ctx->d32, (const void *)ctx->p32[0],
                               (const void *)(ctx->infl32_active ? ctx->ta.d_mats32 : nullptr),
-                              nullptr, (const void *)(uintptr_t)method};
+                              nullptr, (const void *)(uintptr_t)SEVP_METHOD_CHEB};
   int s = graph_loop(ctx, true, key, check_every, check_every, interval);
   if (s) return s;
   *iters_out = ctx->h_st->iter;
@@ -2015,15 +1977,12 @@ static int solve_mixed(sevp_ctx *ctx, const double *b, double *x, const sevp_sol
   double *xa = x, *xb = ctx->x64s;  // ping-pong: the residual kernel reads xa, writes xb
   bool have_d = false;
   const int method = o->method;
-  const float *dsel = nullptr;  // fused CG: the last step alpha_k p_k, left out of d32
-  double dalpha = 0.0;
   for (int refine = 0; refine < 64; ++refine) {
     k_state_init<<<1, 1, 0, ctx->stream>>>(ctx->st, inner2, std::max(o->max_iter - total, 0));
     ctx->launches++;
     int s;
     if (have_d)
-      s = launch_residual<float>(ctx, xa, ctx->d32, xb, b, ctx->r32, 1, inner2, outer2, o->tol_abs,
-                                 dsel, dalpha);
+      s = launch_residual<float>(ctx, xa, ctx->d32, xb, b, ctx->r32, 1, inner2, outer2, o->tol_abs);
     else
       s = launch_residual<float>(ctx, xa, nullptr, nullptr, b, ctx->r32, 1, inner2, outer2,
                                  o->tol_abs);
@@ -2057,14 +2016,7 @@ static int solve_mixed(sevp_ctx *ctx, const double *b, double *x, const sevp_sol
       s = pcg_loop<float>(ctx, ctx->d32, ctx->r32, ctx->z32, ctx->p32[0], ctx->p32[1], ctx->q32,
                           std::max(1, o->check_every), &it);
     } else {
-      s = fused_inner(ctx, method, std::max(1, o->check_every), &it);
-      if (!s && method == SEVP_METHOD_CG && it > 0) {
-        dsel = ctx->p32[it & 1];
-        dalpha = ctx->h_st->alpha;
-      } else {
-        dsel = nullptr;
-        dalpha = 0.0;
-      }
+      s = cheb_inner(ctx, std::max(1, o->check_every), &it);
     }
     if (s) return s;
     total += it;
@@ -2095,11 +2047,11 @@ extern "C" int sevp_solve(sevp_ctx *ctx, const double *b, double *x, const sevp_
     return SEVP_BAD_ARG;
   if (o->method != SEVP_METHOD_PCG) {
     const char *why = nullptr;
-    if (o->method != SEVP_METHOD_CG && o->method != SEVP_METHOD_CHEB) why = "unknown method";
-    else if (o->precision != 1) why = "the fused iterations run in the mixed-precision mode (precision 1)";
-    else if (schwarz_on(ctx)) why = "the fused iterations use the block-Jacobi tiles (no Schwarz)";
-    else if (ctx->ta.tg.hmax > kFusedMaxRows) why = "the fused iterations need tiles of at most 8 rows";
-    else if (o->method == SEVP_METHOD_CHEB && !(ctx->cheb_lmax > ctx->cheb_lmin && ctx->cheb_lmin > 0.0))
+    if (o->method != SEVP_METHOD_CHEB) why = "unknown method";
+    else if (o->precision != 1) why = "the Chebyshev iteration runs in the mixed-precision mode (precision 1)";
+    else if (schwarz_on(ctx)) why = "the Chebyshev iteration uses the block-Jacobi tiles (no Schwarz)";
+    else if (ctx->ta.tg.hmax > kChebMaxRows) why = "the Chebyshev iteration needs tiles of at most 8 rows";
+    else if (!(ctx->cheb_lmax > ctx->cheb_lmin && ctx->cheb_lmin > 0.0))
       why = "Chebyshev needs spectrum bounds (sevp_set_chebyshev_bounds / sevp_estimate_bounds)";
     if (why) {
       std::string m = std::string("sevp_solve: ") + why;
@@ -2626,7 +2578,7 @@ extern "C" int sevp_estimate_bounds(sevp_ctx *ctx, const double *b, double *lmin
   ctx->hist_cap = cap;
   sevp_solve_opts o{};
   o.precision = 0;
-  o.tol = 1e-10;
+  o.tol = 1e-13;
   o.max_iter = cap;
   o.check_every = 4;
   o.method = SEVP_METHOD_PCG;
@@ -2656,4 +2608,34 @@ extern "C" int sevp_estimate_bounds(sevp_ctx *ctx, const double *b, double *lmin
   tridiag_extremes(d, off, lmin, lmax);
   if (iterations) *iterations = k;
   return SEVP_OK;
+}
+
+// One Chebyshev launch on caller buffers with the given scalars (a test
+// hook for the kernel itself; see the header).
+__global__ void k_state_step(SolveState *st, int iter, double theta, double delta, double rho) {
+  SolveState s{};
+  s.iter = iter;
+  s.max_iter = 1 << 30;
+  s.tol2 = 0.0;
+  s.bb = 1.0;
+  s.cheb_theta = theta;
+  s.cheb_delta = delta;
+  s.cheb_sigma = theta / delta;
+  s.cheb_rho = rho;
+  s.status = SEVP_OK;
+  *st = s;
+}
+
+extern "C" int sevp_cheb_step(sevp_ctx *ctx, int iter, double theta, double delta, double rho,
+                              const float *din, float *dout, float *x, float *r,
+                              double *rr_out) {
+  if (!ctx || !ctx->have_op || !din || !dout || !x || !r || iter < 0 || !(delta > 0.0))
+    return SEVP_BAD_ARG;
+  if (ctx->ta.tg.hmax > kChebMaxRows) return SEVP_BAD_ARG;
+  k_state_step<<<1, 1, 0, ctx->stream>>>(ctx->st, iter, theta, delta, rho);
+  int s = launch_cheb_k(ctx, din, dout, x, r);
+  if (!s) s = read_state(ctx);
+  if (s) return s;
+  if (rr_out) *rr_out = ctx->h_st->rr;
+  return ctx->h_st->status;
 }

@@ -455,30 +455,27 @@ __device__ __forceinline__ void load_task_coeffs(const Coeffs &c, size_t idx0, i
   }
 }
 
-// ------------------------------------------- fused one-launch iterations
+// ----------------------------------------- one-launch Chebyshev iteration
 // (fused.cu): one grid pass per iteration, the operator applied inside the
-// tile kernel on the previous launch's direction vector.
-constexpr int kFusedCG = 0;    // conjugate gradients, preconditioned-operator recursion
-constexpr int kFusedCheb = 1;  // Chebyshev
-constexpr int kFusedMaxRows = 8;  // tile rows held in registers
+// tile kernel to the previous launch's direction.
+constexpr int kChebMaxRows = 8;  // tile rows held in registers
 
 template <typename V>
-struct FusedLaunch {
-  int mode;           // kFusedCG or kFusedCheb
+struct ChebLaunch {
   int sym;            // the operator is symmetric: 3-plane reads
   int mats_fp32;      // mats holds FP32 influence data
   TileGeom tg;
   Coeffs c;
   int periodic;
   const void *mats;
-  const V *zi, *ti, *pi;
-  V *zo, *to, *po, *x, *r;
+  const V *din;       // d_k
+  V *dout, *x, *r;    // d_{k+1}; x and r in place
   SolveState *st;
   double *partials;
   unsigned *ticket;
   cudaStream_t stream;
 };
 template <typename V>
-int fused_launch(const FusedLaunch<V> &L);
+int cheb_launch(const ChebLaunch<V> &L);
 
 }  // namespace sevp

@@ -24,9 +24,8 @@ SEVP_CUDA_ERROR = 6
 SEVP_SINGULAR = 7
 SEVP_NONSYMMETRIC = 8
 
-METHOD_PCG = 0   # two-pass PCG
-METHOD_CG = 1    # fused one-launch CG (mixed precision)
-METHOD_CHEB = 2  # fused one-launch Chebyshev (mixed precision, needs bounds)
+METHOD_PCG = 0   # PCG, two grid passes per iteration
+METHOD_CHEB = 1  # one-launch Chebyshev iteration (mixed precision, needs bounds)
 
 GUESS_ZERO, GUESS_PREVIOUS, GUESS_LINEAR, GUESS_LEARNED = 0, 1, 2, 3
 
@@ -96,6 +95,7 @@ _SIGS = {
     "sevp_set_residual_operator": ([P, P, P, P, P, P, P], C.c_int),
     "sevp_set_chebyshev_bounds": ([P, C.c_double, C.c_double], C.c_int),
     "sevp_estimate_bounds": ([P, P, DP, DP, IP], C.c_int),
+    "sevp_cheb_step": ([P, C.c_int, C.c_double, C.c_double, C.c_double] + [P] * 5, C.c_int),
     "sevp_influence_bytes": ([P], C.c_longlong),
     "sevp_solve": ([P, P, P, C.POINTER(SolveOpts), C.POINTER(Report)], C.c_int),
     "sevp_solve_host": ([P, P, P, C.POINTER(SolveOpts), C.POINTER(Report)], C.c_int),

@@ -186,7 +186,7 @@ class SevpSolver:
         if precond_fp32 is None:
             precond_fp32 = self.precond_fp32
         if method is None:
-            # the fused iterations are mixed-precision methods
+            # the Chebyshev iteration is a mixed-precision method
             method = self.method if int(precision) == 1 else N.METHOD_PCG
         return N.SolveOpts(int(precision), float(tol), int(max_iter), float(inner_tol),
                            int(use_guess), int(check_every), int(precond_fp32), int(bool(tol_abs)),
@@ -239,8 +239,8 @@ class SevpSolver:
 
     def set_method(self, method: int):
         """Outer iteration of the mixed-precision solves: N.METHOD_PCG (two
-        passes per iteration), N.METHOD_CG or N.METHOD_CHEB (one fused launch
-        per iteration; Chebyshev needs bounds, see chebyshev_setup)."""
+        passes per iteration) or N.METHOD_CHEB (one launch per iteration;
+        needs bounds, see chebyshev_setup)."""
         self.method = int(method)
 
     def estimate_bounds(self, b):
