@@ -79,6 +79,9 @@ def parse():
                     help="tile shape MxH of the GPU solver, or 'auto' (measured at start-up)")
     ap.add_argument("--precond", default="auto", choices=["auto", "bj", "schwarz"],
                     help="block-Jacobi tiles, the overlapping Schwarz sweep, or 'auto' (measured)")
+    ap.add_argument("--method", default="auto", choices=["auto", "pcg", "cheb"],
+                    help="outer iteration of the mixed solves: PCG, the one-launch Chebyshev "
+                         "iteration, or 'auto' (measured)")
     ap.add_argument("--inner-tol", default="auto",
                     help="relative reduction of each FP32 inner solve, or 'auto' (measured)")
     ap.add_argument("--no-fs", action="store_true",
@@ -87,6 +90,17 @@ def parse():
                     help="skip the 64-member 720x360 ensemble arm")
     ap.add_argument("--no-learned", action="store_true",
                     help="value arm from linear extrapolation instead of the network")
+    ap.add_argument("--profile", choices=["solve", "conv"], default=None,
+                    help="run one small case as a profiler target and exit: 'solve' = one solve "
+                         "of the global grid (--nx, --ny, --tiles, --precond, --method, "
+                         "--profile-precision, --profile-max-iter); 'conv' = forward 3x3 "
+                         "convolutions of the warm-start network (--conv H,W,CIN,COUT)")
+    ap.add_argument("--profile-precision", type=int, default=1, choices=[0, 1])
+    ap.add_argument("--profile-max-iter", type=int, default=3)
+    ap.add_argument("--conv", default="600,904,256,256")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the c1 (96x96 basin), c2 (1440x720), c4 (400-step learned "
+                         "sequence) and reference-call (182x92) arms")
     return ap.parse_args()
 
 
@@ -214,7 +228,7 @@ def max_over_ranks(v, dist, device):
 
 
 # ------------------------------------------------------------ CPU oracle
-def cpu_solve_seconds(p, b, threads, tile_nb=None, tiles=(TILE_M, TILE_H)):
+def cpu_solve_seconds(p, b, threads, tile_nb=None, tiles=(TILE_M, TILE_H), return_x=False):
     """One FP64 tile-SEVP PCG solve with the CPU oracle (setup excluded),
     with the same tile layout as the GPU solver."""
     os.environ["OMP_NUM_THREADS"] = str(threads)
@@ -228,7 +242,7 @@ def cpu_solve_seconds(p, b, threads, tile_nb=None, tiles=(TILE_M, TILE_H)):
     t = time.perf_counter()
     x, it, rel = pc.pcg(b, tol=1e-12)
     dt = time.perf_counter() - t
-    return dt, it, rel
+    return (dt, it, rel, x) if return_x else (dt, it, rel)
 
 
 def run_reference(args, world, rank):
@@ -264,8 +278,339 @@ def run_reference(args, world, rank):
     return 0
 
 
+# ------------------------------------------------- CPU baselines (oracle)
+def _oracle():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    return O
+
+
+def _cpu_iters_child(args):
+    """One process of the all-cores baseline: `iters` PCG iterations of the
+    oracle on one thread (the problem is read from .npy files)."""
+    path, tiles, iters = args
+    os.environ["OMP_NUM_THREADS"] = "1"
+    sys.path.insert(0, ROOT)
+    O = _oracle()
+    from musoc_solver_b200.problems import Problem
+
+    c = [np.load(os.path.join(path, f"{k}.npy")) for k in ("al", "ab", "ac", "ar", "at", "b")]
+    nb = np.load(os.path.join(path, "tile_nb.npy"))
+    p = Problem(*c, periodic=True)
+    pc = O.TilePC(p, tiles[0], tiles[1], tile_nb=nb)
+    t = time.perf_counter()
+    pc.pcg(p.b, tol=1e-300, maxit=iters)
+    return time.perf_counter() - t
+
+
+def cpu_baselines(p, b, tile_nb, tiles, cores, iters_full, sample_iters=4):
+    """The CPU oracle's FP64 tile-SEVP PCG on the host cores, in the two forms
+    the reference's serial code allows: one solve on one thread, and one
+    independent solve per core with every core busy.  Both time
+    `sample_iters` PCG iterations (a bounded sample) and scale to the
+    `iters_full` iterations a full solve takes."""
+    import multiprocessing as mp
+    import tempfile
+
+    # each timing runs in a fresh (spawned) process whose OpenMP runtime
+    # starts with one thread; this process's runtime already has all cores
+    with tempfile.TemporaryDirectory() as d:
+        for k, a in zip(("al", "ab", "ac", "ar", "at"), p.coeffs()):
+            np.save(os.path.join(d, f"{k}.npy"), a)
+        np.save(os.path.join(d, "b.npy"), b)
+        np.save(os.path.join(d, "tile_nb.npy"), tile_nb)
+        ctx = mp.get_context("spawn")
+        job = (d, tuple(tiles), sample_iters)
+        with ctx.Pool(1) as pool:
+            t1 = pool.map(_cpu_iters_child, [job])[0] / sample_iters * iters_full
+        with ctx.Pool(cores) as pool:
+            ts = pool.map(_cpu_iters_child, [job] * cores)
+    t_core = max(ts) / sample_iters * iters_full
+    return {"single_thread": {"value": 1.0 / t1, "unit": "solves/s", "cores": 1,
+                              "seconds_per_solve": t1},
+            "one_solve_per_core": {"value": cores / t_core, "unit": "solves/s", "cores": cores,
+                                   "seconds_per_solve": t_core},
+            "sample": f"{sample_iters} PCG iterations per process, scaled to the {iters_full} "
+                      "iterations of a full solve; setup excluded"}
+
+
+# ----------------------------------------- the other configurations
+def run_c1(K):
+    """c1: the 96x96 closed basin.  The plain FP64 tile-SEVP PCG (24x24 tiles,
+    FP64 marching sub-blocks from the growth bound) on the GPU against the
+    CPU oracle of the same solve; and the reference's own direct method, REP
+    on 12 row blocks of 8 rows (M/sevp.f90:335-438, influence matrices from
+    PRE), as the GPU drop-in rep_ and as the CPU oracle's or_rep."""
+    import ctypes as C
+
+    import torch
+
+    from musoc_solver_b200 import native as N, problems as P
+    from musoc_solver_b200.solver import SevpSolver
+
+    O = _oracle()
+    p = P.basin(0)
+    b = torch.from_numpy(p.b).cuda()
+    s = SevpSolver(p, tile_m=24, tile_h=24, growth_limit=1e10)
+    for _ in range(2):
+        x, r = s.solve(b, precision=0)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(s.stream)
+    for _ in range(K):
+        x, r = s.solve(b, precision=0)
+    ev1.record(s.stream)
+    torch.cuda.synchronize()
+    t_gpu = ev0.elapsed_time(ev1) / 1e3 / K
+    pc = O.TilePC(p, 24, 24, tile_nb=s.tile_nb)
+    t = time.perf_counter()
+    xo, ito, relo = pc.pcg(p.b, tol=1e-12)
+    t_cpu = time.perf_counter() - t
+    xg = x.cpu().numpy()
+    err = float(np.abs(xg - xo).max() / np.abs(xo).max())
+    s.close()
+    out = {"workload": "96x96 closed basin (12 seamounts, dt=60 s), FP64 tile-SEVP PCG, 24x24 "
+                       "tiles, to 1e-12",
+           "gpu": {"value": 1.0 / t_gpu, "unit": "solves/s", "iterations": r.iterations,
+                   "rel_residual": r.rel_residual},
+           "cpu_oracle": {"value": 1.0 / t_cpu, "unit": "solves/s", "iterations": ito,
+                          "threads": int(os.environ["OMP_NUM_THREADS"])},
+           "max_rel_err_vs_cpu_oracle": err}
+    # the reference's REP on full-width row blocks
+    L = N.lib()
+    c = [np.ascontiguousarray(a, np.float32) for a in p.coeffs()]
+    j2, i2 = p.ac.shape
+    ie, _ = O.block_partition(j2, 12)
+    nb = len(ie)
+    rinv = np.zeros((nb, i2, i2))
+    rinv1 = np.zeros((nb - 1, i2, i2))
+    h = np.zeros((j2 + 2, i2 + 2))
+    pp = lambda a: a.ctypes.data_as(C.c_void_p)
+    ii = lambda v: C.byref(C.c_int(int(v)))
+    L.sevp_set_periodic_we(0)
+    L.pre_(*[pp(a) for a in c], pp(rinv), pp(rinv1), pp(h), pp(ie), ii(i2), ii(i2 + 2), ii(i2),
+           ii(nb))
+    f = p.b.astype(np.float32)
+    d0, d1, d2 = np.zeros((nb - 1, i2)), np.zeros(i2), np.zeros(i2)
+    hh = np.zeros((j2 + 2, i2 + 2))
+    xr = np.zeros((j2 + 2, i2 + 2))
+    L.sevp_dropin_cache(1)
+    args = [pp(a) for a in c] + [pp(rinv), pp(rinv1), pp(d0), pp(d1), pp(d2), pp(f), pp(hh),
+                                 pp(xr), pp(ie), ii(i2 + 2), ii(i2), ii(nb)]
+    L.rep_(*args)
+    t = time.perf_counter()
+    for _ in range(K):
+        xr[:] = 0.0
+        L.rep_(*args)
+    t_rep = (time.perf_counter() - t) / K
+    st = L.sevp_last_status()
+    L.sevp_dropin_cache(0)
+    L.sevp_set_periodic_we(1)
+    t = time.perf_counter()
+    xro = O.rep(*c, rinv, rinv1, f, np.zeros((j2 + 2, i2 + 2)), ie)
+    t_rep_cpu = time.perf_counter() - t
+    res = np.linalg.norm(f - P.apply_operator(p, xr[1:-1, 1:-1])) / np.linalg.norm(f)
+    out["reference_method_rep"] = {
+        "method": "REP, 12 row blocks of 8 rows (influence matrices from PRE), host arrays in "
+                  "and out per call, device copies of the coefficients and RINV cached",
+        "gpu_dropin": {"value": 1.0 / t_rep, "unit": "solves/s", "status": st},
+        "cpu_oracle": {"value": 1.0 / t_rep_cpu, "unit": "solves/s", "threads": 1},
+        "bit_identical_to_cpu_oracle": bool(np.array_equal(xr, xro)),
+        "rel_residual": float(res)}
+    return out
+
+
+def run_c2(K, tiles=(16, 6)):
+    """c2: the 1440x720 periodic global grid, plain FP64 tile-SEVP PCG to
+    1e-12 from zero; condition of the preconditioned operator from the
+    CG-Lanczos bounds; the CPU oracle's solve and the error against it."""
+    import torch
+
+    from musoc_solver_b200 import problems as P
+    from musoc_solver_b200.solver import SevpSolver
+
+    O = _oracle()
+    p = P.global_grid(1440, 720, seed=1)
+    b = torch.from_numpy(p.b).cuda()
+    s = SevpSolver(p, tile_m=tiles[0], tile_h=tiles[1], growth_limit=GROWTH)
+    lo, hi, _ = s.estimate_bounds(b)
+    for _ in range(2):
+        x, r = s.solve(b, precision=0)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(s.stream)
+    for _ in range(K):
+        x, r = s.solve(b, precision=0)
+    ev1.record(s.stream)
+    torch.cuda.synchronize()
+    t_gpu = ev0.elapsed_time(ev1) / 1e3 / K
+    xm, rm = s.solve(b, precision=1)
+    pc = O.TilePC(p, tiles[0], tiles[1], tile_nb=s.tile_nb)
+    t = time.perf_counter()
+    xo, ito, relo = pc.pcg(p.b, tol=1e-12)
+    t_cpu = time.perf_counter() - t
+    scale = np.abs(xo).max()
+    out = {"workload": f"1440x720 global grid (lat +-78, ~30% land, dt=60 s), FP64 tile-SEVP "
+                       f"PCG from zero to 1e-12, {tiles[0]}x{tiles[1]} tiles",
+           "gpu_fp64": {"value": 1.0 / t_gpu, "unit": "solves/s", "iterations": r.iterations,
+                        "rel_residual": r.rel_residual},
+           "gpu_mixed": {"ms": rm.ms, "iterations": rm.iterations, "rel_residual": rm.rel_residual},
+           "kappa_preconditioned": hi / lo, "lambda_min": lo, "lambda_max": hi,
+           "cpu_oracle": {"value": 1.0 / t_cpu, "unit": "solves/s", "iterations": ito,
+                          "threads": int(os.environ["OMP_NUM_THREADS"])},
+           "max_rel_err_vs_cpu_oracle": {
+               "fp64": float(np.abs(x.cpu().numpy() - xo).max() / scale),
+               "mixed": float(np.abs(xm.cpu().numpy() - xo).max() / scale)}}
+    s.close()
+    return out
+
+
+def run_reference_call(K):
+    """The reference's solver call at its own 182x92 grid: FS_SOLVER's
+    FL_EVP_STP = 0 path (M/fs_GLOBAL.f90:1852-1853), REP1 on 15 row blocks
+    then p_bicgstab_le, on the reference's test stencil
+    (P/prep_GLOBAL.f90:246-261, AC shifted by 0.01 so that the system is not
+    singular) with a REAL*4 right-hand side: the GPU drop-ins rep1_ and
+    p_bicgstab_le_ (host arrays, device copies of RINV cached) against the
+    CPU oracle's or_rep1 and or_bicgstab_le on one thread; and the fast
+    drop-in p_sevp_pcg_ with the same argument list, to 1e-12 relative."""
+    import ctypes as C
+
+    from musoc_solver_b200 import native as N, problems as P
+
+    O = _oracle()
+    L = N.lib()
+    p = P.idealised(180, 90)
+    p.ac[:] += np.float32(0.01)
+    c = [np.ascontiguousarray(a, np.float32) for a in p.coeffs()]
+    j2, i2 = p.ac.shape
+    rng = np.random.default_rng(5)
+    f = rng.standard_normal((j2, i2)).astype(np.float32)
+    ie, _ = O.block_partition(j2, 15)
+    nb = len(ie)
+    pp = lambda a: a.ctypes.data_as(C.c_void_p)
+    ii = lambda v: C.byref(C.c_int(int(v)))
+    rinv = np.zeros((nb, i2, i2))
+    rinv1 = np.zeros((nb - 1, i2, i2))
+    h = np.zeros((j2 + 2, i2 + 2))
+    L.sevp_set_periodic_we(1)
+    L.pre1_(*[pp(a) for a in c], pp(rinv), pp(rinv1), pp(h), pp(ie), ii(i2 + 2), ii(i2), ii(nb))
+    d0, d1, d2 = np.zeros((nb - 1, i2)), np.zeros(i2), np.zeros(i2)
+    hh = np.zeros((j2 + 2, i2 + 2))
+    x = np.zeros((j2 + 2, i2 + 2))
+    L.sevp_dropin_cache(1)
+
+    def gpu_rep1():
+        x[:] = 0.0
+        L.rep1_(*[pp(a) for a in c], pp(rinv), pp(rinv1), pp(d0), pp(d1), pp(d2), pp(f), pp(hh),
+                pp(x), pp(ie), ii(i2 + 2), ii(i2), ii(nb))
+
+    def gpu_bicg():
+        xb = np.zeros((j2 + 2, i2 + 2))
+        L.p_bicgstab_le_(*[pp(a) for a in c], pp(f), pp(xb), *[pp(a) for a in c], ii(i2), ii(j2))
+        return xb
+
+    def gpu_fast():
+        xf = np.zeros((j2 + 2, i2 + 2))
+        L.p_sevp_pcg_(*[pp(a) for a in c], pp(f), pp(xf), *[pp(a) for a in c], ii(i2), ii(j2))
+        return xf
+
+    def timed(fn, n):
+        fn()
+        t = time.perf_counter()
+        for _ in range(n):
+            out = fn()
+        return (time.perf_counter() - t) / n, out
+
+    t_rep1, _ = timed(gpu_rep1, K)
+    xrep = x.copy()
+    t_bicg, xb = timed(gpu_bicg, max(1, K // 4))
+    o = N.FsOptions()
+    L.sevp_fs_default_options(C.byref(o))
+    L.sevp_fs_set_options(C.byref(o))
+    t_fast, xf = timed(gpu_fast, K)
+    rep = N.Report()
+    L.sevp_fs_last_report(C.byref(rep))
+    L.sevp_dropin_cache(0)
+    L.sevp_fs_release()
+    t = time.perf_counter()
+    xro = O.rep1(*c, rinv, rinv1, f, np.zeros((j2 + 2, i2 + 2)), ie)
+    t_rep1_cpu = time.perf_counter() - t
+    t = time.perf_counter()
+    xbo, itbo, resbo = O.bicgstab(*c, f, np.zeros((j2 + 2, i2 + 2)))
+    t_bicg_cpu = time.perf_counter() - t
+    rel = lambda xx: float(np.linalg.norm(f - P.apply_operator(p, xx[1:-1, 1:-1]))
+                           / np.linalg.norm(f))
+    return {"workload": "182x92 (I0 x J0), the reference's test stencil (AC + 0.01), REAL*4 "
+                        "right-hand side N(0,1); FS_SOLVER FL_EVP_STP=0: REP1 (15 row blocks) "
+                        "then p_bicgstab_le (stop: sqrt(r.r) <= 1e-8)",
+            "rep1": {"gpu_dropin": {"value": 1.0 / t_rep1, "unit": "calls/s"},
+                     "cpu_oracle": {"value": 1.0 / t_rep1_cpu, "unit": "calls/s", "threads": 1},
+                     "bit_identical_to_cpu_oracle": bool(np.array_equal(xrep, xro)),
+                     "rel_residual": rel(xrep)},
+            "p_bicgstab_le": {"gpu_dropin": {"value": 1.0 / t_bicg, "unit": "calls/s"},
+                              "cpu_oracle": {"value": 1.0 / t_bicg_cpu, "unit": "calls/s",
+                                             "threads": 1, "iterations": itbo},
+                              "rel_residual": rel(xb),
+                              "max_abs_diff_vs_cpu_oracle": float(np.abs(xb - xbo).max())},
+            "p_sevp_pcg": {"gpu_dropin": {"value": 1.0 / t_fast, "unit": "calls/s",
+                                          "iterations": rep.iterations},
+                           "rel_residual": rel(xf),
+                           "max_rel_err_vs_rep1_cpu_oracle":
+                               float(np.abs(xf - xro)[1:-1, 1:-1].max()
+                                     / np.abs(xro[1:-1, 1:-1]).max())}}
+
+
+def run_c4(steps=400, train_steps=300, coarse=4, epochs=3, tiles=(16, 8)):
+    """c4: the learned warm start on a 400-step 1440x720 eddy sequence: FP64
+    solves of every step (the training data), the U-Net trained on steps
+    2..299 and tested on 302..399 with iterations and device time (guess +
+    mixed solve to 1e-12) from the zero, previous, linear and learned
+    guesses."""
+    import torch
+
+    from musoc_solver_b200 import problems as P
+    from musoc_solver_b200.solver import SevpSolver
+    from musoc_solver_b200.warmstart import LearnedWarmStart, evaluate, solve_sequence, train
+
+    t0 = time.perf_counter()
+    p = P.global_grid(1440, 720, seed=1)
+    wet = p.meta["wet"]
+    rhs = [torch.from_numpy(np.where(wet, b, 0.0)).cuda()
+           for _, b in P.eddy_rhs(1440, 720, range(steps), seed=3)]
+    s = SevpSolver(p, tile_m=tiles[0], tile_h=tiles[1], growth_limit=GROWTH)
+    etas = solve_sequence(s, rhs)
+    torch.cuda.synchronize()
+    t_seq = time.perf_counter() - t0
+    train_idx = list(range(2, train_steps))
+    test_idx = list(range(train_steps + 2, steps))
+    t1 = time.perf_counter()
+    w = LearnedWarmStart.create(s, seed=0, train=True, coarse=coarse)
+    losses = train(w, etas, rhs, train_idx, epochs=epochs, lr=2e-3, lr_final=2e-4)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t1
+    w = w.inference_copy()
+    x = torch.zeros_like(etas[0])
+    gain = []
+    for n in test_idx:
+        w.predict(etas[n - 1], etas[n - 2], rhs[n], x)
+        gain.append(float((w.e + w.m - etas[n]).norm() / (x - etas[n]).norm()))
+    w.attach()
+    res = evaluate(s, w, etas, rhs, test_idx)
+    w.close()
+    s.close()
+    return {"workload": f"1440x720 global grid, {steps}-step eddy sequence (300 eddies, 0.2 m/s), "
+                        f"train steps 2-{train_steps - 1}, test {train_steps + 2}-{steps - 1}; "
+                        f"network on the 1/{coarse} grid; mixed solve to 1e-12, "
+                        f"{tiles[0]}x{tiles[1]} tiles",
+            "fp64_sequence_seconds": t_seq, "train_seconds": t_train, "epochs": epochs,
+            "loss_first_last": [losses[0][1], losses[-1][1]],
+            "guess_error_ratio_without_over_with_network": float(np.median(gain)),
+            "test": res}
+
+
 # --------------------------------------------------------------- ensemble
-def run_ensemble(K, W, members=64, nx=720, ny=360, schwarz=False, inner_tol=1e-5):
+def run_ensemble(K, W, members=64, nx=720, ny=360, schwarz=False, inner_tol=1e-5,
+                 oracle_check=True):
     """64 members x 720x360 (independently perturbed depths and right-hand
     sides) stacked into one system: every kernel launch covers all members."""
     import torch
@@ -308,11 +653,29 @@ def run_ensemble(K, W, members=64, nx=720, ny=360, schwarz=False, inner_tol=1e-5
             xm = x.clone()
         if name == "fp64":
             x64 = x.clone()
-    # per-member error of the mixed solve against the FP64 solve
+    # per-member error of the mixed solve against the FP64 solve on the GPU
     d = (xm - x64).reshape(members, -1).abs().amax(dim=1)
     ref = x64.reshape(members, -1).abs().amax(dim=1)
     out["mixed"]["max_member_rel_err_vs_fp64"] = float((d / ref).max())
     e.close()
+    # and every member of both solves against the CPU oracle's FP64 PCG of
+    # that member alone
+    if oracle_check:
+        from musoc_solver_b200.solver import tile_sub_blocks
+
+        O = _oracle()
+        xm_h = xm.reshape(members, ny, nx).cpu().numpy()
+        x64_h = x64.reshape(members, ny, nx).cpu().numpy()
+        errs_m, errs_64, t0 = [], [], time.perf_counter()
+        for k, m in enumerate(ms):
+            pc = O.TilePC(m, 16, 8, tile_nb=tile_sub_blocks(m, 16, 8, GROWTH))
+            xo, _, relo = pc.pcg(m.b, tol=1e-12)
+            sc = np.abs(xo).max()
+            errs_m.append(float(np.abs(xm_h[k] - xo).max() / sc))
+            errs_64.append(float(np.abs(x64_h[k] - xo).max() / sc))
+        out["max_member_rel_err_vs_cpu_oracle"] = {"mixed": max(errs_m), "fp64": max(errs_64),
+                                                   "members": members,
+                                                   "oracle_seconds": time.perf_counter() - t0}
     return out
 
 
@@ -406,19 +769,22 @@ def run_native(args, world, rank, local, dist):
         tuple(int(v) for v in args.tiles.lower().split("x")),)
     sw_opts = {"auto": (False, True), "bj": (False,), "schwarz": (True,)}[args.precond]
     itols = (1e-5, 1e-6) if args.inner_tol == "auto" else (float(args.inner_tol),)
-    if len(cands) * len(sw_opts) * len(itols) > 1:
+    methods = {"auto": (N.METHOD_PCG, N.METHOD_CHEB), "pcg": (N.METHOD_PCG,),
+               "cheb": (N.METHOD_CHEB,)}[args.method]
+    if len(cands) * len(sw_opts) * len(itols) * len(methods) > 1:
         best, tune_table = autotune(p, b_dev[T - 1], candidates=cands, precision=1,
                                     growth_limit=GROWTH, schwarz=sw_opts, inner_tols=itols,
-                                    history=(eta[T - 2], eta[T - 3]))
+                                    history=(eta[T - 2], eta[T - 3]), methods=methods)
         tiles, use_sw, itol = (best["tile_m"], best["tile_h"]), best["schwarz"], best["inner_tol"]
+        method = best["method"]
     else:
-        tiles, use_sw, itol = cands[0], sw_opts[0], itols[0]
+        tiles, use_sw, itol, method = cands[0], sw_opts[0], itols[0], methods[0]
     if dist is not None:
         # every rank runs the same arms (and so the same collectives): rank
         # 0's choice holds for all
-        choice = [(tuple(tiles), bool(use_sw), float(itol))]
+        choice = [(tuple(tiles), bool(use_sw), float(itol), int(method))]
         dist.broadcast_object_list(choice, src=0)
-        tiles, use_sw, itol = choice[0]
+        tiles, use_sw, itol, method = choice[0]
     if use_sw and tiles[1] > SCHWARZ_MAX_ROWS:
         raise SystemExit(f"the Schwarz preconditioner needs tiles of at most {SCHWARZ_MAX_ROWS} rows")
     if tuple(tiles) == (16, 6) and not use_sw:
@@ -428,6 +794,12 @@ def run_native(args, world, rank, local, dist):
         solver = SevpSolver(p, tile_m=tiles[0], tile_h=tiles[1], growth_limit=GROWTH,
                             precond_fp32=args.precond_fp32, schwarz=use_sw)
     stream = solver.stream
+    cheb_bounds = None
+    if method == N.METHOD_CHEB:
+        # spectrum bounds of the operator's set-up (untimed, like the
+        # influence data)
+        cheb_bounds = solver.chebyshev_setup(b_dev[T - 1])
+    solver.set_method(method)
     torch.cuda.synchronize()
 
     eta += [torch.zeros_like(eta[0]) for _ in range(W + K)]
@@ -492,14 +864,19 @@ def run_native(args, world, rank, local, dist):
     # ---- the same sequence from linear extrapolation (no network)
     eta_lin = eta[:T] + [torch.zeros_like(eta[0]) for _ in range(W + K)]
     t_lin, reps_lin, _ = run_arm(N.GUESS_LINEAR, eta_lin)
+    x_lin0 = eta_lin[timed[0]].cpu().numpy()
     del eta_lin
 
-    # error of the value arm against an FP64 solve of the same steps
+    # error of the value arm against an FP64 solve of the same steps (the
+    # FP64 solve of the first timed step is kept for the CPU-oracle check)
     ref_x = torch.zeros_like(eta[0])
     errs = []
+    x64_0 = None
     for k in (timed[0], timed[-1]):
         solver.solve(b_dev[k], x=ref_x.zero_(), precision=0)
         errs.append(float((eta[k] - ref_x).abs().max() / ref_x.abs().max()))
+        if x64_0 is None:
+            x64_0 = ref_x.cpu().numpy()
 
     # ---- plain FP64 SEVP-PCG from a zero guess (block-Jacobi tiles)
     def fp64_zero_arm():
@@ -603,10 +980,17 @@ def run_native(args, world, rank, local, dist):
     b_stage2 = n * (4 + 4 + halo + 4 * ncoef) + infl_b
     b_stage3 = n * (4 + 4 + 4 + 4 + halo + 4 * ncoef) + infl_a
     b_couple = 0.5 * (b_stage2 + b_stage3)
+    # one Chebyshev launch: d (own rows, halo from L2), x, r in; x, r, d out;
+    # coefficient planes; influence data
+    b_cheb = n * (4 * 3 + 4 * 3 + 4 * ncoef) + infl_a
     short_tiles = tiles[1] <= 6  # FP32 vectors with tiles up to 6 rows run the short-tile kernel
     passb_name = ("k_tile_short<float, update, dots>" if short_tiles
                   else "k_tile_apply<float, update, dots>") + " (PCG pass B)"
-    if use_sw and cpl_n:
+    if method == N.METHOD_CHEB:
+        dom_name = "k_cheb<float> (one-launch Chebyshev iteration)"
+        bytes_per_launch, avg_s, dom_n = b_cheb, tile_ms / 1e3 / max(tile_n, 1), tile_n
+        traffic = None
+    elif use_sw and cpl_n:
         dom_name = "k_tile_couple<float> (Schwarz stages 2 and 3, averaged per launch)"
         bytes_per_launch, avg_s, dom_n = b_couple, cpl_ms / 1e3 / cpl_n, cpl_n
         traffic = ncu_traffic(p.nx, p.ny, tiles, "couple")
@@ -626,15 +1010,36 @@ def run_native(args, world, rank, local, dist):
     if not args.no_fs:
         fs = run_fs(p.nx, p.ny, 20, tiles, peak=peak, schwarz=use_sw, inner_tol=itol)
 
-    # ---- CPU baseline (rank 0 at N = 1)
-    cpu = None
+    # ---- the other configurations (rank 0 at N = 1; no collectives)
+    c1 = c2 = c4 = ref_call = None
+    if rank == 0 and world == 1 and not args.no_configs:
+        c1 = run_c1(max(K, 10))
+        c2 = run_c2(max(2, K // 2))
+        ref_call = run_reference_call(max(4, K // 2))
+        if not args.no_learned:
+            c4 = run_c4()
+
+    # ---- CPU baseline and the error against the CPU oracle (rank 0 at N = 1)
+    cpu, cpu_forms, oracle_err = None, None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cores = os.cpu_count() or 1
-        dt, itc, relc = cpu_solve_seconds(p, rhs[timed[0]], cores, solver.tile_nb, tiles)
+        k0 = timed[0]
+        dt, itc, relc, xo = cpu_solve_seconds(p, rhs[k0], cores, solver.tile_nb, tiles,
+                                              return_x=True)
         cpu = {"value": 1.0 / dt, "unit": "solves/s", "cores": cores, "kind": "port",
-               "sample": f"one full FP64 tile-SEVP PCG solve of step {timed[0]} with the C oracle "
+               "sample": f"one full FP64 tile-SEVP PCG solve of step {k0} with the C oracle "
                          f"(OpenMP, {cores} threads, {itc} iterations, rel. residual {relc:.2e}), "
                          "setup excluded"}
+        cpu_forms = cpu_baselines(p, rhs[k0], solver.tile_nb, tiles, cores, itc)
+        sc = float(np.abs(xo).max())
+
+        def err(xg):
+            d = float(np.abs(xg - xo).max())
+            return {"max_abs_deta": d, "max_rel_deta": d / sc}
+
+        oracle_err = {"step": k0, "oracle": "C oracle FP64 tile-SEVP PCG to 1e-12",
+                      "value_arm": err(eta[k0].cpu().numpy()), "linear_mixed": err(x_lin0),
+                      "fp64_plain": err(x64_0)}
 
     value = world * K / t_value
     line = {
@@ -658,8 +1063,11 @@ def run_native(args, world, rank, local, dist):
             "preconditioner": (f"overlapping Schwarz, second tiling shifted by "
                                f"{solver.schwarz_shift} columns" if use_sw else "block-Jacobi tiles"),
             "inner_tol": itol,
+            "outer_iteration": "one-launch Chebyshev" if method == N.METHOD_CHEB else "PCG",
+            "chebyshev_bounds": cheb_bounds,
             "tile_autotune": None if tune_table is None else
-            {f"{r['tile_m']}x{r['tile_h']}{' schwarz' if r['schwarz'] else ''} itol={r['inner_tol']:g}":
+            {f"{r['tile_m']}x{r['tile_h']}{' schwarz' if r['schwarz'] else ''}"
+             f"{' cheb' if r['method'] == N.METHOD_CHEB else ''} itol={r['inner_tol']:g}":
              round(r["ms"], 2) for r in tune_table},
             "tile_autotune_workload": "one warm-start step (linear extrapolation), mixed solve",
             "marching_growth_limit": GROWTH,
@@ -668,22 +1076,10 @@ def run_native(args, world, rank, local, dist):
             "tol": 1e-12, "parallelism": f"replicas x{world}",
             "l2": "inputs larger than L2 (69 MB per FP64 field), no flush",
         },
-        "fp64_plain": {"value": world * K / t_fp64, "unit": "solves/s",
-                       "ms_per_step": 1e3 * t_fp64 / K,
-                       "mean_iterations": float(np.mean(it64)),
-                       "preconditioner": "block-Jacobi tiles"},
         "fp64_schwarz_zero_guess": fp64_sw,
         "mixed_zero_guess": {"value": world * K / t_mixed0, "unit": "solves/s",
                              "mean_iterations": float(np.mean(itmz))},
-        "linear_mixed": {"value": world * K / t_lin, "unit": "solves/s",
-                         "ms_per_step": 1e3 * t_lin / K,
-                         "mean_iterations": float(np.mean([r.iterations for r in reps_lin]))},
         "warm_start_training": train_info,
-        "value_arm": {"mean_iterations": float(np.mean([r.iterations for r in reps])),
-                      "mean_refinements": float(np.mean([r.refinements for r in reps])),
-                      "max_rel_residual": float(max(relres)), "status": sorted(set(status)),
-                      "max_rel_err_vs_fp64": float(max(errs))},
-        "speedup_vs_fp64_plain": (K / t_value) / (K / t_fp64),
         "e2e": {"value": world * K / t_e2e, "unit": "solves/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h,
                 "api": "sevp_step_prefetch / sevp_step_submit / sevp_step_wait (history of the "
@@ -700,9 +1096,11 @@ def run_native(args, world, rank, local, dist):
                      "algorithmic_bytes_per_launch": bytes_per_launch,
                      "avg_launch_ms": avg_s * 1e3, "launches": dom_n,
                      "peak_source": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)"},
-        "kernels": {"tile_pass_b": {"launches": tile_n,
+        "kernels": {"tile_pass_b" if method != N.METHOD_CHEB else "chebyshev": {
+                                    "launches": tile_n,
                                     "avg_ms": tile_ms / max(tile_n, 1),
-                                    "hbm_frac": (b_passb / (tile_ms / 1e3 / tile_n) / 1e9 / peak)
+                                    "hbm_frac": ((b_cheb if method == N.METHOD_CHEB else b_passb)
+                                                 / (tile_ms / 1e3 / tile_n) / 1e9 / peak)
                                     if tile_n else None},
                     "schwarz_stages": {"launches": cpl_n, "avg_ms": cpl_ms / max(cpl_n, 1),
                                        "hbm_frac": (b_couple / (cpl_ms / 1e3 / cpl_n) / 1e9 / peak)
@@ -713,10 +1111,30 @@ def run_native(args, world, rank, local, dist):
                                            "avg_ms": prof["precond"][0] / max(prof["precond"][1], 1)}},
         "ensemble_c5": ens,
         "fs_barotropic_loop": fs,
+        "config_c1_basin": c1,
+        "config_c2_1440x720": c2,
+        "config_c4_learned_sequence": c4,
+        "reference_solver_call_182x92": ref_call,
         "cpu_baseline": cpu,
+        "cpu_baseline_forms": cpu_forms,
         "clocks": clk.summary(),
         "gpu_launches": int(launches_value),
         "gpu_launches_e2e": int(launches_e2e),
+        # the north-star comparison, last so that a stored tail of the line keeps it
+        "value_arm": {"mean_iterations": float(np.mean([r.iterations for r in reps])),
+                      "mean_refinements": float(np.mean([r.refinements for r in reps])),
+                      "max_rel_residual": float(max(relres)), "status": sorted(set(status)),
+                      "max_rel_err_vs_fp64_gpu": float(max(errs))},
+        "linear_mixed": {"value": world * K / t_lin, "unit": "solves/s",
+                         "ms_per_step": 1e3 * t_lin / K,
+                         "mean_iterations": float(np.mean([r.iterations for r in reps_lin]))},
+        "fp64_plain": {"value": world * K / t_fp64, "unit": "solves/s",
+                       "ms_per_step": 1e3 * t_fp64 / K,
+                       "mean_iterations": float(np.mean(it64)),
+                       "preconditioner": "block-Jacobi tiles"},
+        "speedup_vs_fp64_plain": (K / t_value) / (K / t_fp64),
+        "linear_mixed_speedup_vs_fp64_plain": (K / t_lin) / (K / t_fp64),
+        "error_vs_cpu_oracle": oracle_err,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -729,8 +1147,58 @@ def run_native(args, world, rank, local, dist):
     return 0
 
 
+def run_profile(args):
+    """A small case for ncu: no timing, no JSON line."""
+    import ctypes as C
+
+    import torch
+
+    from musoc_solver_b200 import build, native as N, problems as P
+    from musoc_solver_b200.solver import SevpSolver
+
+    build.build()
+    if args.profile == "solve":
+        p = P.global_grid(args.nx, args.ny, seed=11)
+        tiles = (16, 6) if args.tiles == "auto" else tuple(int(v) for v in args.tiles.split("x"))
+        s = SevpSolver(p, tile_m=tiles[0], tile_h=tiles[1], growth_limit=GROWTH,
+                       schwarz=args.precond == "schwarz")
+        b = torch.from_numpy(p.b).cuda()
+        if args.method == "cheb":
+            s.chebyshev_setup(b)
+            s.set_method(N.METHOD_CHEB)
+        _, rep = s.solve(b, precision=args.profile_precision, max_iter=args.profile_max_iter)
+        torch.cuda.synchronize()
+        print("ok", rep)
+        s.close()
+        return 0
+    from musoc_solver_b200.unet import lib as nnlib
+
+    H, W, cin, cout = (int(v) for v in args.conv.split(","))
+    L = nnlib()
+    g = torch.Generator(device="cuda").manual_seed(0)
+    x = torch.randn(H * W, cin, device="cuda", generator=g).to(torch.bfloat16)
+    wk = (torch.randn(9, cout, cin, device="cuda", generator=g) / 30).to(torch.bfloat16)
+    bias = torch.zeros(cout, device="cuda")
+    y = torch.zeros(H * W, cout, dtype=torch.bfloat16, device="cuda")
+    ptr = lambda t: C.c_void_p(t.data_ptr())
+    for _ in range(3):
+        st = L.sevp_nn_conv3x3_tma(ptr(x), cin, 0, cin, ptr(wk), ptr(bias), ptr(y), cout, 0, cout,
+                                   1, H, W, 1, None)
+        assert st == 0, st
+    code = C.c_int(-1)
+    assert L.sevp_nn_tc_status(C.byref(code)) == 0 and code.value == 0
+    torch.cuda.synchronize()
+    print("ok", args.conv)
+    return 0
+
+
 def main():
     args = parse()
+    # the CPU oracle's OpenMP runtime (tile PCG legs) uses every host core;
+    # serial legs (REP, BiCGSTAB, the single-thread baseline) say so
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+    if args.profile:
+        return run_profile(args)
     world, rank, local, dist = dist_setup(args)
     if args.impl == "reference":
         rc = run_reference(args, world, rank)

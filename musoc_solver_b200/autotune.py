@@ -12,7 +12,11 @@ choice depends on the grid, so it is measured: every candidate shape gets a
 solver (its influence data precomputed on the GPU) for each preconditioner,
 one untimed solve and `repeats` timed solves of the same right-hand side,
 from a zero guess or from the linear extrapolation of a given history, per
-inner tolerance; the fastest wins.
+inner tolerance; the fastest wins.  The outer iteration is a candidate too:
+PCG (two grid passes per iteration) or, for block-Jacobi tiles of at most 8
+rows, the one-launch Chebyshev iteration on the CG-Lanczos spectrum bounds
+(estimated once per candidate, untimed: they belong to the operator's set-up
+like the influence data).
 """
 from __future__ import annotations
 
@@ -22,13 +26,15 @@ from .solver import SevpSolver
 
 CANDIDATES = ((8, 8), (8, 16), (16, 4), (16, 6), (16, 8), (16, 12), (16, 16), (16, 24),
               (32, 8), (32, 16), (32, 32))
-# the Schwarz stage kernel holds at most this many tile rows
+# the Schwarz stage kernel and the Chebyshev kernel hold at most this many
+# tile rows
 SCHWARZ_MAX_ROWS = 8
+CHEB_MAX_ROWS = 8
 
 
 def autotune(problem, b, candidates=CANDIDATES, precision=1, tol=1e-12, repeats=2,
              growth_limit=1e10, device="cuda", schwarz=(False, True), inner_tols=(1e-5,),
-             history=None):
+             history=None, methods=(0,)):
     """Returns (best, table): best = dict(tile_m, tile_h, schwarz, inner_tol,
     ms, ...) of the fastest candidate, table = one such dict per candidate
     measured.  b is the right-hand side on the device (float64, shape
@@ -60,18 +66,25 @@ def autotune(problem, b, candidates=CANDIDATES, precision=1, tol=1e-12, repeats=
             torch.cuda.synchronize()
             setup_s = time.perf_counter() - t0
             x = torch.zeros_like(b)
-            for itol in (inner_tols if precision == 1 else inner_tols[:1]):
-                run(s, x, itol)
-                best_ms, res = None, None
-                for _ in range(repeats):
-                    res = run(s, x, itol)
-                    best_ms = res.ms if best_ms is None else min(best_ms, res.ms)
-                table.append(dict(tile_m=tm, tile_h=th, schwarz=bool(sw), inner_tol=itol,
-                                  ms=best_ms, iterations=res.iterations,
-                                  refinements=res.refinements, status=res.status,
-                                  rel_residual=res.rel_residual,
-                                  influence_mb=(s.influence_bytes() + s.schwarz_influence_bytes())
-                                  / 1e6, setup_s=setup_s))
+            for method in methods:
+                if method == N.METHOD_CHEB and (precision != 1 or sw or th > CHEB_MAX_ROWS):
+                    continue
+                if method == N.METHOD_CHEB:
+                    s.chebyshev_setup(b)
+                s.set_method(method)
+                for itol in (inner_tols if precision == 1 else inner_tols[:1]):
+                    run(s, x, itol)
+                    best_ms, res = None, None
+                    for _ in range(repeats):
+                        res = run(s, x, itol)
+                        best_ms = res.ms if best_ms is None else min(best_ms, res.ms)
+                    table.append(dict(tile_m=tm, tile_h=th, schwarz=bool(sw), inner_tol=itol,
+                                      method=int(method), ms=best_ms, iterations=res.iterations,
+                                      refinements=res.refinements, status=res.status,
+                                      rel_residual=res.rel_residual,
+                                      influence_mb=(s.influence_bytes()
+                                                    + s.schwarz_influence_bytes()) / 1e6,
+                                      setup_s=setup_s))
             s.close()
             del s
     ok = [r for r in table if r["status"] == 0]
