@@ -53,6 +53,13 @@ int sevp_nn_conv3x3_tma(const void *in, int in_ld, int in_off, int cin, const vo
 /* First error code (SEVP_TIMEOUT) a tensor-core kernel recorded since the
  * last call, 0 if none; clears it.  Synchronises the device. */
 int sevp_nn_tc_status(int *code);
+/* Test hook for the bounded waits of sevp_nn_conv3x3_tma: the number of
+ * polls its load and MMA waits make before giving up (0: give up at once;
+ * 0xFFFFFFFF: the default, about 4 M polls).  A wait that gives up records
+ * SEVP_TIMEOUT for sevp_nn_tc_status, skips the stores and returns after
+ * draining (with the default limit) the copies and MMAs already issued.
+ * Process-wide; synchronises the device. */
+int sevp_nn_tc_set_wait_limit(unsigned limit);
 
 /* Weight gradient of the 3x3 convolution, FP32, accumulated into dw
  * [9][cin][cout] (and db [cout] when given); dy is masked like the data

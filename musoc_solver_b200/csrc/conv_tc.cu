@@ -38,6 +38,11 @@ constexpr int kTcAhead = kTcStages - 2;  // steps of loads in flight ahead of th
 constexpr unsigned kSpinLimit = 1u << 22;
 
 __device__ int g_tc_error;  // first error recorded by a tensor-core kernel
+// Polls allowed to the producer and MMA-issuer waits of k_conv3x3_tma
+// (sevp_nn_tc_set_wait_limit; the drains that follow a failure always use
+// kSpinLimit, so every copy and MMA in flight completes before the CTA
+// releases its shared memory and TMEM).
+__device__ unsigned g_tc_wait_limit = kSpinLimit;
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -67,8 +72,9 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, unsigned parity) {
   return ok != 0;
 }
 // Bounded wait for the completion of the phase with the given parity.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, unsigned parity) {
-  for (unsigned k = 0; k < kSpinLimit; ++k)
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, unsigned parity,
+                                          unsigned limit = kSpinLimit) {
+  for (unsigned k = 0; k < limit; ++k)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
@@ -343,11 +349,12 @@ __global__ void __launch_bounds__(kTcThreads)
 
   bool failed = false;
   int issued = 0;
+  const unsigned wait_limit = g_tc_wait_limit;
   if (warp == 0 && lane == 0) {  // producer
     for (int s = 0; s < T; ++s) {
       const int st = s % kTmStages;
       if (s >= kTmStages &&
-          !mbar_wait(smem_u32(&empty[st]), (unsigned)((s / kTmStages) - 1) & 1u)) {
+          !mbar_wait(smem_u32(&empty[st]), (unsigned)((s / kTmStages) - 1) & 1u, wait_limit)) {
         failed = true;
         break;
       }
@@ -363,7 +370,7 @@ __global__ void __launch_bounds__(kTcThreads)
     const uint32_t idesc = instr_desc_bf16(kTcM, cout);
     for (int s = 0; s < T; ++s) {
       const int st = s % kTmStages;
-      if (!mbar_wait(smem_u32(&full[st]), (unsigned)(s / kTmStages) & 1u)) {
+      if (!mbar_wait(smem_u32(&full[st]), (unsigned)(s / kTmStages) & 1u, wait_limit)) {
         failed = true;
         break;
       }
@@ -375,7 +382,9 @@ __global__ void __launch_bounds__(kTcThreads)
                (s > 0 || k16 > 0) ? 1u : 0u);
       tc_commit(smem_u32(&empty[st]));
     }
-    if (!failed) tc_commit(smem_u32(&done));  // arrives once every MMA has completed
+    // arrives once every MMA issued so far has completed (also after a
+    // failed wait, so that none is left running when TMEM is freed)
+    tc_commit(smem_u32(&done));
   }
   __syncwarp();
   if (!mbar_wait(smem_u32(&done), 0u)) failed = true;
@@ -552,6 +561,13 @@ int sevp_nn_conv3x3_tma(const void *in, int in_ld, int in_off, int cin, const vo
                                relu, stream, enc);
   return launch_conv_tma<64>(in, in_ld, in_off, cin, wk, bias, out, out_ld, out_off, cout, B, H, W,
                              relu, stream, enc);
+}
+
+int sevp_nn_tc_set_wait_limit(unsigned limit) {
+  const unsigned v = limit == 0xFFFFFFFFu ? kSpinLimit : limit;
+  SEVP_CUDA_TRY(cudaMemcpyToSymbol(g_tc_wait_limit, &v, sizeof(unsigned)));
+  SEVP_CUDA_TRY(cudaDeviceSynchronize());
+  return SEVP_OK;
 }
 
 // First error a tensor-core kernel recorded since the last call (0 if none);

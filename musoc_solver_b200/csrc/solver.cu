@@ -1742,6 +1742,18 @@ __global__ void k_state_init(SolveState *st, double tol2, int max_iter, double *
   *st = s;
 }
 
+// State for a residual replacement that keeps the search direction: as
+// k_state_init, but r.z of the last iteration stays for the next beta.
+__global__ void k_state_keep(SolveState *st, double tol2, int max_iter) {
+  SolveState s{};
+  s.tol2 = tol2;
+  s.max_iter = max_iter;
+  s.status = SEVP_OK;
+  s.rz = st->rz;
+  s.keep_dir = 1;
+  *st = s;
+}
+
 // Starts an FP64 PCG run from the residual pass's norms: the recursive
 // (row-scaled) residual must fall by the factor the outer test still needs,
 // target / ||b - A x||^2 with target = tol^2 ||b||^2 (relative test) or
@@ -1977,8 +1989,17 @@ static int solve_mixed(sevp_ctx *ctx, const double *b, double *x, const sevp_sol
   double *xa = x, *xb = ctx->x64s;  // ping-pong: the residual kernel reads xa, writes xb
   bool have_d = false;
   const int method = o->method;
+  // PCG with reliable updates: after the first inner solve, every FP64
+  // residual replaces the FP32 recursive residual, the correction is folded
+  // into x, and CG goes on along its previous search direction (unless the
+  // caller asks for restarts)
+  const bool keep = method == SEVP_METHOD_PCG && !o->restart_inner;
+  bool have_dir = false;
   for (int refine = 0; refine < 64; ++refine) {
-    k_state_init<<<1, 1, 0, ctx->stream>>>(ctx->st, inner2, std::max(o->max_iter - total, 0));
+    if (keep && have_dir)
+      k_state_keep<<<1, 1, 0, ctx->stream>>>(ctx->st, inner2, std::max(o->max_iter - total, 0));
+    else
+      k_state_init<<<1, 1, 0, ctx->stream>>>(ctx->st, inner2, std::max(o->max_iter - total, 0));
     ctx->launches++;
     int s;
     if (have_d)
@@ -2015,6 +2036,12 @@ static int solve_mixed(sevp_ctx *ctx, const double *b, double *x, const sevp_sol
       if (s) return s;
       s = pcg_loop<float>(ctx, ctx->d32, ctx->r32, ctx->z32, ctx->p32[0], ctx->p32[1], ctx->q32,
                           std::max(1, o->check_every), &it);
+      // iteration k writes its search direction into p32[(k + 1) & 1]; the
+      // next loop starts from p32[0]
+      if (!s && keep && (it & 1))
+        SEVP_CUDA_TRY(cudaMemcpyAsync(ctx->p32[0], ctx->p32[1], ctx->n * sizeof(float),
+                                      cudaMemcpyDeviceToDevice, ctx->stream));
+      have_dir = have_dir || it > 0;
     } else {
       s = cheb_inner(ctx, std::max(1, o->check_every), &it);
     }

@@ -23,6 +23,9 @@ struct SolveState {
   // Chebyshev scalars of the fused iteration (sevp_set_chebyshev_bounds)
   double cheb_theta, cheb_delta, cheb_sigma, cheb_rho;
   int iter, max_iter, done, status;
+  // 1: the next tile pass continues the previous search direction after a
+  // residual replacement (beta = new r.z / old r.z instead of a restart)
+  int keep_dir;
   unsigned ticket[4];
   // optional record of the PCG coefficients: alpha_j at hist[2 (j-1)],
   // beta_j at hist[2 (j-1) + 1] for iterations j = 1..hist_cap
@@ -138,23 +141,25 @@ struct TileFin {
   SolveState *st;
   __device__ void operator()(double (&s)[2]) {
     double rz = s[0], rr = s[1];
-    int first = (st->beta == 0.0 && st->iter == 0);
+    int first = (st->beta == 0.0 && st->iter == 0 && !st->keep_dir);
+    st->keep_dir = 0;
     st->rr = rr;
     if (!isfinite(rz) || !isfinite(rr)) {
       st->status = SEVP_NONFINITE;
       st->done = 1;
       return;
     }
+    // a finished run keeps the previous r.z: a continuation after a
+    // residual replacement takes beta = (new r.z) / (that r.z), the step
+    // this run would have taken next
     if (rr <= st->tol2 * st->bb) {
       st->done = 1;
       st->status = SEVP_OK;
-      st->rz = rz;
       return;
     }
     if (st->iter >= st->max_iter) {
       st->done = 1;
       st->status = SEVP_MAXITER;
-      st->rz = rz;
       return;
     }
     if (rz == 0.0) {

@@ -49,7 +49,8 @@ class Tiling(C.Structure):
 class SolveOpts(C.Structure):
     _fields_ = [("precision", C.c_int), ("tol", C.c_double), ("max_iter", C.c_int),
                 ("inner_tol", C.c_double), ("use_guess", C.c_int), ("check_every", C.c_int),
-                ("precond_fp32", C.c_int), ("tol_abs", C.c_int), ("method", C.c_int)]
+                ("precond_fp32", C.c_int), ("tol_abs", C.c_int), ("method", C.c_int),
+                ("restart_inner", C.c_int)]
 
 
 class FsOptions(C.Structure):

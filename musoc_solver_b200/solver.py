@@ -111,6 +111,8 @@ class SevpSolver:
 
         self.precond_fp32 = bool(precond_fp32)
         self.method = N.METHOD_PCG
+        # mixed precision: True restarts CG at every FP64 residual
+        self.restart_inner = False
 
         self.torch = torch
         self.p = problem
@@ -182,15 +184,17 @@ class SevpSolver:
                 "couple": (ms[3], n[3])}
 
     def opts(self, precision=0, tol=1e-12, max_iter=5000, inner_tol=1e-5, use_guess=False,
-             check_every=4, precond_fp32=None, tol_abs=False, method=None):
+             check_every=4, precond_fp32=None, tol_abs=False, method=None, restart_inner=None):
         if precond_fp32 is None:
             precond_fp32 = self.precond_fp32
         if method is None:
             # the Chebyshev iteration is a mixed-precision method
             method = self.method if int(precision) == 1 else N.METHOD_PCG
+        if restart_inner is None:
+            restart_inner = self.restart_inner
         return N.SolveOpts(int(precision), float(tol), int(max_iter), float(inner_tol),
                            int(use_guess), int(check_every), int(precond_fp32), int(bool(tol_abs)),
-                           int(method))
+                           int(method), int(bool(restart_inner)))
 
     def set_schwarz(self, shift: int = -1):
         """Overlapping Schwarz preconditioner: a second tiling rolled west by

@@ -50,6 +50,7 @@ _SIGS = {
                              C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                              C.c_int, C.c_void_p], C.c_int),
     "sevp_nn_tc_status": ([C.c_void_p], C.c_int),
+    "sevp_nn_tc_set_wait_limit": ([C.c_uint], C.c_int),
     "sevp_nn_conv3x3_wgrad": ([C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int,
                                C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
                                C.c_int, C.c_int, C.c_int, C.c_void_p], C.c_int),

@@ -155,6 +155,36 @@ def rep(al, ab, ac, ar, at, rinv, rinv1, f, x, ie):
     return _rep_common(lib().or_rep, al, ab, ac, ar, at, rinv, rinv1, f, x, ie)
 
 
+def _strip_common(fn, al, ab, ac, ar, at, rinv, rinv1, f, x, ie, m2):
+    """REPBIR-style call on the first m2 columns: coefficients keep the full
+    leading dimension I2, F and RINV have m2 columns, X and H have m2 + 2."""
+    j2, i2 = ac.shape
+    nb = len(ie)
+    i0 = x.shape[1]
+    m0 = m2 + 2
+    x = _c(x, np.float64).copy()
+    dum0 = np.zeros((max(nb - 1, 1), m2))
+    dum1 = np.zeros(m2)
+    dum2 = np.zeros(m2)
+    h = np.zeros((x.shape[0], m0))
+    st = fn(*[_c(a, np.float32) for a in (al, ab, ac, ar, at)], _c(rinv, np.float64),
+            _c(rinv1, np.float64), dum0, dum1, dum2, _c(f, np.float32), h, x, _c(ie, np.int32),
+            i0, i2, m0, m2, nb)
+    return x, st
+
+
+def repbir(al, ab, ac, ar, at, rinv, rinv1, f, x, ie, m2):
+    """REPBIR (M/sevp.f90:218-328) on the first m2 columns; x is (J0, m2+2)
+    or wider (leading dimension I0 = x.shape[1])."""
+    return _strip_common(lib().or_repbir, al, ab, ac, ar, at, rinv, rinv1, f, x, ie, m2)
+
+
+def repbir_period(al, ab, ac, ar, at, rinv, rinv1, f, x, ie):
+    """REPBIR_PERIOD (M/sevp.f90:109-217), defined for M0 == I0 (full width)."""
+    j2, i2 = ac.shape
+    return _strip_common(lib().or_repbir_period, al, ab, ac, ar, at, rinv, rinv1, f, x, ie, i2)
+
+
 def matinv(b, pivot=False):
     b = np.array(b, dtype=np.float64, order="C")
     # the C routine is column-major: pass the transpose buffer and transpose back

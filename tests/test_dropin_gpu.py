@@ -300,3 +300,42 @@ def test_dropin_bad_args(L):
     x = np.zeros((4, 5))
     L.p_inprod_(_p(x), _p(x), None, _i(3), _i(2))
     assert L.sevp_last_status() == 5
+
+
+def test_repbir_period_and_repbir_bit_exact(L, oracle):
+    """REPBIR_PERIOD (full width, M/sevp.f90:109-217) and REPBIR on a strip
+    of M2 columns (M/sevp.f90:218-328) equal the oracle bit for bit."""
+    p = _shifted_idealised(120, 60)
+    c = _coeffs(p)
+    j2, i2 = p.ac.shape
+    ie, ok = oracle.block_partition(j2, 10)
+    nb = len(ie)
+    rng = np.random.default_rng(6)
+    # full width, periodic
+    rinv, rinv1, st = oracle.pre1(*c, ie)
+    f = rng.standard_normal((j2, i2)).astype(np.float32)
+    x = np.zeros((j2 + 2, i2 + 2))
+    x[0] = rng.standard_normal(i2 + 2)
+    xg = x.copy()
+    d0, d1, d2 = np.zeros((nb - 1, i2)), np.zeros(i2), np.zeros(i2)
+    hh = np.zeros((j2 + 2, i2 + 2))
+    L.repbir_period_(*[_p(a) for a in c], _p(rinv), _p(rinv1), _p(d0), _p(d1), _p(d2), _p(f),
+                     _p(hh), _p(xg), _p(ie), _i(i2 + 2), _i(i2), _i(i2 + 2), _i(i2), _i(nb))
+    assert L.sevp_last_status() == 0
+    xo, st = oracle.repbir_period(*c, rinv, rinv1, f, x, ie)
+    assert st == 0 and np.array_equal(xg, xo)
+    # strip of m2 columns with Dirichlet side columns
+    m2 = 40
+    rinv, rinv1, st = oracle.pre(*c, ie, m2=m2)
+    f = rng.standard_normal((j2, m2)).astype(np.float32)
+    x = np.zeros((j2 + 2, m2 + 2))
+    x[:, 0] = rng.standard_normal(j2 + 2)
+    x[:, -1] = rng.standard_normal(j2 + 2)
+    xg = x.copy()
+    d0, d1, d2 = np.zeros((nb - 1, m2)), np.zeros(m2), np.zeros(m2)
+    hh = np.zeros((j2 + 2, m2 + 2))
+    L.repbir_(*[_p(a) for a in c], _p(rinv), _p(rinv1), _p(d0), _p(d1), _p(d2), _p(f), _p(hh),
+              _p(xg), _p(ie), _i(m2 + 2), _i(i2), _i(m2 + 2), _i(m2), _i(nb))
+    assert L.sevp_last_status() == 0
+    xo, _ = oracle.repbir(*c, rinv, rinv1, f, x, ie, m2)
+    assert np.array_equal(xg, xo)

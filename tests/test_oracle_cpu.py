@@ -295,3 +295,45 @@ def test_tile_chebyshev_matches_scipy(oracle, grid):
     # Chebyshev with exact bounds takes no more than about the CG bound
     _, it_cg, _ = pc.pcg(p.b, tol=1e-12)
     assert it <= 3 * it_cg + 10, (it, it_cg)
+
+
+def test_repbir_period_equals_rep1_full_width(oracle):
+    """REPBIR_PERIOD (M/sevp.f90:109-217) at full width (M0 = I0, M2 = I2)
+    marches the same equations with the same periodic ghost refresh as REP1
+    (M/sevp.f90:11-107): equal results bit for bit."""
+    p = P.idealised(120, 60)
+    p.ac[:] += np.float32(0.01)
+    c = p.coeffs()
+    ie, ok = oracle.block_partition(60, 10)
+    rinv, rinv1, st = oracle.pre1(*c, ie)
+    assert st == 0
+    rng = np.random.default_rng(4)
+    f = rng.standard_normal((60, 120)).astype(np.float32)
+    x = np.zeros((62, 122))
+    x[0] = rng.standard_normal(122)
+    x1 = oracle.rep1(*c, rinv, rinv1, f, x, ie)
+    xp, st = oracle.repbir_period(*c, rinv, rinv1, f, x, ie)
+    assert st == 0
+    assert np.array_equal(x1, xp)
+
+
+def test_repbir_strip_satisfies_its_equations(oracle):
+    """REPBIR (M/sevp.f90:218-328) on a strip of M2 columns with Dirichlet
+    side columns: the solution satisfies the strip's equations."""
+    p = P.idealised(120, 60)
+    p.ac[:] += np.float32(0.01)
+    c = p.coeffs()
+    m2 = 40
+    ie, ok = oracle.block_partition(60, 10)
+    rinv, rinv1, st = oracle.pre(*c, ie, m2=m2)
+    assert st == 0
+    rng = np.random.default_rng(5)
+    f = rng.standard_normal((60, m2)).astype(np.float32)
+    x = np.zeros((62, m2 + 2))
+    x[:, 0] = rng.standard_normal(62)
+    x[:, -1] = rng.standard_normal(62)
+    xs, _ = oracle.repbir(*c, rinv, rinv1, f, x, ie, m2)
+    al, ab, ac, ar, at = (a[:, :m2].astype(np.float64) for a in c)
+    lhs = (ab * xs[:-2, 1:-1] + al * xs[1:-1, :-2] + ac * xs[1:-1, 1:-1] + ar * xs[1:-1, 2:]
+           + at * xs[2:, 1:-1])
+    assert np.abs(lhs - f).max() <= 1e-8 * np.abs(f).max()

@@ -276,3 +276,45 @@ def test_pool_upsample_exact(torch_cuda, Cc):
     ur = F.interpolate(pooled.double().cpu().reshape(1, H // 2, W // 2, Cc).permute(0, 3, 1, 2),
                        scale_factor=2, mode="nearest").permute(0, 2, 3, 1).reshape(-1, Cc)
     assert torch.equal(up.double().cpu(), ur)
+
+
+def test_tma_conv_wait_timeout_is_reported_and_recovers(torch_cuda):
+    """The bounded mbarrier waits of the TMA convolution: with the wait limit
+    set to zero polls every tile gives up at its first wait, records
+    SEVP_TIMEOUT (read by sevp_nn_tc_status), skips its stores and returns
+    after draining the copies it issued; with the default limit restored the
+    same call computes the convolution again and reports no error."""
+    import ctypes as C
+
+    import torch
+
+    from musoc_solver_b200.unet import lib as nnlib
+
+    L = nnlib()
+    H, W, cin, cout = 64, 128, 64, 32
+    g = torch.Generator(device="cuda").manual_seed(1)
+    x = torch.randn(H * W, cin, device="cuda", generator=g).to(torch.bfloat16)
+    wk = (torch.randn(9, cout, cin, device="cuda", generator=g) / 30).to(torch.bfloat16)
+    bias = torch.zeros(cout, device="cuda")
+    ptr = lambda t: C.c_void_p(t.data_ptr())
+    code = C.c_int(-1)
+    assert L.sevp_nn_tc_status(C.byref(code)) == 0
+    try:
+        assert L.sevp_nn_tc_set_wait_limit(0) == 0
+        y = torch.full((H * W, cout), 7.0, dtype=torch.bfloat16, device="cuda")
+        assert L.sevp_nn_conv3x3_tma(ptr(x), cin, 0, cin, ptr(wk), ptr(bias), ptr(y), cout, 0,
+                                     cout, 1, H, W, 1, None) == 0
+        assert L.sevp_nn_tc_status(C.byref(code)) == 0
+        assert code.value == 4  # SEVP_TIMEOUT
+        assert bool((y == 7.0).all())  # no tile stored a result
+    finally:
+        assert L.sevp_nn_tc_set_wait_limit(0xFFFFFFFF) == 0
+    y = torch.zeros((H * W, cout), dtype=torch.bfloat16, device="cuda")
+    assert L.sevp_nn_conv3x3_tma(ptr(x), cin, 0, cin, ptr(wk), ptr(bias), ptr(y), cout, 0, cout, 1,
+                                 H, W, 1, None) == 0
+    assert L.sevp_nn_tc_status(C.byref(code)) == 0 and code.value == 0
+    y2 = torch.zeros_like(y)
+    assert L.sevp_nn_conv3x3_tc(ptr(x), cin, 0, cin, ptr(wk), ptr(bias), ptr(y2), cout, 0, cout, 1,
+                                H, W, 1, None) == 0
+    torch.cuda.synchronize()
+    assert torch.equal(y, y2)
