@@ -245,6 +245,22 @@ int sevp_set_residual_operator(sevp_ctx *ctx, const float *al, const float *ab, 
  * once per context on a private stream and replayed on the context stream.
  * Not part of the reference interface. */
 int sevp_set_graphs(sevp_ctx *ctx, int enable);
+/* Kernel of the PCG's stencil pass (p = z + beta p_old, q = A p, p.q):
+ * SEVP_PASS_A_TILES (default) stages 64 x 32 tiles and their halos in shared
+ * memory with tensor copies where the grid allows it (nx a multiple of 4,
+ * 16-byte aligned buffers; other grids fall back);
+ * SEVP_PASS_A_COLUMNS walks columns with warp shuffles.  Both give the same
+ * p and q bit for bit.  Not part of the reference interface. */
+#define SEVP_PASS_A_TILES 0
+#define SEVP_PASS_A_COLUMNS 1
+int sevp_set_pass_a_kernel(sevp_ctx *ctx, int kind);
+/* One stencil pass on caller device buffers with the context's operator and
+ * pass A kernel: p = z + beta p_old (z alone when beta == 0), q = A p, and
+ * p.q through pq_out.  Test hook; not part of the reference interface. */
+int sevp_pass_a_f32(sevp_ctx *ctx, const float *z, const float *pold, double beta, float *pnew,
+                    float *q, double *pq_out);
+int sevp_pass_a_f64(sevp_ctx *ctx, const double *z, const double *pold, double beta,
+                    double *pnew, double *q, double *pq_out);
 
 int sevp_set_full_coefficients(sevp_ctx *ctx, int force);
 /* Device bytes held by the tile influence data (block-Jacobi tiling). */

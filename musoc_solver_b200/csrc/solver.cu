@@ -123,11 +123,7 @@ __global__ void __launch_bounds__(kStencilThreads, SEVP_STENCIL_MINB)
           cbu = (u == 0) ? at_prev : cn[u - 1];          // AB = AT of the south point
         }
         if (out) {
-          T av = T(cbu) * vb;
-          av += T(cwu) * vw;
-          av += T(ccn[u]) * vc;
-          av += T(ce[u]) * ve;
-          av += T(cn[u]) * va[u];
+          const T av = stencil5(cbu, vb, cwu, vw, ccn[u], vc, ce[u], ve, cn[u], va[u]);
           op.emit((size_t)j * nx + i, j, vc, av, acc);
         }
         vb = vc;
@@ -186,27 +182,14 @@ struct OpPassA {
   }
   __device__ V value(size_t idx) const {
     V zv = z[idx];
-    return first ? zv : zv + beta * pold[idx];
+    return first ? zv : fma_rn(beta, pold[idx], zv);
   }
   __device__ void emit(size_t idx, int, V vc, V av, double (&acc)[NV]) const {
     pnew[idx] = vc;
     q[idx] = av;
     acc[0] += (double)vc * (double)av;
   }
-  __device__ void operator()(double (&s)[NV]) {
-    st->pq = s[0];
-    st->iter += 1;
-    if (!isfinite(s[0])) {
-      st->status = SEVP_NONFINITE;
-      st->done = 1;
-    } else if (s[0] == 0.0) {
-      st->status = SEVP_BREAKDOWN;
-      st->done = 1;
-    } else {
-      st->alpha = st->rz / s[0];
-      if (st->hist && st->iter <= st->hist_cap) st->hist[2 * (st->iter - 1)] = st->alpha;
-    }
-  }
+  __device__ void operator()(double (&s)[NV]) { PassAFin{st}(s); }
 };
 
 // FP64 residual: x_out = x + d (d optional, FP32 correction); ru = b - A x_out
@@ -991,6 +974,7 @@ struct sevp_ctx {
   // and influence-data choice it was captured with
   int use_graphs = 1;
   int stencil_rpw = 0;  // rows per CTA of the stencil kernels (0: not chosen yet)
+  int pass_a_kernel = SEVP_PASS_A_TILES;
   cudaStream_t cap_stream = nullptr;
   cudaGraphExec_t inner_graph = nullptr;
   int inner_graph_ce = 0;
@@ -1369,6 +1353,13 @@ extern "C" int sevp_set_graphs(sevp_ctx *ctx, int enable) {
   if (!ctx) return SEVP_BAD_ARG;
   ctx->use_graphs = enable ? 1 : 0;
   if (!enable) drop_inner_graph(ctx);
+  return SEVP_OK;
+}
+
+extern "C" int sevp_set_pass_a_kernel(sevp_ctx *ctx, int kind) {
+  if (!ctx || (kind != SEVP_PASS_A_TILES && kind != SEVP_PASS_A_COLUMNS)) return SEVP_BAD_ARG;
+  ctx->pass_a_kernel = kind;
+  drop_inner_graph(ctx);
   return SEVP_OK;
 }
 
@@ -1833,6 +1824,33 @@ static int graph_loop(sevp_ctx *ctx, bool graph, const void *const (&key)[5], in
   return SEVP_OK;
 }
 
+// PCG pass A: the tile kernel of stencil_tma.cu where the context chose it
+// and the grid allows it, else the column-walking k_stencil.
+template <typename V>
+static int launch_pass_a(sevp_ctx *ctx, const OpPassA<V> &op) {
+  if (ctx->pass_a_kernel == SEVP_PASS_A_TILES) {
+    PassALaunch<V> L{GridDims{ctx->nx, ctx->ny, ctx->periodic},
+                     ctx->c,
+                     ctx->sym,
+                     op.z,
+                     op.pold,
+                     op.pnew,
+                     op.q,
+                     ctx->st,
+                     ctx->partials,
+                     ctx->partials_n,
+                     ctx->tickets + 3,
+                     ctx->stream};
+    if (pass_a_tma_eligible(L)) {
+      ProfScope ps(ctx, 1);
+      const int s = pass_a_tma_launch(L);
+      ctx->launches++;
+      return s;
+    }
+  }
+  return launch_stencil(ctx, op, 3);
+}
+
 // Runs PCG iterations on vectors of type V until the device state says done.
 // x, r hold the iterate and residual; the first z = M^{-1} r must already be
 // in place (with rz, beta = 0 set).  Returns iterations done.
@@ -1843,7 +1861,7 @@ static int pcg_loop(sevp_ctx *ctx, V *x, V *r, V *z, V *p0, V *p1, V *q, int che
   auto interval = [&](int &cur) -> int {  // check_every iterations of passes A and B
     for (int k = 0; k < check_every; ++k) {
       OpPassA<V> op{z, pp[cur], pp[cur ^ 1], q, ctx->st};
-      int s = launch_stencil(ctx, op, 3);
+      int s = launch_pass_a(ctx, op);
       if (s) return s;
       s = precondition_pass<V, true, true>(ctx, x, pp[cur ^ 1], r, q, z);
       if (s) return s;
@@ -2665,4 +2683,38 @@ extern "C" int sevp_cheb_step(sevp_ctx *ctx, int iter, double theta, double delt
   if (s) return s;
   if (rr_out) *rr_out = ctx->h_st->rr;
   return ctx->h_st->status;
+}
+
+// One pass A on caller buffers (test hook): p = z + beta p_old (z alone for
+// beta = 0), q = A p; returns p.q through pq_out.
+__global__ void k_state_pass_a(SolveState *st, double beta) {
+  SolveState s{};
+  s.beta = beta;
+  s.rz = 1.0;
+  s.bb = 1.0;
+  s.max_iter = 1 << 30;
+  s.status = SEVP_OK;
+  *st = s;
+}
+
+template <typename V>
+static int pass_a_step(sevp_ctx *ctx, const V *z, const V *pold, double beta, V *pnew, V *q,
+                       double *pq_out) {
+  if (!ctx || !ctx->have_op || !z || !pold || !pnew || !q) return SEVP_BAD_ARG;
+  k_state_pass_a<<<1, 1, 0, ctx->stream>>>(ctx->st, beta);
+  OpPassA<V> op{z, pold, pnew, q, ctx->st};
+  int s = launch_pass_a(ctx, op);
+  if (!s) s = read_state(ctx);
+  if (s) return s;
+  if (pq_out) *pq_out = ctx->h_st->pq;
+  return ctx->h_st->status;
+}
+
+extern "C" int sevp_pass_a_f32(sevp_ctx *ctx, const float *z, const float *pold, double beta,
+                               float *pnew, float *q, double *pq_out) {
+  return pass_a_step(ctx, z, pold, beta, pnew, q, pq_out);
+}
+extern "C" int sevp_pass_a_f64(sevp_ctx *ctx, const double *z, const double *pold, double beta,
+                               double *pnew, double *q, double *pq_out) {
+  return pass_a_step(ctx, z, pold, beta, pnew, q, pq_out);
 }

@@ -41,6 +41,27 @@ struct GridDims {
   int nx, ny, periodic;
 };
 
+// ------------------------------------------------ five-point stencil row
+// Explicitly rounded multiply and fused multiply-add: the compiler may not
+// pick which product of a sum it fuses, so every kernel that applies the
+// operator forms the same value bit for bit.
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
+
+// A x at one point: south, west, centre, east, north, accumulated in that
+// order in the vector type T.
+template <typename T>
+__device__ __forceinline__ T stencil5(float cb, T vb, float cw, T vw, float cc, T vc, float ce,
+                                      T ve, float cn, T va) {
+  T av = mul_rn(T(cb), vb);
+  av = fma_rn(T(cw), vw, av);
+  av = fma_rn(T(cc), vc, av);
+  av = fma_rn(T(ce), ve, av);
+  return fma_rn(T(cn), va, av);
+}
+
 // ------------------------------------------------- reductions / finisher
 // Writes this CTA's NV partial sums, and lets the last CTA to arrive sum all
 // partials in block order and call fin(sums) once.
@@ -482,5 +503,47 @@ struct ChebLaunch {
 };
 template <typename V>
 int cheb_launch(const ChebLaunch<V> &L);
+
+// ------------------------------------------------------- PCG pass A
+// Finisher of pass A: p.q is complete; alpha = r.z / p.q.
+struct PassAFin {
+  SolveState *st;
+  __device__ void operator()(double (&s)[1]) {
+    st->pq = s[0];
+    st->iter += 1;
+    if (!isfinite(s[0])) {
+      st->status = SEVP_NONFINITE;
+      st->done = 1;
+    } else if (s[0] == 0.0) {
+      st->status = SEVP_BREAKDOWN;
+      st->done = 1;
+    } else {
+      st->alpha = st->rz / s[0];
+      if (st->hist && st->iter <= st->hist_cap) st->hist[2 * (st->iter - 1)] = st->alpha;
+    }
+  }
+};
+
+// Pass A on TMA-staged tiles (stencil_tma.cu): p = z + beta p_old (z alone
+// when beta = 0), q = A p, alpha = r.z / p.q.
+template <typename V>
+struct PassALaunch {
+  GridDims g;
+  Coeffs c;
+  int sym;
+  const V *z, *pold;
+  V *pnew, *q;
+  SolveState *st;
+  double *partials;
+  size_t partials_n;  // doubles in partials
+  unsigned *ticket;
+  cudaStream_t stream;
+};
+// Whether the grid and the buffers meet the tensor copy's alignment rules;
+// the launch returns SEVP_BAD_ARG (nothing launched) when they do not.
+template <typename V>
+bool pass_a_tma_eligible(const PassALaunch<V> &L);
+template <typename V>
+int pass_a_tma_launch(const PassALaunch<V> &L);
 
 }  // namespace sevp

@@ -27,6 +27,9 @@ SEVP_NONSYMMETRIC = 8
 METHOD_PCG = 0   # PCG, two grid passes per iteration
 METHOD_CHEB = 1  # one-launch Chebyshev iteration (mixed precision, needs bounds)
 
+PASS_A_TILES = 0    # stencil pass on tensor-copied shared-memory tiles
+PASS_A_COLUMNS = 1  # stencil pass walking columns with warp shuffles
+
 GUESS_ZERO, GUESS_PREVIOUS, GUESS_LINEAR, GUESS_LEARNED = 0, 1, 2, 3
 
 
@@ -109,6 +112,9 @@ _SIGS = {
     "sevp_operator_symmetric": ([P], C.c_int),
     "sevp_set_full_coefficients": ([P, C.c_int], C.c_int),
     "sevp_set_graphs": ([P, C.c_int], C.c_int),
+    "sevp_set_pass_a_kernel": ([P, C.c_int], C.c_int),
+    "sevp_pass_a_f32": ([P, P, P, C.c_double, P, P, P], C.c_int),
+    "sevp_pass_a_f64": ([P, P, P, C.c_double, P, P, P], C.c_int),
     "sevp_set_schwarz": ([P, C.c_int], C.c_int),
     "sevp_schwarz_shift": ([P], C.c_int),
     "sevp_record_coefficients": ([P, C.c_int], C.c_int),

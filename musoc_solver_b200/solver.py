@@ -374,6 +374,21 @@ class SevpSolver:
         N.check(N.lib().sevp_apply(self.h, N.ptr(x), N.ptr(y)), "sevp_apply")
         return y
 
+    def set_pass_a_kernel(self, kind: int):
+        """Kernel of the PCG's stencil pass: N.PASS_A_TILES (tensor-copied
+        tiles, the default where the grid allows) or N.PASS_A_COLUMNS."""
+        N.check(N.lib().sevp_set_pass_a_kernel(self.h, int(kind)), "sevp_set_pass_a_kernel")
+
+    def pass_a(self, z, pold, beta: float):
+        """One stencil pass: (p, q, p.q) with p = z + beta p_old, q = A p."""
+        pnew = self.torch.empty_like(z)
+        q = self.torch.empty_like(z)
+        pq = C.c_double()
+        fn = N.lib().sevp_pass_a_f64 if z.dtype == self.torch.float64 else N.lib().sevp_pass_a_f32
+        N.check(fn(self.h, N.ptr(z), N.ptr(pold), float(beta), N.ptr(pnew), N.ptr(q),
+                   C.byref(pq)), "sevp_pass_a")
+        return pnew, q, pq.value
+
     def precondition(self, r):
         z = self.torch.empty_like(r)
         fn = N.lib().sevp_precondition if r.dtype == self.torch.float64 else N.lib().sevp_precondition_f32
