@@ -154,6 +154,40 @@ void sevp_pre_strips_(const float *al, const float *ab, const float *ac, const f
                       const float *at, double *rinv, double *rinv1, const int *ie, const int *i2,
                       const int *j2, const int *nb0, const int *nbir);
 
+/* ------------------------------------------------ PREP's preprocessing */
+
+/* Row-block boundaries IE(NB0) of the reference's SEVP blocks,
+ * P/prep_GLOBAL.f90:148-168: NN = ANINT(REAL(J2) / REAL(NB0)),
+ * IE(N) = MIN(1 + NN N, J1), then the validity test of :156-165 and
+ * IE(NB0) = J1.  Host code, no GPU.  Where the reference prints "IE(NB1),J1
+ * not properly defined" and stops, this returns SEVP_BAD_ARG with that text
+ * in sevp_last_error (ie is still filled).  nb0 >= 2; dimen 2 or 3. */
+int sevp_block_partition(int j2, int nb0, int dimen, int *ie);
+
+/* Five-point coefficients of the barotropic operator, PREP's assembly
+ * (P/prep_GLOBAL.f90:170-261) on the GPU, equal to the reference's REAL*4
+ * results bit for bit.  DEVICE arrays with the reference's shapes
+ * (column-major): ODX, ODY, OCS (J0), CSV, ODYV (J1), ODZ (K1) REAL*4;
+ * IU (I0, J0, K1) and IV (I0, J1, K1) INTEGER*2 layer masks (read for
+ * K = 2..K1; unused when dimen == 2 or k1 == 1, may then be NULL).
+ * dimen 2: the constant couplings of :170-181 (ODX(1), ODY(1), ODZ(1) only);
+ * dimen 3: the top layer all water plus the masked lower layers (:183-212).
+ * nbir == 1: closed side walls and the pressure pin AB(I2/2,1) = AB(I2/2,2)
+ * (:214-230).  gamma is the free-surface term (1/(0.5 DT^2 G) under FLAG_FS,
+ * :232-236, else 0).  idealised != 0 applies the reference's constant test
+ * stencil with Neumann north and south rows (:244-258), which the reference
+ * as shipped always applies.  Outputs AL, AR, AB, AT, AC (I2, J2). */
+int sevp_prep_assemble(int i2, int j2, int k1, int dimen, const float *odx, const float *ody,
+                       const float *csv, const float *ocs, const float *odyv, const float *odz,
+                       const int16_t *iu, const int16_t *iv, int nbir, float gamma, int idealised,
+                       float *al, float *ar, float *ab, float *at, float *ac, void *stream);
+/* The same on HOST arrays (copied to the GPU and back inside the call). */
+int sevp_prep_assemble_host(int i2, int j2, int k1, int dimen, const float *odx,
+                            const float *ody, const float *csv, const float *ocs,
+                            const float *odyv, const float *odz, const int16_t *iu,
+                            const int16_t *iv, int nbir, float gamma, int idealised, float *al,
+                            float *ar, float *ab, float *at, float *ac);
+
 /* ---------------------------------------------------- native device API */
 
 typedef struct sevp_ctx sevp_ctx;

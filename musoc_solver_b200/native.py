@@ -93,6 +93,11 @@ _SIGS = {
     "sevp_fs_last_report": ([P], C.c_int),
     "sevp_fs_release": ([], C.c_int),
     "sevp_row_symmetrize": ([P] * 5 + [C.c_int, C.c_int, C.c_int, P, P], C.c_int),
+    "sevp_block_partition": ([C.c_int, C.c_int, C.c_int, P], C.c_int),
+    "sevp_prep_assemble": ([C.c_int] * 4 + [P] * 8 + [C.c_int, C.c_float, C.c_int] + [P] * 6,
+                           C.c_int),
+    "sevp_prep_assemble_host": ([C.c_int] * 4 + [P] * 8 + [C.c_int, C.c_float, C.c_int] + [P] * 5,
+                                C.c_int),
     "sevp_create": ([C.POINTER(P), C.c_int, C.c_int, C.c_int, P], C.c_int),
     "sevp_destroy": ([P], C.c_int),
     "sevp_set_operator": ([P, P, P, P, P, P, C.POINTER(Tiling)], C.c_int),

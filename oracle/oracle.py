@@ -74,6 +74,8 @@ def lib():
         L.or_pre_strips.restype = C.c_int
         L.or_assemble.argtypes = ([C.c_int] * 3 + [f32p] * 6 + [i32p, i32p, C.c_int, C.c_float, C.c_int]
                                   + [f32p] * 5)
+        L.or_assemble_dim.argtypes = ([C.c_int] * 4 + [f32p] * 6
+                                      + [i32p, i32p, C.c_int, C.c_float, C.c_int] + [f32p] * 5)
         L.or_tile_setup.argtypes = c5 + [C.c_int] * 4 + [i32p, C.POINTER(C.c_int)]
         L.or_tile_setup.restype = C.c_void_p
         L.or_tile_free.argtypes = [C.c_void_p]
@@ -244,6 +246,17 @@ def assemble(i2, j2, k1, odx, ody, csv, ocs, odyv, odz, iu, iv, nbir, gamma, ide
     out = [np.zeros((j2, i2), np.float32) for _ in range(5)]
     lib().or_assemble(i2, j2, k1, *[_c(a, np.float32) for a in (odx, ody, csv, ocs, odyv, odz)],
                       _c(iu, np.int32), _c(iv, np.int32), nbir, gamma, int(idealised), *out)
+    al, ar, ab, at, ac = out
+    return al, ab, ac, ar, at
+
+
+def assemble_dim(i2, j2, k1, dimen, odx, ody, csv, ocs, odyv, odz, iu, iv, nbir, gamma, idealised):
+    """PREP's assembly with the DIMEN switch of P/prep_GLOBAL.f90:170-212;
+    iu, iv are int32 masks of shape (K, J0, I0)."""
+    out = [np.zeros((j2, i2), np.float32) for _ in range(5)]
+    lib().or_assemble_dim(i2, j2, k1, dimen,
+                          *[_c(a, np.float32) for a in (odx, ody, csv, ocs, odyv, odz)],
+                          _c(iu, np.int32), _c(iv, np.int32), nbir, gamma, int(idealised), *out)
     al, ar, ab, at, ac = out
     return al, ab, ac, ar, at
 

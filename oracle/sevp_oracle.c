@@ -17,7 +17,7 @@
  *   or_pre             P/prep_GLOBAL.f90:457-513   strip influence precompute
  *   or_matinv          P/prep_GLOBAL.f90:516-568   Gauss-Jordan inverse, no pivoting
  *   or_block_partition P/prep_GLOBAL.f90:148-168   block boundaries IE
- *   or_assemble        P/prep_GLOBAL.f90:170-261   5-point coefficients
+ *   or_assemble(_dim)  P/prep_GLOBAL.f90:170-261   5-point coefficients (2-D and 3-D)
  *   or_sqprod          M/sevp.f90:696-713   operator apply
  *   or_sqprod_t        M/sevp.f90:714-742   transpose apply
  *   or_inprod          M/sevp.f90:743-757   interior dot product
@@ -461,19 +461,31 @@ int or_block_partition(int J2, int NB0, int dimen, int *IE) {
 }
 
 /* ------------------------------------------------------------------------ */
-/* Coefficient assembly, P/prep_GLOBAL.f90:170-261 (3-D branch).            */
+/* Coefficient assembly, P/prep_GLOBAL.f90:170-261 (dimen 2: :170-181).     */
 /* Metric arrays are indexed 1..J0 (ODX, ODY, CSV, OCS, ODYV); ODZ 1..K1;   */
 /* IU, IV are (I0, J0, K0) integer masks.  idealised != 0 applies the        */
 /* constant test stencil and Neumann rows of :246-261.                        */
 /* ------------------------------------------------------------------------ */
-void or_assemble(int I2, int J2, int K1, const float *ODX, const float *ODY, const float *CSV,
-                 const float *OCS, const float *ODYV, const float *ODZ, const int *IU,
-                 const int *IV, int nbir, float gamma, int idealised, float *AL, float *AR,
-                 float *AB, float *AT, float *AC) {
+void or_assemble_dim(int I2, int J2, int K1, int dimen, const float *ODX, const float *ODY,
+                     const float *CSV, const float *OCS, const float *ODYV, const float *ODZ,
+                     const int *IU, const int *IV, int nbir, float gamma, int idealised, float *AL,
+                     float *AR, float *AB, float *AT, float *AC) {
   int I0 = I2 + 2, J0 = J2 + 2;
+  if (dimen == 2) {
+    /* :170-181 */
+    float dzx = ODX[0] * ODX[0] / ODZ[0];
+    float dzy = ODY[0] * ODY[0] / ODZ[0];
+    for (size_t k = 0; k < (size_t)I2 * J2; ++k) {
+      AL[k] = dzx;
+      AR[k] = dzx;
+      AB[k] = dzy;
+      AT[k] = dzy;
+    }
+    K1 = 0; /* no layer loop */
+  }
   /* top layer all water */
   float tmp = 1.f / ODZ[0];
-  for (int j = 1; j <= J2; ++j) {
+  for (int j = 1; j <= J2 && dimen == 3; ++j) {
     float dzx = ODX[j] * ODX[j] * tmp;
     float dzyb = CSV[j - 1] * OCS[j] * ODYV[j - 1] * ODY[j] * tmp;
     float dzyt = CSV[j] * OCS[j] * ODYV[j] * ODY[j] * tmp;
@@ -527,6 +539,15 @@ void or_assemble(int I2, int J2, int K1, const float *ODX, const float *ODY, con
       AB[IX(I2, i, 1)] = 0.f;
     }
   }
+}
+
+/* The 3-D branch (the one PREP takes for the global model). */
+void or_assemble(int I2, int J2, int K1, const float *ODX, const float *ODY, const float *CSV,
+                 const float *OCS, const float *ODYV, const float *ODZ, const int *IU,
+                 const int *IV, int nbir, float gamma, int idealised, float *AL, float *AR,
+                 float *AB, float *AT, float *AC) {
+  or_assemble_dim(I2, J2, K1, 3, ODX, ODY, CSV, OCS, ODYV, ODZ, IU, IV, nbir, gamma, idealised, AL,
+                  AR, AB, AT, AC);
 }
 
 /* ------------------------------------------------------------------------ */

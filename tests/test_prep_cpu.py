@@ -86,3 +86,29 @@ def test_unsymmetrisable_operator_refused(L):
     st, _, _ = _sym(L, planes, True)
     assert st == 8
     assert "AR(I,J) differs from AL(I+1,J)" in L.sevp_last_error().decode()
+
+
+def test_block_partition_matches_oracle(L, oracle):
+    """sevp_block_partition (host code in the library) against the oracle's
+    restatement of P/prep_GLOBAL.f90:148-168, valid and invalid partitions,
+    including quotients that round half away from zero."""
+    seen_bad = seen_ok = 0
+    for dimen in (2, 3):
+        for j2 in (1, 2, 3, 5, 7, 10, 15, 24, 25, 90, 92, 181, 2398, 2400):
+            for nb0 in (2, 3, 4, 5, 6, 8, 12, 15, 16, 50, 400):
+                ie = np.zeros(nb0, np.int32)
+                st = L.sevp_block_partition(j2, nb0, dimen, ie.ctypes.data_as(C.c_void_p))
+                ref, ok = oracle.block_partition(j2, nb0, dimen)
+                assert np.array_equal(ie, ref), (j2, nb0, dimen)
+                assert (st == 0) == ok, (j2, nb0, dimen, st)
+                if ok:
+                    seen_ok += 1
+                else:
+                    seen_bad += 1
+                    assert "not properly defined" in L.sevp_last_error().decode()
+    assert seen_ok > 20 and seen_bad > 20
+    # the reference's 182 x 92 grid with 15 blocks (I2 = 180, J2 = 90)
+    ie = np.zeros(15, np.int32)
+    assert L.sevp_block_partition(90, 15, 3, ie.ctypes.data_as(C.c_void_p)) == 0
+    assert ie.tolist() == [7, 13, 19, 25, 31, 37, 43, 49, 55, 61, 67, 73, 79, 85, 91]
+    assert L.sevp_block_partition(90, 1, 3, ie.ctypes.data_as(C.c_void_p)) == 5
