@@ -84,6 +84,9 @@ def parse():
                          "iteration, or 'auto' (measured)")
     ap.add_argument("--inner-tol", default="auto",
                     help="relative reduction of each FP32 inner solve, or 'auto' (measured)")
+    ap.add_argument("--influence-fp32", default="auto",
+                    help="growth limit of the per-group FP32 influence data of the inner "
+                         "iterations: a number, 'off', or 'auto' (measured)")
     ap.add_argument("--no-fs", action="store_true",
                     help="skip the barotropic correction loop arm (3600x2400, 20 layers)")
     ap.add_argument("--no-ensemble", action="store_true",
@@ -802,6 +805,36 @@ def run_native(args, world, rank, local, dist):
     solver.set_method(method)
     torch.cuda.synchronize()
 
+    # per-group FP32 influence data of the inner iterations (PCG tile passes):
+    # growth limit measured (untimed) on the same warm-start step, unless given
+    mix_limit, mix_table = 0.0, None
+    if args.influence_fp32 == "auto" and not args.precond_fp32 and method == N.METHOD_PCG:
+        mix_table, xw = {}, torch.zeros_like(eta[0])
+        for lim in (0.0, 1e3, 1e4, 1e5, 1e6):
+            solver.set_influence_fp32(lim)
+            ts, ok = [], True
+            for _ in range(3):
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                _, r = solver.solve_step(b_dev[T - 1], eta[T - 2], eta[T - 3], xw,
+                                         guess=N.GUESS_LINEAR, precision=1, inner_tol=itol)
+                torch.cuda.synchronize()
+                ts.append(time.perf_counter() - t0)
+                ok = ok and r.status == 0
+            if ok:
+                mix_table[f"{lim:g}" if lim else "off"] = round(min(ts[1:]) * 1e3, 3)
+                if min(ts[1:]) * 1e3 <= min(mix_table.values()):
+                    mix_limit = lim
+    elif args.influence_fp32 not in ("auto", "off"):
+        mix_limit = float(args.influence_fp32)
+    if dist is not None:
+        choice = [float(mix_limit)]
+        dist.broadcast_object_list(choice, src=0)
+        mix_limit = choice[0]
+    solver.set_influence_fp32(mix_limit)
+    mix_groups = solver.influence_fp32_groups()
+    torch.cuda.synchronize()
+
     eta += [torch.zeros_like(eta[0]) for _ in range(W + K)]
     guess_mode, guess_name = N.GUESS_LINEAR, "linear extrapolation 2*eta[n-1]-eta[n-2]"
     warm, train_info = None, None
@@ -968,7 +1001,9 @@ def run_native(args, world, rank, local, dist):
     cpl_ms, cpl_n = prof["couple"]
     ncoef = 3 if solver.symmetric else 5
     scale = 0.5 if args.precond_fp32 else 1.0
-    infl_a = int(solver.influence_bytes() * scale)
+    # influence bytes one block-Jacobi tile pass reads (per-group precision
+    # when it is on)
+    infl_a = int(solver.influence_bytes() * scale) if args.precond_fp32 else mix_groups[2]
     infl_b = int(solver.schwarz_influence_bytes() * scale)
     # pass B: x,p,r,q in; x,r,z out (without r.z and z with the Schwarz
     # preconditioner: z1 out); coefficient planes; influence data
@@ -1073,6 +1108,10 @@ def run_native(args, world, rank, local, dist):
             "marching_growth_limit": GROWTH,
             "coefficient_planes": 3 if solver.symmetric else 5,
             "influence_fp32_in_inner_solve": bool(args.precond_fp32),
+            "influence_fp32_growth_limit": mix_limit or None,
+            "influence_fp32_groups": [mix_groups[0], mix_groups[1]],
+            "influence_bytes_per_tile_pass": mix_groups[2],
+            "influence_fp32_autotune_ms": mix_table,
             "tol": 1e-12, "parallelism": f"replicas x{world}",
             "l2": "inputs larger than L2 (69 MB per FP64 field), no flush",
         },

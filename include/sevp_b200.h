@@ -299,6 +299,24 @@ int sevp_pass_a_f64(sevp_ctx *ctx, const double *z, const double *pold, double b
 int sevp_set_full_coefficients(sevp_ctx *ctx, int force);
 /* Device bytes held by the tile influence data (block-Jacobi tiling). */
 long long sevp_influence_bytes(const sevp_ctx *ctx);
+/* Influence-data precision chosen per warp group of tiles for the FP32
+ * inner iterations of mixed solves and sevp_precondition_f32 (not part of
+ * the reference interface).  growth_limit > 1: the groups whose every tile
+ * has a marching growth bound z^s <= growth_limit over its sub-blocks of s
+ * rows (z as in sevp_tiling.growth_limit) read their matrices as FP32, the
+ * others keep FP64; their mat-vecs then read half the bytes.  The inverse
+ * influence matrices are about as ill-conditioned as that growth, so the
+ * limit bounds the relative error FP32 storage brings into a tile's
+ * correction (about 6e-8 times the limit).  growth_limit <= 1 turns it off
+ * (the default).  A solve that sets sevp_solve_opts.precond_fp32 still
+ * reads every tile as FP32.  Kept across sevp_set_operator (the choice is
+ * rebuilt for the new operator). */
+int sevp_set_influence_fp32(sevp_ctx *ctx, double growth_limit);
+/* Warp groups of the block-Jacobi tiling reading FP32 influence data, all
+ * groups, and the influence bytes one preconditioner pass reads with that
+ * choice (sevp_influence_bytes when it is off).  Pointers may be NULL. */
+int sevp_influence_fp32_groups(const sevp_ctx *ctx, int *fp32_groups, int *groups,
+                               long long *bytes_per_pass);
 /* Overlapping Schwarz preconditioner (not part of the reference interface;
  * the reference's BIR method, M/fs_GLOBAL.f90:1902-1966, sweeps overlapping
  * strips with 50 % overlap as a stand-alone solver).  shift != 0 adds a

@@ -68,8 +68,42 @@ int sevp_nn_conv3x3_wgrad(const void *x, int x_ld, int x_off, int cin, const voi
                           int dy_off, int cout, const void *mask, int mask_ld, int mask_off,
                           float *dw, float *db, int B, int H, int W, void *stream);
 
+/* Weight gradient of the 3x3 convolution on the tcgen05 tensor cores (FP32
+ * accumulator in tensor memory), accumulated into dw [9][cin][cout]:
+ *   dw[tap][ci][co] += sum_p x[p + shift(tap)][x_off + ci] * g[p][co]
+ * with g the packed output gradient [B*H*W][cout] (ReLU mask already
+ * applied).  cin and cout multiples of 16 up to 256; x_ld, x_off multiples
+ * of 8; x and g 16-byte aligned.  The same sums as sevp_nn_conv3x3_wgrad up
+ * to the FP32 summation order. */
+int sevp_nn_conv3x3_wgrad_tc(const void *x, int x_ld, int x_off, int cin, const void *g, int cout,
+                             float *dw, int B, int H, int W, void *stream);
+/* The whole backward of one 3x3 convolution + ReLU on the tensor cores:
+ * packs dy masked by mask > 0 into scratch (B*H*W*cout BF16), then the
+ * weight gradient (sevp_nn_conv3x3_wgrad_tc, into dw), the bias gradient
+ * (into db when given) and, when dx is given, the data gradient
+ * (sevp_nn_conv3x3_tma with the mirrored weights wm, written to dx). */
+int sevp_nn_conv3x3_backward_tc(const void *x, int x_ld, int x_off, int cin, const void *dy,
+                                int dy_ld, int dy_off, int cout, const void *mask, int mask_ld,
+                                int mask_off, const void *wm, void *scratch, float *dw, float *db,
+                                void *dx, int dx_ld, int dx_off, int B, int H, int W,
+                                void *stream);
+
 /* wt[tap][co][ci] = w[tap][ci][co] (BF16). */
 int sevp_nn_weight_transpose(const void *w, void *wt, int cin, int cout, void *stream);
+/* wm[tap][ci][co] = w[8 - tap][ci][co] (BF16): the K-major weights of the
+ * data gradient as a forward convolution from cout to cin channels. */
+int sevp_nn_weight_mirror(const void *w, void *wm, int cin, int cout, void *stream);
+/* Data gradient of the 3x3 convolution on the tcgen05 tensor cores:
+ *   dx[p][dx_off + ci] = sum_{tap, co} dy'[p + shift(tap)][co] * wm[tap][ci][co]
+ * with dy' = dy where mask > 0 (the ReLU of the forward output; all of dy
+ * when mask is NULL), packed into scratch (B*H*W*cout BF16, 16-byte
+ * aligned) and convolved by sevp_nn_conv3x3_tma with the mirrored weights
+ * of sevp_nn_weight_mirror.  The same result as sevp_nn_conv3x3 with flip
+ * = 1 up to the FP32 summation order; limits of sevp_nn_conv3x3_tma, with
+ * cout as its input channels. */
+int sevp_nn_conv3x3_dgrad_tc(const void *dy, int dy_ld, int dy_off, int cout, const void *mask,
+                             int mask_ld, int mask_off, const void *wm, void *scratch, void *dx,
+                             int dx_ld, int dx_off, int cin, int B, int H, int W, void *stream);
 
 /* 2x2 average pooling of C channels (H, W even): forward H x W -> H/2 x W/2;
  * backward spreads a quarter of each gradient to its four inputs (added to

@@ -38,23 +38,48 @@ __global__ void k_fs_mask(int i0, int j0, float *u, float *v, const int16_t *iu0
     v[IDX3(j0 - 1, i, j, 1)] = __fmul_rn((float)iv0[IDX2(i, j)], v[IDX3(j0 - 1, i, j, 1)]);
 }
 
-// one thread per interior column: W from the bottom (W(K0) = 0) to the top
-__global__ void k_fs_rhs(int i0, int j0, int k0, const float *u, const float *v, const float *odx,
-                         const float *ody, const float *ocs, const float *csv, const float *odz,
+// Layers a thread of the column kernels loads before it uses the first of
+// them (loads in flight per thread).
+constexpr int kFsLayerBatch = 4;
+
+// one thread per interior column: W from the bottom (W(K0) = 0) to the top.
+// The layer thicknesses' reciprocals are formed once per CTA (rdz, k1
+// floats of dynamic shared memory), and the velocities of kFsLayerBatch
+// layers are loaded before they are summed in the reference's order.
+__global__ void k_fs_rhs(int i0, int j0, int k0, const float *__restrict__ u,
+                         const float *__restrict__ v, const float *odx, const float *ody,
+                         const float *ocs, const float *csv, const float *odz,
                          const float *rscale, float *s, double *b) {
+  extern __shared__ float rdz[];
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 2, j = blockIdx.y + 2;
   const int i1 = i0 - 1, i2 = i0 - 2, j1 = j0 - 1, k1 = k0 - 1;
+  for (int k = threadIdx.x; k < k1; k += blockDim.x) rdz[k] = __fdiv_rn(1.f, odz[k]);
+  __syncthreads();
   if (i > i1 || j > j1) return;
   const float temp = __fmul_rn(ocs[j - 1], ody[j - 1]);
   const float dx = odx[j - 1], cn = csv[j - 1], cs = csv[j - 2];
   float w = 0.f;
-  for (int k = k1; k >= 1; --k) {
-    const float temp1 = __fdiv_rn(1.f, odz[k - 1]);
-    const float a = __fmul_rn(__fsub_rn(u[IDX3(j0, i, j, k)], u[IDX3(j0, i - 1, j, k)]), dx);
-    const float bb = __fsub_rn(__fmul_rn(cn, v[IDX3(j0 - 1, i, j, k)]),
-                               __fmul_rn(cs, v[IDX3(j0 - 1, i, j - 1, k)]));
-    w = __fadd_rn(w, __fmul_rn(__fadd_rn(a, __fmul_rn(bb, temp)), temp1));
+  auto layer = [&](float ue, float uw, float vn, float vs, int k) {
+    const float a = __fmul_rn(__fsub_rn(ue, uw), dx);
+    const float bb = __fsub_rn(__fmul_rn(cn, vn), __fmul_rn(cs, vs));
+    w = __fadd_rn(w, __fmul_rn(__fadd_rn(a, __fmul_rn(bb, temp)), rdz[k - 1]));
+  };
+  int k = k1;
+  for (; k >= kFsLayerBatch; k -= kFsLayerBatch) {
+    float ue[kFsLayerBatch], uw[kFsLayerBatch], vn[kFsLayerBatch], vs[kFsLayerBatch];
+#pragma unroll
+    for (int q = 0; q < kFsLayerBatch; ++q) {
+      ue[q] = u[IDX3(j0, i, j, k - q)];
+      uw[q] = u[IDX3(j0, i - 1, j, k - q)];
+      vn[q] = v[IDX3(j0 - 1, i, j, k - q)];
+      vs[q] = v[IDX3(j0 - 1, i, j - 1, k - q)];
+    }
+#pragma unroll
+    for (int q = 0; q < kFsLayerBatch; ++q) layer(ue[q], uw[q], vn[q], vs[q], k - q);
   }
+  for (; k >= 1; --k)
+    layer(u[IDX3(j0, i, j, k)], u[IDX3(j0, i - 1, j, k)], v[IDX3(j0 - 1, i, j, k)],
+          v[IDX3(j0 - 1, i, j - 1, k)], k);
   const size_t o = (size_t)(j - 2) * i2 + (i - 2);
   if (s) s[o] = w;
   if (b) b[o] = rscale ? (double)w * (double)rscale[j - 2] : (double)w;
@@ -62,6 +87,28 @@ __global__ void k_fs_rhs(int i0, int j0, int k0, const float *u, const float *v,
 
 __device__ __forceinline__ float face_corr(double xr, double xl, float metric) {
   return __double2float_rn(-__dmul_rn(__dsub_rn(xr, xl), (double)metric));
+}
+
+// f[o + l * stride] += c * m[o + l * stride] for the n layers below the top
+// (the land mask of each layer), kFsLayerBatch layers loaded at a time.
+__device__ __forceinline__ void correct_layers(float *f, const int16_t *m, size_t o,
+                                               size_t stride, int n, float c) {
+  int l = 0;
+  for (; l + kFsLayerBatch <= n; l += kFsLayerBatch) {
+    float fv[kFsLayerBatch];
+    int16_t mv[kFsLayerBatch];
+#pragma unroll
+    for (int q = 0; q < kFsLayerBatch; ++q) {
+      fv[q] = f[o + (size_t)(l + q) * stride];
+      mv[q] = m[o + (size_t)(l + q) * stride];
+    }
+#pragma unroll
+    for (int q = 0; q < kFsLayerBatch; ++q)
+      f[o + (size_t)(l + q) * stride] = __fadd_rn(fv[q], __fmul_rn(c, (float)mv[q]));
+  }
+  for (; l < n; ++l)
+    f[o + (size_t)l * stride] = __fadd_rn(f[o + (size_t)l * stride],
+                                          __fmul_rn(c, (float)m[o + (size_t)l * stride]));
 }
 
 // one thread per (I, J): P0 at the cell, the U face east of it, the V face
@@ -92,10 +139,7 @@ __global__ void k_fs_correct(int i0, int j0, int k0, const double *x, float odt,
     s3[o] = __fadd_rn(s3[o], c);
     const float top = __fadd_rn(u[IDX3(j0, i, j, 1)], c);
     u[IDX3(j0, i, j, 1)] = top;
-#pragma unroll 4
-    for (int k = 2; k <= k1; ++k)
-      u[IDX3(j0, i, j, k)] =
-          __fadd_rn(u[IDX3(j0, i, j, k)], __fmul_rn(c, (float)iu[IDX3(j0, i, j, k)]));
+    correct_layers(u, iu, IDX3(j0, i, j, 2), plane, k1 - 1, c);
     if (i >= 2 && i <= i2) land = __fmul_rn((float)(1 - iu0[o]), fabsf(top));
   }
   if (i >= 2 && i <= i1 && j <= j1) {  // V face (I, J), J = 1 .. J1
@@ -106,10 +150,7 @@ __global__ void k_fs_correct(int i0, int j0, int k0, const double *x, float odt,
     s4[o] = __fadd_rn(s4[o], c);
     const float top = __fadd_rn(v[IDX3(j0 - 1, i, j, 1)], c);
     v[IDX3(j0 - 1, i, j, 1)] = top;
-#pragma unroll 4
-    for (int k = 2; k <= k1; ++k)
-      v[IDX3(j0 - 1, i, j, k)] =
-          __fadd_rn(v[IDX3(j0 - 1, i, j, k)], __fmul_rn(c, (float)iv[IDX3(j0 - 1, i, j, k)]));
+    correct_layers(v, iv, IDX3(j0 - 1, i, j, 2), (size_t)i0 * (j0 - 1), k1 - 1, c);
     if (j >= 2 && j <= j2) land = fmaxf(land, __fmul_rn((float)(1 - iv0[o]), fabsf(top)));
   }
   // non-negative floats order like their bit patterns
@@ -141,8 +182,8 @@ int sevp_fs_rhs(int i0, int j0, int k0, const float *u, const float *v, const fl
   if (!fs_dims_ok(i0, j0, k0) || !u || !v || !odx || !ody || !ocs || !csv || !odz || (!s && !b))
     return SEVP_BAD_ARG;
   dim3 grid((unsigned)((i0 - 2 + 127) / 128), (unsigned)(j0 - 2));
-  k_fs_rhs<<<grid, 128, 0, (cudaStream_t)stream>>>(i0, j0, k0, u, v, odx, ody, ocs, csv, odz, rscale,
-                                                   s, b);
+  k_fs_rhs<<<grid, 128, (size_t)(k0 - 1) * sizeof(float), (cudaStream_t)stream>>>(
+      i0, j0, k0, u, v, odx, ody, ocs, csv, odz, rscale, s, b);
   SEVP_CUDA_TRY(cudaGetLastError());
   return SEVP_OK;
 }

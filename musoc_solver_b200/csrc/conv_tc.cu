@@ -259,6 +259,168 @@ __global__ void __launch_bounds__(kTcThreads)
 }
 
 
+// ------------------------------------------------ weight gradient
+// dW[tap][ci][co] += sum_p X[p + shift(tap)][ci] * G[p][co] as an implicit
+// GEMM on tcgen05: D[m][n] = sum_k A[m][k] B[n][k] with m = co (a block of
+// 128 rows; rows past cout are zero), n = ci (all cin <= 256 channels), k =
+// the pixels of this CTA's chunk, kWgK per pipeline step.  G is the packed
+// output gradient [P][cout] (already masked by the ReLU).  Both operands lie
+// channels-contiguous (NHWC) in memory, so the staging transposes them into
+// the K-major no-swizzle core-matrix layout of k_conv3x3_tc: a thread loads
+// 8 channels of two neighbouring pixels (two 16-byte loads) and writes eight
+// 4-byte (k, k+1) pairs, one per row.  Thread 0 issues the K = 16 MMAs of a
+// step and commits them to the stage's mbarrier; with kWgStages stages a
+// stage is refilled while the MMAs of the two before it run.  The FP32 tile
+// in TMEM is added to dW with atomics (the pixel chunks of a tap are spread
+// over CTAs).  Waits are bounded as in k_conv3x3_tc.
+constexpr int kWgStages = 3;
+constexpr int kWgK = 64;  // pixels per step
+
+__device__ __forceinline__ void store_k_pairs(unsigned char *base, int grp, int k, const uint4 &v0,
+                                              const uint4 &v1) {
+  // rows 8 grp .. 8 grp + 7, K elements k and k + 1 (k even)
+  const uint16_t *a = reinterpret_cast<const uint16_t *>(&v0);
+  const uint16_t *b = reinterpret_cast<const uint16_t *>(&v1);
+  unsigned char *core = base + (k >> 3) * 128 + grp * (kWgK / 8 * 128) + (k & 7) * 2;
+#pragma unroll
+  for (int j = 0; j < 8; ++j)
+    *reinterpret_cast<uint32_t *>(core + j * 16) = (uint32_t)a[j] | ((uint32_t)b[j] << 16);
+}
+
+__global__ void __launch_bounds__(kTcThreads)
+    k_conv3x3_wgrad_tc(const bf16 *__restrict__ x, int x_ld, int x_off, int cin,
+                       const bf16 *__restrict__ g, int cout, float *__restrict__ dw, int B, int H,
+                       int W, long long ppc, uint32_t tmem_cols) {
+  extern __shared__ __align__(1024) unsigned char sm[];
+  __shared__ __align__(8) uint64_t bars[kWgStages];
+  __shared__ uint32_t s_tmem;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const long long HW = (long long)H * W, P = (long long)B * HW;
+  const int cob = (cout + 127) / 128;
+  const int tap = blockIdx.y / cob, co0 = (blockIdx.y % cob) * 128;
+  const int mrows = min(cout - co0, 128);
+  const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+  const long long pb = (long long)blockIdx.x * ppc;
+  const long long pe = min(P, pb + ppc);
+  const int T = pe > pb ? (int)((pe - pb + kWgK - 1) / kWgK) : 0;
+  constexpr uint32_t a_bytes = 128 * kWgK * 2;
+  const uint32_t stage_bytes = a_bytes + (uint32_t)cin * kWgK * 2;
+  const uint32_t sbase = smem_u32(sm);
+  constexpr uint32_t core_sbo = kWgK / 8 * 128;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                     smem_u32(&s_tmem)),
+                 "r"(tmem_cols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+  }
+  if (tid == 0) {
+    for (int q = 0; q < kWgStages; ++q) mbar_init(smem_u32(&bars[q]), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  // A rows past cout stay zero in every stage (8-row groups are 1 KB apart)
+  for (int q = 0; q < kWgStages; ++q)
+    for (uint32_t e = (uint32_t)(mrows / 8) * core_sbo + tid * 16; e < a_bytes; e += kTcThreads * 16)
+      *reinterpret_cast<uint4 *>(sm + q * stage_bytes + e) = make_uint4(0, 0, 0, 0);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = s_tmem;
+
+  auto stage = [&](int s) {
+    unsigned char *a_p = sm + (s % kWgStages) * stage_bytes;
+    unsigned char *b_p = a_p + a_bytes;
+    const long long k0 = pb + (long long)s * kWgK;
+    const uint4 zero = make_uint4(0, 0, 0, 0);
+    const int mg = mrows / 8, ng = cin / 8;
+    for (int e = tid; e < (kWgK / 2) * mg; e += kTcThreads) {
+      const int kp = e / mg, grp = e - kp * mg, k = 2 * kp;
+      const long long p = k0 + k;
+      const uint4 v0 = p < pe ? *reinterpret_cast<const uint4 *>(g + p * cout + co0 + grp * 8) : zero;
+      const uint4 v1 =
+          p + 1 < pe ? *reinterpret_cast<const uint4 *>(g + (p + 1) * cout + co0 + grp * 8) : zero;
+      store_k_pairs(a_p, grp, k, v0, v1);
+    }
+    for (int e = tid; e < (kWgK / 2) * ng; e += kTcThreads) {
+      const int kp = e / ng, grp = e - kp * ng, k = 2 * kp;
+      uint4 v[2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const long long p = k0 + k + h;
+        v[h] = zero;
+        if (p < pe) {
+          const long long img = p / HW;
+          const int rem = (int)(p - img * HW);
+          const int yy = rem / W + dy, xx = rem - (rem / W) * W + dx;
+          if (yy >= 0 && yy < H && xx >= 0 && xx < W)
+            v[h] = *reinterpret_cast<const uint4 *>(
+                x + ((img * H + yy) * W + xx) * x_ld + x_off + grp * 8);
+        }
+      }
+      store_k_pairs(b_p, grp, k, v[0], v[1]);
+    }
+  };
+
+  const uint32_t idesc = instr_desc_bf16(128, cin);
+  bool failed = false;
+  int issued = 0;  // steps whose MMAs were committed
+  for (int s = 0; s < T; ++s) {
+    if (s >= kWgStages) {  // the stage was last read by the MMAs of step s - kWgStages
+      const int sp = s - kWgStages;
+      if (!mbar_wait(smem_u32(&bars[sp % kWgStages]), (unsigned)(sp / kWgStages) & 1u,
+                     g_tc_wait_limit))
+        failed = true;
+    }
+    if (__syncthreads_or(failed)) {
+      failed = true;
+      break;
+    }
+    stage(s);
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      tc_fence_after();
+      const uint32_t a_s = sbase + (uint32_t)(s % kWgStages) * stage_bytes, b_s = a_s + a_bytes;
+#pragma unroll
+      for (int k16 = 0; k16 < kWgK / 16; ++k16) {
+        const uint64_t ad = smem_desc(a_s + k16 * 256, 128, core_sbo);
+        const uint64_t bd = smem_desc(b_s + k16 * 256, 128, core_sbo);
+        tc_mma(tmem, ad, bd, idesc, (s > 0 || k16 > 0) ? 1u : 0u);
+      }
+      tc_commit(smem_u32(&bars[s % kWgStages]));
+    }
+    issued = s + 1;
+  }
+  // every committed MMA has completed once the last commit has arrived (the
+  // drain after a failure uses the full limit)
+  if (issued > 0 &&
+      !mbar_wait(smem_u32(&bars[(issued - 1) % kWgStages]), (unsigned)((issued - 1) / kWgStages) & 1u))
+    failed = true;
+  failed = __syncthreads_or(failed) != 0;
+  tc_fence_after();
+  if (issued > 0) {
+    const int m = warp * 32 + lane;
+    const uint32_t tl = tmem + ((uint32_t)(warp * 32) << 16);
+    for (int n0 = 0; n0 < cin; n0 += 16) {
+      uint32_t v[16];
+      tmem_ld16(tl + (uint32_t)n0, v);
+      if (!failed && m < mrows) {
+#pragma unroll
+        for (int q = 0; q < 16; ++q)
+          atomicAdd(dw + ((size_t)tap * cin + n0 + q) * cout + co0 + m, __uint_as_float(v[q]));
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(tmem_cols)
+                 : "memory");
+  if (failed) atomicCAS(&g_tc_error, 0, SEVP_TIMEOUT);
+}
+
+
 // ------------------------------------------------ TMA-fed variant (cin % 64 == 0)
 // The same implicit GEMM with the operands brought in by the tensor memory
 // accelerator: per step one 4-D tensor-map load of the tap-shifted A tile
@@ -561,6 +723,40 @@ int sevp_nn_conv3x3_tma(const void *in, int in_ld, int in_off, int cin, const vo
                                relu, stream, enc);
   return launch_conv_tma<64>(in, in_ld, in_off, cin, wk, bias, out, out_ld, out_off, cout, B, H, W,
                              relu, stream, enc);
+}
+
+// dw[tap][ci][co] += sum_p x[p + shift(tap)][x_off + ci] * g[p][co] (FP32),
+// with g the packed output gradient [B*H*W][cout] (already masked by the
+// ReLU).  cin and cout multiples of 16 up to 256; x_ld and x_off multiples
+// of 8; x and g 16-byte aligned.
+int sevp_nn_conv3x3_wgrad_tc(const void *x, int x_ld, int x_off, int cin, const void *g, int cout,
+                             float *dw, int B, int H, int W, void *stream) {
+  if (!x || !g || !dw || B < 1 || H < 1 || W < 1) return SEVP_BAD_ARG;
+  if (cin < 16 || cin > 256 || cin % 16 || cout < 16 || cout > 256 || cout % 16)
+    return SEVP_BAD_ARG;
+  if ((x_ld % 8) || (x_off % 8) || x_off + cin > x_ld || !aligned16(x) || !aligned16(g))
+    return SEVP_BAD_ARG;
+  const long long P = (long long)B * H * W;
+  const int cob = (cout + 127) / 128;
+  // enough CTAs to cover the GPU twice, each with whole steps of kWgK pixels
+  long long chunks = (2LL * 148 + 9LL * cob - 1) / (9LL * cob);
+  long long ppc = (P + chunks - 1) / chunks;
+  ppc = (ppc + kWgK - 1) / kWgK * kWgK;
+  chunks = (P + ppc - 1) / ppc;
+  uint32_t cols = 32;
+  while (cols < (uint32_t)cin) cols <<= 1;
+  const size_t smem = (size_t)kWgStages * (128 * kWgK * 2 + (size_t)cin * kWgK * 2);
+  static size_t set_smem = 0;
+  if (smem > set_smem) {
+    SEVP_CUDA_TRY(cudaFuncSetAttribute(k_conv3x3_wgrad_tc,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    set_smem = smem;
+  }
+  dim3 grid((unsigned)chunks, (unsigned)(9 * cob));
+  k_conv3x3_wgrad_tc<<<grid, kTcThreads, smem, (cudaStream_t)stream>>>(
+      (const bf16 *)x, x_ld, x_off, cin, (const bf16 *)g, cout, dw, B, H, W, ppc, cols);
+  SEVP_CUDA_TRY(cudaGetLastError());
+  return SEVP_OK;
 }
 
 int sevp_nn_tc_set_wait_limit(unsigned limit) {

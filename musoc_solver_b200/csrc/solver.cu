@@ -318,7 +318,7 @@ __global__ void __launch_bounds__(kTileWarps * 32, SEVP_TILE_MINB)
     const int nx = tg.nx;
     const int j0 = b * tg.th, hh = tile_height(tg, b), nb = tg.grp_nb[(size_t)b * tg.txg + grp];
     const int i = tile_col(tg, a, n);
-    const MT *mt = mats + (mw > 0 ? tg.moff[(size_t)b * tg.tx + a] : 0);
+    const MT *mt = tile_mats(mats, tg, b, grp, a, mw);
     const size_t msz = (size_t)mw * mw;
     double alpha = 0.0;
     if (UPDATE) alpha = st->alpha;
@@ -491,8 +491,11 @@ __global__ void __launch_bounds__(kTileWarps * 32, 2)
   if ((DOTS || UPDATE) && st->done) return;
   constexpr bool kChain = sizeof(V) == 4;
   __shared__ double dv_all[kTileWarps * 32];
+  // per warp: the influence matrices of its group (tiles up to 16 wide)
+  __shared__ __align__(16) double mslot_all[kTileWarps * kGroupMatSlots];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   double *dv = dv_all + wib * 32;
+  double *mslot = mslot_all + wib * kGroupMatSlots;
   double acc_rz = 0.0, acc_rr = 0.0;
   double alpha = 0.0;
   if (UPDATE) alpha = st->alpha;
@@ -507,37 +510,50 @@ __global__ void __launch_bounds__(kTileWarps * 32, 2)
     const int nx = tg.nx;
     const int j0 = b * tg.th, hh = tile_height(tg, b), nb = tg.grp_nb[(size_t)b * tg.txg + grp];
     const int i = tile_col(tg, a, n);
-    const MT *mt = mats + (mw > 0 ? tg.moff[(size_t)b * tg.tx + a] : 0);
+    const MT *mt = tile_mats(mats, tg, b, grp, a, mw);
     const size_t idx0 = (size_t)j0 * nx + i;
+    // a full-height single-sub-block group (the common case) copies its
+    // matrices to shared memory first: the copy overlaps the row loads and
+    // the forward sweep instead of following them
+    const bool pre = nb == 1 && hh == HM && tg.wseg * tg.wseg * tg.tpw <= kGroupMatSlots;
+    const MT *mts = pre ? prefetch_group_mats(mats, tg, b, grp, seg, lane, mslot) : mt;
 
-    // ---- all loads of the task
-    V rr[HM], xx[UPDATE ? HM : 1], pp[UPDATE ? HM : 1], qq[UPDATE ? HM : 1];
+    // ---- all loads of the task, and the fused update x += alpha p,
+    //      r -= alpha q (its stores leave before the march)
+    V rr[HM];
     float cc_[HM], ce_[HM], cn_[HM], cw_[SYM ? 1 : HM], cs_[SYM ? 1 : HM];
+    {
+      V xx[UPDATE ? HM : 1], pp[UPDATE ? HM : 1], qq[UPDATE ? HM : 1];
 #pragma unroll
-    for (int k = 0; k < HM; ++k) {
-      const bool ok = active && k < hh;
-      const size_t id = ok ? idx0 + (size_t)k * nx : 0;
-      rr[k] = ok ? r[id] : V(0);
+      for (int k = 0; k < HM; ++k) {
+        const bool ok = active && k < hh;
+        const size_t id = ok ? idx0 + (size_t)k * nx : 0;
+        rr[k] = ok ? r[id] : V(0);
+        if (UPDATE) {
+          xx[k] = ok ? x[id] : V(0);
+          pp[k] = ok ? p[id] : V(0);
+          qq[k] = ok ? q[id] : V(0);
+        }
+      }
+      load_task_coeffs<SYM, HM>(c, idx0, nx, hh, active, cc_, ce_, cn_, cw_, cs_);
       if (UPDATE) {
-        xx[k] = ok ? x[id] : V(0);
-        pp[k] = ok ? p[id] : V(0);
-        qq[k] = ok ? q[id] : V(0);
+#pragma unroll
+        for (int k = 0; k < HM; ++k) {
+          if (active && k < hh) {
+            const size_t idx = idx0 + (size_t)k * nx;
+            const V xn = xx[k] + (V)alpha * pp[k];
+            const V rn = rr[k] - (V)alpha * qq[k];
+            x[idx] = xn;
+            r[idx] = rn;
+            rr[k] = rn;
+          }
+        }
       }
     }
-    load_task_coeffs<SYM, HM>(c, idx0, nx, hh, active, cc_, ce_, cn_, cw_, cs_);
 
-    // row k's right-hand side: the residual, after the fused update
-    // x += alpha p, r -= alpha q
+    // row k's right-hand side: the (updated) residual
     auto rhs = [&](int k) -> double {
       if (!active) return 0.0;
-      if (UPDATE) {
-        const size_t idx = idx0 + (size_t)k * nx;
-        const V xn = xx[k] + (V)alpha * pp[k];
-        const V rn = rr[k] - (V)alpha * qq[k];
-        x[idx] = xn;
-        r[idx] = rn;
-        rr[k] = rn;
-      }
       const double rv = (double)rr[k];
       acc_rr += rv * rv;
       return rv;
@@ -547,8 +563,13 @@ __global__ void __launch_bounds__(kTileWarps * 32, 2)
       z[idx0 + (size_t)k * nx] = zv;
       if (DOTS) acc_rz += (double)rr[k] * (double)zv;
     };
-    march_task_regs<MT, SYM, kChain, HM, UPDATE && !DOTS>(cc_, ce_, cn_, cw_, cs_, hh, nb, n, mw,
-                                                          active, lane, segbase, dv, mt, rhs, emit);
+    if (pre)
+      march_task_full<MT, SYM, kChain, HM, UPDATE && !DOTS, true>(
+          cc_, ce_, cn_, cw_, cs_, n, mw, active, lane, segbase, dv, mts, rhs, emit);
+    else
+      march_task_regs<MT, SYM, kChain, HM, UPDATE && !DOTS>(cc_, ce_, cn_, cw_, cs_, hh, nb, n,
+                                                            mw, active, lane, segbase, dv, mt, rhs,
+                                                            emit);
   }
   if (DOTS) {
     double v2[2] = {acc_rz, acc_rr};
@@ -597,7 +618,7 @@ __global__ void __launch_bounds__(kTileWarps * 32, 2)
     const int nx = tg.nx;
     const int j0 = b * tg.th, hh = tile_height(tg, b), nb = tg.grp_nb[(size_t)b * tg.txg + grp];
     const int i = tile_col(tg, a, n);
-    const MT *mt = mats + (mw > 0 ? tg.moff[(size_t)b * tg.tx + a] : 0);
+    const MT *mt = tile_mats(mats, tg, b, grp, a, mw);
     const size_t idx0 = (size_t)j0 * nx + i;
     if constexpr (kStage > 0) {
 #pragma unroll
@@ -686,8 +707,10 @@ __global__ void k_to_float(const double *a, float *b, size_t n) {
 
 // Per-tile marching growth: the smallest sub-block height s_max such that
 // z^s <= growth, with z + 1/z = max over the tile's marched rows of
-// (|AC| + |AL| + |AR|) / |AT|.  One warp per tile; writes s per tile.
-__global__ void k_tile_growth(TileGeom tg, Coeffs c, double log_growth, int *s_tile) {
+// (|AC| + |AL| + |AR|) / |AT|.  One warp per tile; writes s per tile, and
+// log z per tile when lz is given (infinity where a marched AT is zero).
+__global__ void k_tile_growth(TileGeom tg, Coeffs c, double log_growth, int *s_tile,
+                              float *lz = nullptr) {
   const int lane = threadIdx.x & 31;
   const int tile = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (tile >= tg.tx * tg.ty) return;
@@ -714,8 +737,32 @@ __global__ void k_tile_growth(TileGeom tg, Coeffs c, double log_growth, int *s_t
     } else {
       const double zz = 0.5 * (cmax + sqrt(fmax(cmax * cmax - 4.0, 0.0)));
       if (zz > 1.0) s = (int)floor(log_growth / log(zz));
+      if (lz) lz[tile] = (float)log(zz);
     }
+    if (lz && bad) lz[tile] = INFINITY;
     s_tile[tile] = s < 1 ? 1 : (s > tg.th ? tg.th : s);
+  }
+}
+
+// Influence data with the precision chosen per warp group (MixMat layout):
+// a group flagged in tg.grp_f32 gets each matrix rounded to FP32 in the
+// first half of its FP64 slot, the others an FP64 copy.  One CTA per tile.
+__global__ void k_mix_influence(TileGeom tg, const double *mats, double *mix) {
+  const int tile = blockIdx.x;
+  const int a = tile % tg.tx, b = tile / tg.tx;
+  const int grp = a / tg.tpw, mw = tile_width(tg, a);
+  const int nb = tg.grp_nb[(size_t)b * tg.txg + grp];
+  const bool f32 = tg.grp_f32[(size_t)b * tg.txg + grp] != 0;
+  const size_t msz = (size_t)mw * mw, base = (size_t)tg.moff[tile];
+  for (int t = 0; t < 2 * nb - 1; ++t) {
+    const double *src = mats + base + t * msz;
+    double *dst = mix + base + t * msz;
+    for (size_t e = threadIdx.x; e < msz; e += blockDim.x) {
+      if (f32)
+        reinterpret_cast<float *>(dst)[e] = (float)src[e];
+      else
+        dst[e] = src[e];
+    }
   }
 }
 
@@ -883,16 +930,25 @@ struct Tiling {
   long long *d_moff = nullptr;
   double *d_mats = nullptr;
   float *d_mats32 = nullptr;
+  // per-group-precision copy (MixMat layout) and its group flags
+  // (sevp_set_influence_fp32)
+  double *d_matsmix = nullptr;
+  unsigned char *d_grp_f32 = nullptr;
+  int f32_groups = 0;
+  long long mix_bytes_per_pass = 0;
   long long mats_elems = 0;
   std::vector<int> grp_nb;   // per warp group (ty * txg)
   std::vector<int> tile_nb;  // effective sub-blocks per tile (ty * tx)
   bool built = false;
   void release() {
     for (void *p : {(void *)d_grp_nb, (void *)d_moff, (void *)d_mats, (void *)d_mats32,
-                    (void *)d_al, (void *)d_ar})
+                    (void *)d_al, (void *)d_ar, (void *)d_matsmix, (void *)d_grp_f32})
       if (p) cudaFree(p);
     d_grp_nb = nullptr, d_moff = nullptr, d_mats = nullptr, d_mats32 = nullptr;
-    d_al = nullptr, d_ar = nullptr;
+    d_al = nullptr, d_ar = nullptr, d_matsmix = nullptr, d_grp_f32 = nullptr;
+    tg.grp_f32 = nullptr;
+    f32_groups = 0;
+    mix_bytes_per_pass = 0;
     mats_elems = 0;
     built = false;
   }
@@ -918,6 +974,9 @@ struct sevp_ctx {
   bool have_res = false;
   const double *roww = nullptr;
   bool infl32_active = false;   // current solve uses the FP32 influence copies
+  // growth limit of the per-group FP32 influence data of the FP32-vector
+  // tile passes (sevp_set_influence_fp32; <= 1: off)
+  double mix_limit = 0.0;
   // the tiling request of the last sevp_set_operator (the second tiling is
   // built from it)
   sevp_tiling treq{};
@@ -1138,6 +1197,12 @@ static int launch_tile(sevp_ctx *ctx, const Tiling &T, V *x, const V *p, V *r, c
       if (ctx->sym)
         return launch_tile_k<V, float, UPDATE, DOTS, true>(ctx, T, T.d_mats32, x, p, r, q, z, ticket_slot);
       return launch_tile_k<V, float, UPDATE, DOTS, false>(ctx, T, T.d_mats32, x, p, r, q, z, ticket_slot);
+    }
+    if (T.d_matsmix) {
+      const MixMat *mm = reinterpret_cast<const MixMat *>(T.d_matsmix);
+      if (ctx->sym)
+        return launch_tile_k<V, MixMat, UPDATE, DOTS, true>(ctx, T, mm, x, p, r, q, z, ticket_slot);
+      return launch_tile_k<V, MixMat, UPDATE, DOTS, false>(ctx, T, mm, x, p, r, q, z, ticket_slot);
     }
   }
   if (ctx->sym)
@@ -1508,6 +1573,75 @@ static int build_tiling(sevp_ctx *ctx, Tiling &T, int xs) {
   return SEVP_OK;
 }
 
+// Per-group FP32 influence data of tiling T for ctx->mix_limit (see
+// sevp_set_influence_fp32): a group reads FP32 matrices when every tile in
+// it has z^s <= mix_limit, s its sub-block height and z its row growth
+// (k_tile_growth).  Drops the previous copy first; nothing more when off.
+static int build_mix(sevp_ctx *ctx, Tiling &T) {
+  if (T.d_matsmix) cudaFree(T.d_matsmix);
+  if (T.d_grp_f32) cudaFree(T.d_grp_f32);
+  T.d_matsmix = nullptr;
+  T.d_grp_f32 = nullptr;
+  T.tg.grp_f32 = nullptr;
+  T.f32_groups = 0;
+  T.mix_bytes_per_pass = 0;
+  if (ctx->mix_limit <= 1.0 || !T.built) return SEVP_OK;
+  TileGeom &tg = T.tg;
+  const int ntiles = tg.tx * tg.ty;
+  std::vector<float> lz((size_t)ntiles, 0.f);
+  {
+    int *d_s = nullptr;
+    float *d_lz = nullptr;
+    SEVP_CUDA_TRY(cudaMalloc((void **)&d_s, sizeof(int) * ntiles));
+    cudaError_t e = cudaMalloc((void **)&d_lz, sizeof(float) * ntiles);
+    if (e == cudaSuccess) {
+      k_tile_growth<<<(ntiles + 7) / 8, 256, 0, ctx->stream>>>(tg, T.c, log(2.0), d_s, d_lz);
+      ctx->launches++;
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(lz.data(), d_lz, sizeof(float) * ntiles, cudaMemcpyDeviceToHost,
+                          ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(d_s);
+    if (d_lz) cudaFree(d_lz);
+    if (e != cudaSuccess) {
+      sevp_internal_set_error(e, "influence precision", __FILE__, __LINE__);
+      return SEVP_CUDA_ERROR;
+    }
+  }
+  const double lim = log(ctx->mix_limit);
+  std::vector<unsigned char> f32(T.grp_nb.size(), 1);
+  for (int t = 0; t < ntiles; ++t) {
+    const int a = t % tg.tx, b = t / tg.tx;
+    const size_t g = (size_t)b * tg.txg + a / tg.tpw;
+    const int hs = ceil_div(tile_height(tg, b), T.grp_nb[g]);
+    if (!((double)hs * (double)lz[t] <= lim)) f32[g] = 0;
+  }
+  long long bytes = 0;
+  for (int t = 0; t < ntiles; ++t) {
+    const int a = t % tg.tx, b = t / tg.tx;
+    const size_t g = (size_t)b * tg.txg + a / tg.tpw;
+    const long long mw = tile_width(tg, a);
+    bytes += (2LL * T.grp_nb[g] - 1) * mw * mw * (f32[g] ? 4 : 8);
+  }
+  for (unsigned char v : f32) T.f32_groups += v;
+  T.mix_bytes_per_pass = bytes;
+  SEVP_CUDA_TRY(cudaMalloc((void **)&T.d_grp_f32, f32.size()));
+  SEVP_CUDA_TRY(cudaMemcpyAsync(T.d_grp_f32, f32.data(), f32.size(), cudaMemcpyHostToDevice,
+                                ctx->stream));
+  const size_t n = (size_t)std::max<long long>(T.mats_elems, 1);
+  SEVP_CUDA_TRY(cudaMalloc((void **)&T.d_matsmix, n * sizeof(double)));
+  SEVP_CUDA_TRY(cudaMemsetAsync(T.d_matsmix, 0, n * sizeof(double), ctx->stream));
+  tg.grp_f32 = T.d_grp_f32;
+  k_mix_influence<<<ntiles, 256, 0, ctx->stream>>>(tg, T.d_mats, T.d_matsmix);
+  ctx->launches++;
+  SEVP_CUDA_TRY(cudaGetLastError());
+  // the host vector f32 must outlive the copy above
+  SEVP_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return SEVP_OK;
+}
+
 // Column cuts of the tiling with shift xs: the first column of every tile.
 static std::vector<char> tiling_cuts(const sevp_ctx *ctx, int xs) {
   std::vector<char> cut((size_t)ctx->nx, 0);
@@ -1629,10 +1763,30 @@ extern "C" int sevp_set_operator(sevp_ctx *ctx, const float *al, const float *ab
   ctx->treq.sub_rows_by_tile_row = nullptr;
   int s = build_tiling(ctx, ctx->ta, 0);
   if (s) return s;
+  s = build_mix(ctx, ctx->ta);
+  if (s) return s;
   ctx->have_op = true;
   s = build_schwarz(ctx);
   if (s) ctx->schwarz_req = 0;  // the block-Jacobi operator stays usable
   return s;
+}
+
+extern "C" int sevp_set_influence_fp32(sevp_ctx *ctx, double growth_limit) {
+  if (!ctx || !(growth_limit == growth_limit)) return SEVP_BAD_ARG;
+  drop_inner_graph(ctx);
+  ctx->mix_limit = growth_limit > 1.0 ? growth_limit : 0.0;
+  return ctx->have_op ? build_mix(ctx, ctx->ta) : SEVP_OK;
+}
+
+extern "C" int sevp_influence_fp32_groups(const sevp_ctx *ctx, int *fp32_groups, int *groups,
+                                          long long *bytes_per_pass) {
+  if (!ctx) return SEVP_BAD_ARG;
+  const Tiling &T = ctx->ta;
+  if (fp32_groups) *fp32_groups = T.d_matsmix ? T.f32_groups : 0;
+  if (groups) *groups = (int)T.grp_nb.size();
+  if (bytes_per_pass)
+    *bytes_per_pass = T.d_matsmix ? T.mix_bytes_per_pass : T.mats_elems * (long long)sizeof(double);
+  return SEVP_OK;
 }
 
 extern "C" int sevp_set_schwarz(sevp_ctx *ctx, int shift) {
@@ -1871,7 +2025,8 @@ static int pcg_loop(sevp_ctx *ctx, V *x, V *r, V *z, V *p0, V *p1, V *q, int che
   };
   // FP32 inner loop: one graph replay per check interval
   const void *const key[5] = {(const void *)x, (const void *)p0,
-                              (const void *)(ctx->infl32_active ? ctx->ta.d_mats32 : nullptr),
+                              ctx->infl32_active ? (const void *)ctx->ta.d_mats32
+                                                 : (const void *)ctx->ta.d_matsmix,
                               (const void *)(schwarz_on(ctx) ? ctx->tb.d_mats : nullptr),
                               (const void *)(uintptr_t)SEVP_METHOD_PCG};
   int s = graph_loop(ctx, sizeof(V) == 4, key, check_every,

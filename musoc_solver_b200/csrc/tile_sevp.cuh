@@ -44,6 +44,9 @@ struct TileGeom {
   int xs;     // column shift of the tiling (0 <= xs < nx)
   const int *grp_nb;         // [ty * txg] sub-blocks of the tiles of one warp group
   const long long *moff;     // [ty * tx] offset of each tile's influence data
+  // [ty * txg] 1 where the group's matrices are stored as FP32 in a
+  // per-group-precision copy of the influence data (MixMat); may be null
+  const unsigned char *grp_f32;
 };
 
 __host__ __device__ inline int tile_width(const TileGeom &g, int a) {

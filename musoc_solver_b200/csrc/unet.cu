@@ -13,6 +13,7 @@
 #include <cuda_bf16.h>
 #include <mma.h>
 
+#include "../../include/sevp_nn.h"
 #include "common.cuh"
 
 using namespace nvcuda;
@@ -229,6 +230,42 @@ __global__ void k_weight_transpose(const bf16 *w, bf16 *wt, int cin, int cout) {
     const int rem = (int)(e % ((size_t)cin * cout));
     const int ci = rem / cout, co = rem % cout;
     wt[((size_t)tap * cout + co) * cin + ci] = w[e];
+  }
+}
+
+// Tap-mirrored copy for the data gradient on the tensor cores:
+// wm[tap][ci][co] = w[8 - tap][ci][co].  Read as the [tap][n][k] weights of
+// a forward convolution from co input to ci output channels, it gives
+// dX[p][ci] = sum_{tap, co} dY[p + shift(tap)][co] w[8 - tap][ci][co].
+__global__ void k_weight_mirror(const bf16 *w, bf16 *wm, int cin, int cout) {
+  const size_t per_tap = (size_t)cin * cout, n = 9 * per_tap;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n;
+       e += (size_t)gridDim.x * blockDim.x) {
+    const size_t tap = e / per_tap;
+    wm[e] = w[(8 - tap) * per_tap + e % per_tap];
+  }
+}
+
+// Output gradient through the ReLU of the forward output, packed:
+// out[p][c] = mask[p][c] > 0 ? dy[p][c] : 0 (c < C), or dy itself when mask
+// is null.  8 channels per thread.
+__global__ void k_relu_mask8(const bf16 *dy, int dy_ld, int dy_off, const bf16 *mask, int mask_ld,
+                             int mask_off, int C8, bf16 *out, long long P) {
+  const long long n = P * C8;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long p = e / C8;
+    const int c = (int)(e % C8) * 8;
+    uint4 g = *reinterpret_cast<const uint4 *>(dy + p * dy_ld + dy_off + c);
+    if (mask) {
+      const uint4 m = *reinterpret_cast<const uint4 *>(mask + p * mask_ld + mask_off + c);
+      const bf16 *mv = reinterpret_cast<const bf16 *>(&m);
+      bf16 *gv = reinterpret_cast<bf16 *>(&g);
+#pragma unroll
+      for (int k = 0; k < 8; ++k)
+        if (!(__bfloat162float(mv[k]) > 0.f)) gv[k] = __float2bfloat16(0.f);
+    }
+    *reinterpret_cast<uint4 *>(out + p * (long long)C8 * 8 + c) = g;
   }
 }
 
@@ -498,6 +535,61 @@ int sevp_nn_conv3x3_wgrad(const void *x, int x_ld, int x_off, int cin, const voi
   }
   SEVP_CUDA_TRY(cudaGetLastError());
   return SEVP_OK;
+}
+
+int sevp_nn_weight_mirror(const void *w, void *wm, int cin, int cout, void *stream) {
+  if (!w || !wm) return SEVP_BAD_ARG;
+  const long long n = 9LL * cin * cout;
+  k_weight_mirror<<<ew_grid(n), 256, 0, (cudaStream_t)stream>>>((const bf16 *)w, (bf16 *)wm, cin,
+                                                                cout);
+  SEVP_CUDA_TRY(cudaGetLastError());
+  return SEVP_OK;
+}
+
+int sevp_nn_conv3x3_dgrad_tc(const void *dy, int dy_ld, int dy_off, int cout, const void *mask,
+                             int mask_ld, int mask_off, const void *wm, void *scratch, void *dx,
+                             int dx_ld, int dx_off, int cin, int B, int H, int W, void *stream) {
+  if (!dy || !wm || !scratch || !dx || bad_channels(cin) || bad_channels(cout) || B < 1 ||
+      H < 1 || W < 1 || (dy_ld % 8) || (dy_off % 8) || ((uintptr_t)dy & 15) ||
+      ((uintptr_t)scratch & 15) || (mask && ((mask_ld % 8) || (mask_off % 8) ||
+                                              ((uintptr_t)mask & 15))))
+    return SEVP_BAD_ARG;
+  const long long P = (long long)B * H * W;
+  cudaStream_t st = (cudaStream_t)stream;
+  k_relu_mask8<<<ew_grid(P * (cout / 8)), 256, 0, st>>>((const bf16 *)dy, dy_ld, dy_off,
+                                                        (const bf16 *)mask, mask_ld, mask_off,
+                                                        cout / 8, (bf16 *)scratch, P);
+  SEVP_CUDA_TRY(cudaGetLastError());
+  return sevp_nn_conv3x3_tma(scratch, cout, 0, cout, wm, nullptr, dx, dx_ld, dx_off, cin, B, H, W,
+                             0, stream);
+}
+
+int sevp_nn_conv3x3_backward_tc(const void *x, int x_ld, int x_off, int cin, const void *dy,
+                                int dy_ld, int dy_off, int cout, const void *mask, int mask_ld,
+                                int mask_off, const void *wm, void *scratch, float *dw, float *db,
+                                void *dx, int dx_ld, int dx_off, int B, int H, int W,
+                                void *stream) {
+  if (!x || !dy || !scratch || !dw || bad_channels(cin) || bad_channels(cout) || B < 1 || H < 1 ||
+      W < 1 || (dy_ld % 8) || (dy_off % 8) || ((uintptr_t)dy & 15) || ((uintptr_t)scratch & 15) ||
+      (mask && ((mask_ld % 8) || (mask_off % 8) || ((uintptr_t)mask & 15))) || (dx && !wm))
+    return SEVP_BAD_ARG;
+  const long long P = (long long)B * H * W;
+  cudaStream_t st = (cudaStream_t)stream;
+  // the ReLU-masked output gradient, packed [P][cout], feeds all three
+  k_relu_mask8<<<ew_grid(P * (cout / 8)), 256, 0, st>>>((const bf16 *)dy, dy_ld, dy_off,
+                                                        (const bf16 *)mask, mask_ld, mask_off,
+                                                        cout / 8, (bf16 *)scratch, P);
+  SEVP_CUDA_TRY(cudaGetLastError());
+  int s = sevp_nn_conv3x3_wgrad_tc(x, x_ld, x_off, cin, scratch, cout, dw, B, H, W, stream);
+  if (s) return s;
+  if (db) {
+    dim3 g2(256, (unsigned)((cout + 255) / 256));
+    k_bias_grad<<<g2, 256, 0, st>>>((const bf16 *)scratch, cout, 0, cout, nullptr, 0, 0, db, P);
+    SEVP_CUDA_TRY(cudaGetLastError());
+  }
+  if (!dx) return SEVP_OK;
+  return sevp_nn_conv3x3_tma(scratch, cout, 0, cout, wm, nullptr, dx, dx_ld, dx_off, cin, B, H, W,
+                             0, stream);
 }
 
 int sevp_nn_weight_transpose(const void *w, void *wt, int cin, int cout, void *stream) {

@@ -106,6 +106,9 @@ _SIGS = {
     "sevp_estimate_bounds": ([P, P, DP, DP, IP], C.c_int),
     "sevp_cheb_step": ([P, C.c_int, C.c_double, C.c_double, C.c_double] + [P] * 5, C.c_int),
     "sevp_influence_bytes": ([P], C.c_longlong),
+    "sevp_set_influence_fp32": ([P, C.c_double], C.c_int),
+    "sevp_influence_fp32_groups": ([P, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                    C.POINTER(C.c_longlong)], C.c_int),
     "sevp_solve": ([P, P, P, C.POINTER(SolveOpts), C.POINTER(Report)], C.c_int),
     "sevp_solve_host": ([P, P, P, C.POINTER(SolveOpts), C.POINTER(Report)], C.c_int),
     "sevp_apply": ([P, P, P], C.c_int),

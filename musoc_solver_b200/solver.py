@@ -168,6 +168,20 @@ class SevpSolver:
     def influence_bytes(self) -> int:
         return int(N.lib().sevp_influence_bytes(self.h))
 
+    def set_influence_fp32(self, growth_limit: float):
+        """Per-group influence precision of the FP32 inner iterations: the
+        warp groups whose tiles' marching growth bound is <= growth_limit
+        read FP32 matrices, the rest FP64 (growth_limit <= 1: all FP64)."""
+        N.check(N.lib().sevp_set_influence_fp32(self.h, float(growth_limit)),
+                "sevp_set_influence_fp32")
+
+    def influence_fp32_groups(self):
+        """(FP32 groups, all groups, influence bytes read per tile pass)."""
+        f, g, b = C.c_int(), C.c_int(), C.c_longlong()
+        N.check(N.lib().sevp_influence_fp32_groups(self.h, C.byref(f), C.byref(g), C.byref(b)),
+                "sevp_influence_fp32_groups")
+        return f.value, g.value, b.value
+
     def launches(self) -> int:
         return int(N.lib().sevp_kernel_launches(self.h))
 

@@ -14,8 +14,8 @@ The network predicts a correction for the warm start of the barotropic solve
 
 Every convolution is followed by ReLU.  Activations and weights are BF16
 (NHWC), products accumulate in FP32 on the tensor cores (the forward
-convolutions on tcgen05 with the accumulator in tensor memory, the backward
-ones on warp-level MMA), the master weights and Adam state are FP32.  Every arithmetic step is a kernel of
+convolutions and both gradients of every convolution on tcgen05 with the
+accumulator in tensor memory), the master weights and Adam state are FP32.  Every arithmetic step is a kernel of
 ``libsevp_b200.so``; PyTorch only allocates the buffers.
 """
 from __future__ import annotations
@@ -55,6 +55,16 @@ _SIGS = {
                                C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
                                C.c_int, C.c_int, C.c_int, C.c_void_p], C.c_int),
     "sevp_nn_weight_transpose": ([C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p], C.c_int),
+    "sevp_nn_weight_mirror": ([C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p], C.c_int),
+    "sevp_nn_conv3x3_wgrad_tc": ([C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int,
+                                  C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p], C.c_int),
+    "sevp_nn_conv3x3_backward_tc": ([C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int,
+                                     C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_void_p,
+                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                     C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p], C.c_int),
+    "sevp_nn_conv3x3_dgrad_tc": ([C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int,
+                                  C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
+                                  C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p], C.c_int),
     "sevp_nn_pool": ([C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
                       C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p], C.c_int),
     "sevp_nn_upsample": ([C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int,
@@ -161,6 +171,12 @@ class UNet:
         # the data gradient's transposed weights
         self.wt16 = {n: torch.zeros((9, co, ci), dtype=bf, device=self.dev) for n, ci, co in CONVS}
         if self.train:
+            # tap-mirrored weights ([9][ci][co]) of the tensor-core data
+            # gradient, and its packed masked output gradient (the largest
+            # layer has P[0] x 32 values)
+            self.wm16 = {n: torch.zeros((9, ci, co), dtype=bf, device=self.dev)
+                         for n, ci, co in CONVS}
+            self.gscratch = torch.zeros(P[0] * 64, dtype=bf, device=self.dev)
             G = {}
             for k in ("d0b", "d0a", "d1b", "d1a", "d2b", "d2a", "b1", "b0", "e2a", "e1a", "e0a"):
                 G[k] = torch.zeros_like(A[k])
@@ -190,6 +206,9 @@ class UNet:
             self._ck(L.sevp_nn_to_bf16(_p(w), _p(self.w16[name]), w.numel(), self.sp), "to_bf16")
             self._ck(L.sevp_nn_weight_transpose(_p(self.w16[name]), _p(self.wt16[name]), ci, co,
                                                 self.sp), "transpose")
+            if self.train:
+                self._ck(L.sevp_nn_weight_mirror(_p(self.w16[name]), _p(self.wm16[name]), ci, co,
+                                                 self.sp), "mirror")
 
     def _conv(self, name, src, src_off, src_ld, dst, dst_off, dst_ld, lvl):
         """Forward 3x3 conv + bias + ReLU on the tcgen05 tensor cores, operands
@@ -240,15 +259,14 @@ class UNet:
         H, W = self.H >> lvl, self.W >> lvl
         L = lib()
         gw, gb = self.gw[name]
-        self._ck(L.sevp_nn_conv3x3_wgrad(_p(src), src_ld, src_off, ci, _p(gout), gout_ld, gout_off, co,
-                                         _p(out), out_ld, out_off, _p(gw), _p(gb), self.B, H, W,
-                                         self.sp), name + " wgrad")
-        if dsrc is not None:
-            # data gradient: conv of the masked output gradient with the
-            # transposed, tap-mirrored weights
-            self._ck(L.sevp_nn_conv3x3(_p(gout), gout_ld, gout_off, co, _p(self.wt16[name]), None,
-                                       _p(dsrc), dsrc_ld, dsrc_off, ci, self.B, H, W, 0, _p(out),
-                                       out_ld, out_off, 1, self.sp), name + " dgrad")
+        # on the tcgen05 tensor cores: the ReLU-masked output gradient packed
+        # once, the weight gradient as a pixel-contraction GEMM, the data
+        # gradient as a forward conv with the tap-mirrored weights
+        self._ck(L.sevp_nn_conv3x3_backward_tc(
+            _p(src), src_ld, src_off, ci, _p(gout), gout_ld, gout_off, co, _p(out), out_ld, out_off,
+            _p(self.wm16[name]), _p(self.gscratch), _p(gw), _p(gb),
+            None if dsrc is None else _p(dsrc), dsrc_ld, dsrc_off, self.B, H, W, self.sp),
+            name + " backward")
 
     def backward(self, target, valid=None):
         """MSE(y, target) -> parameter gradients in self.gw (zeroed first)."""

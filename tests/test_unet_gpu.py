@@ -318,3 +318,193 @@ def test_tma_conv_wait_timeout_is_reported_and_recovers(torch_cuda):
                                 H, W, 1, None) == 0
     torch.cuda.synchronize()
     assert torch.equal(y, y2)
+
+
+@pytest.mark.parametrize("cin,cout,B,H,W,dy_ld,dy_off,dx_ld,dx_off",
+                         [(32, 32, 1, 8, 16, 32, 0, 64, 32), (64, 32, 1, 9, 150, 64, 32, 64, 0),
+                          (32, 64, 2, 5, 40, 128, 64, 32, 0), (128, 128, 1, 6, 130, 256, 128, 256, 0),
+                          (256, 128, 1, 4, 20, 128, 0, 256, 0), (128, 256, 1, 3, 24, 256, 0, 128, 0)])
+def test_conv_dgrad_tcgen05(torch_cuda, cin, cout, B, H, W, dy_ld, dy_off, dx_ld, dx_off):
+    """The data gradient on the tcgen05 tensor cores (masked output gradient
+    packed, then a TMA forward conv with the tap-mirrored weights) against
+    torch FP64 on the same BF16 values, to one BF16 rounding, and within one
+    BF16 step of the warp-MMA data gradient."""
+    torch = torch_cuda
+    import ctypes as C
+
+    from musoc_solver_b200.unet import lib
+
+    L = lib()
+    rng = np.random.default_rng(cin * 5 + cout + W)
+    P = B * H * W
+    w = _bf(torch, rng.normal(0, (2.0 / (9 * cin)) ** 0.5, (9, cin, cout)))
+    dy = _bf(torch, rng.standard_normal((P, dy_ld)))
+    mask = _bf(torch, rng.standard_normal((P, cout)))  # forward output: ReLU passes where > 0
+    wd, dyd, md = w.cuda(), dy.cuda(), mask.cuda()
+    p = lambda t: C.c_void_p(t.data_ptr())
+    wm = torch.zeros_like(wd)
+    assert L.sevp_nn_weight_mirror(p(wd), p(wm), cin, cout, None) == 0
+    scratch = torch.zeros(P * cout, dtype=torch.bfloat16, device="cuda")
+    dx = torch.full((P, dx_ld), 7.0, dtype=torch.bfloat16, device="cuda")
+    assert L.sevp_nn_conv3x3_dgrad_tc(p(dyd), dy_ld, dy_off, cout, p(md), cout, 0, p(wm), p(scratch),
+                                      p(dx), dx_ld, dx_off, cin, B, H, W, None) == 0
+    code = C.c_int(-1)
+    assert L.sevp_nn_tc_status(C.byref(code)) == 0 and code.value == 0
+    wr = w.double().reshape(3, 3, cin, cout).permute(3, 2, 0, 1)
+    gm = (dy[:, dy_off:dy_off + cout].double() * (mask.double() > 0))
+    gm = gm.reshape(B, H, W, cout).permute(0, 3, 1, 2)
+    dxr = torch.nn.grad.conv2d_input((B, cin, H, W), wr, gm, padding=1)
+    dxr = dxr.permute(0, 2, 3, 1).reshape(P, cin)
+    dg = dx.double().cpu()
+    assert (torch.norm(dg[:, dx_off:dx_off + cin] - dxr) / torch.norm(dxr)).item() < 4e-3
+    rest = torch.cat([dg[:, :dx_off], dg[:, dx_off + cin:]], dim=1)
+    assert bool((rest == 7.0).all())
+    # the warp-MMA data gradient of the same values
+    wt = torch.zeros((9, cout, cin), dtype=torch.bfloat16, device="cuda")
+    assert L.sevp_nn_weight_transpose(p(wd), p(wt), cin, cout, None) == 0
+    dx2 = torch.zeros((P, cin), dtype=torch.bfloat16, device="cuda")
+    assert L.sevp_nn_conv3x3(p(dyd), dy_ld, dy_off, cout, p(wt), None, p(dx2), cin, 0, cin, B, H, W,
+                             0, p(md), cout, 0, 1, None) == 0
+    d = (dg[:, dx_off:dx_off + cin] - dx2.double().cpu()).abs()
+    assert (d <= 2 ** -7 * dxr.abs().clamp(min=1e-3) + 1e-6).all()
+
+
+def test_unet_layers_through_the_network(torch_cuda):
+    """Every convolution of a whole forward and backward pass, checked where
+    it runs: each layer's output, weight and bias gradients and data
+    gradient against torch FP64 on the BF16 values the network actually fed
+    it (its wiring: sources, channel offsets, masks, concatenations).
+    Forward outputs and data gradients to one BF16 rounding, weight and bias
+    gradients to FP32 accumulation."""
+    torch = torch_cuda
+    import torch.nn.functional as F
+
+    from musoc_solver_b200.unet import CONVS, UNet
+
+    H, W = 32, 48
+    net = UNet(H, W, seed=5)
+    rng = np.random.default_rng(6)
+    for name, v in net.params.items():
+        v[1].copy_(torch.from_numpy(rng.normal(0, 0.05, v[1].shape).astype(np.float32)))
+    net.params["head"][0].copy_(torch.from_numpy(rng.normal(0, 0.2, 32).astype(np.float32)))
+    net.sync_weights()
+    x = np.zeros((H * W, 16), np.float32)
+    x[:, :3] = rng.standard_normal((H * W, 3))
+    net.A["x"].copy_(torch.from_numpy(x).to(torch.bfloat16))
+    t = torch.from_numpy(rng.standard_normal(H * W).astype(np.float32)).cuda()
+    dims = {n: (ci, co) for n, ci, co in CONVS}
+    errs = {}
+
+    def region(tns, off, ld, c, lvl):
+        h, w = H >> lvl, W >> lvl
+        a = tns.reshape(-1, ld)[:, off:off + c].double().cpu()
+        return a.reshape(1, h, w, c).permute(0, 3, 1, 2)
+
+    def wref(name):
+        ci, co = dims[name]
+        return net.w16[name].double().cpu().reshape(3, 3, ci, co).permute(3, 2, 0, 1)
+
+    conv_f, conv_b = net._conv, net._conv_bwd
+
+    def rel(a, b):
+        return (torch.norm(a - b) / max(torch.norm(b).item(), 1e-30)).item()
+
+    def checked_conv(name, src, src_off, src_ld, dst, dst_off, dst_ld, lvl):
+        ci, co = dims[name]
+        xr = region(src, src_off, src_ld, ci, lvl)
+        conv_f(name, src, src_off, src_ld, dst, dst_off, dst_ld, lvl)
+        torch.cuda.synchronize()
+        yr = F.relu(F.conv2d(xr, wref(name), bias=net.params[name][1].double().cpu(), padding=1))
+        errs[name + ".fwd"] = rel(region(dst, dst_off, dst_ld, co, lvl), yr)
+
+    def checked_bwd(name, src, src_off, src_ld, gout, gout_off, gout_ld, out, out_off, out_ld,
+                    dsrc, dsrc_off, dsrc_ld, lvl):
+        ci, co = dims[name]
+        xr = region(src, src_off, src_ld, ci, lvl)
+        gm = region(gout, gout_off, gout_ld, co, lvl) * (region(out, out_off, out_ld, co, lvl) > 0)
+        conv_b(name, src, src_off, src_ld, gout, gout_off, gout_ld, out, out_off, out_ld, dsrc,
+               dsrc_off, dsrc_ld, lvl)
+        torch.cuda.synchronize()
+        dwr = torch.nn.grad.conv2d_weight(xr, (co, ci, 3, 3), gm, padding=1)
+        dwr = dwr.permute(2, 3, 1, 0).reshape(9, ci, co)
+        gw, gb = net.gw[name]
+        errs[name + ".wgrad"] = rel(gw.double().cpu(), dwr)
+        errs[name + ".bgrad"] = rel(gb.double().cpu(), gm.sum(dim=(0, 2, 3)))
+        if dsrc is not None:
+            dxr = torch.nn.grad.conv2d_input(xr.shape, wref(name), gm, padding=1)
+            errs[name + ".dgrad"] = rel(region(dsrc, dsrc_off, dsrc_ld, ci, lvl), dxr)
+
+    net._conv, net._conv_bwd = checked_conv, checked_bwd
+    net.forward()
+    net.backward(t)
+    torch.cuda.synchronize()
+    kinds = {k.rsplit(".", 1)[1] for k in errs}
+    assert kinds == {"fwd", "wgrad", "bgrad", "dgrad"}
+    assert sum(k.endswith(".fwd") for k in errs) == len(CONVS)
+    assert sum(k.endswith(".wgrad") for k in errs) == len(CONVS)
+    assert sum(k.endswith(".dgrad") for k in errs) == len(CONVS) - 1
+    bad = {k: v for k, v in errs.items()
+           if v >= (4e-3 if k.endswith((".fwd", ".dgrad")) else 1e-5)}
+    assert not bad, bad
+
+
+@pytest.mark.parametrize("cin,cout,B,H,W,x_ld,x_off",
+                         [(16, 32, 1, 8, 16, 16, 0), (32, 64, 1, 9, 150, 64, 32),
+                          (64, 32, 2, 5, 40, 128, 64), (128, 128, 1, 6, 130, 256, 128),
+                          (256, 128, 1, 4, 20, 256, 0), (128, 256, 1, 3, 24, 128, 0)])
+def test_conv_wgrad_tcgen05(torch_cuda, cin, cout, B, H, W, x_ld, x_off):
+    """The weight gradient on the tcgen05 tensor cores (pixel-contraction
+    GEMM per tap, split over CTAs, FP32 atomics) against torch FP64 on the
+    same BF16 values, to FP32 accumulation; the whole backward call
+    (packing, weight, bias and data gradients) against the separate pieces."""
+    torch = torch_cuda
+    import ctypes as C
+
+    import torch.nn.functional as F  # noqa: F401
+
+    from musoc_solver_b200.unet import lib
+
+    L = lib()
+    rng = np.random.default_rng(cin * 3 + cout + W)
+    P = B * H * W
+    x = _bf(torch, rng.standard_normal((P, x_ld)))
+    g = _bf(torch, rng.standard_normal((P, cout)))
+    xd, gd = x.cuda(), g.cuda()
+    p = lambda t: C.c_void_p(t.data_ptr())
+    dw = torch.zeros((9, cin, cout), dtype=torch.float32, device="cuda")
+    assert L.sevp_nn_conv3x3_wgrad_tc(p(xd), x_ld, x_off, cin, p(gd), cout, p(dw), B, H, W,
+                                      None) == 0
+    code = C.c_int(-1)
+    assert L.sevp_nn_tc_status(C.byref(code)) == 0 and code.value == 0
+    xr = x[:, x_off:x_off + cin].double().reshape(B, H, W, cin).permute(0, 3, 1, 2)
+    gr = g.double().reshape(B, H, W, cout).permute(0, 3, 1, 2)
+    dwr = torch.nn.grad.conv2d_weight(xr, (cout, cin, 3, 3), gr, padding=1)
+    dwr = dwr.permute(2, 3, 1, 0).reshape(9, cin, cout)
+    assert (torch.norm(dw.double().cpu() - dwr) / torch.norm(dwr)).item() < 1e-5
+    # accumulates: a second call doubles it
+    assert L.sevp_nn_conv3x3_wgrad_tc(p(xd), x_ld, x_off, cin, p(gd), cout, p(dw), B, H, W,
+                                      None) == 0
+    assert (torch.norm(dw.double().cpu() - 2 * dwr) / torch.norm(2 * dwr)).item() < 1e-5
+    # the combined backward with a ReLU mask
+    mask = _bf(torch, rng.standard_normal((P, cout))).cuda()
+    w = _bf(torch, rng.normal(0, (2.0 / (9 * cin)) ** 0.5, (9, cin, cout))).cuda()
+    wm = torch.zeros_like(w)
+    assert L.sevp_nn_weight_mirror(p(w), p(wm), cin, cout, None) == 0
+    scratch = torch.zeros(P * cout, dtype=torch.bfloat16, device="cuda")
+    dw2 = torch.zeros_like(dw)
+    db2 = torch.zeros(cout, dtype=torch.float32, device="cuda")
+    dx2 = torch.zeros((P, cin), dtype=torch.bfloat16, device="cuda")
+    assert L.sevp_nn_conv3x3_backward_tc(p(xd), x_ld, x_off, cin, p(gd), cout, 0, cout, p(mask),
+                                         cout, 0, p(wm), p(scratch), p(dw2), p(db2), p(dx2), cin, 0,
+                                         B, H, W, None) == 0
+    assert L.sevp_nn_tc_status(C.byref(code)) == 0 and code.value == 0
+    gm = (g.double() * (mask.double().cpu() > 0)).reshape(B, H, W, cout).permute(0, 3, 1, 2)
+    dwm = torch.nn.grad.conv2d_weight(xr, (cout, cin, 3, 3), gm, padding=1)
+    dwm = dwm.permute(2, 3, 1, 0).reshape(9, cin, cout)
+    assert (torch.norm(dw2.double().cpu() - dwm) / torch.norm(dwm)).item() < 1e-5
+    dbm = gm.sum(dim=(0, 2, 3))
+    assert (torch.norm(db2.double().cpu() - dbm) / torch.norm(dbm)).item() < 1e-5
+    wr = w.double().cpu().reshape(3, 3, cin, cout).permute(3, 2, 0, 1)
+    dxr = torch.nn.grad.conv2d_input((B, cin, H, W), wr, gm, padding=1).permute(0, 2, 3, 1)
+    dxr = dxr.reshape(P, cin)
+    assert (torch.norm(dx2.double().cpu() - dxr) / torch.norm(dxr)).item() < 4e-3
