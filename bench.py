@@ -631,12 +631,19 @@ def run_ensemble(K, W, members=64, nx=720, ny=360, schwarz=False, inner_tol=1e-5
     out = {"workload": f"{members} members x {nx}x{ny}, +-5% depth noise, own right-hand sides, "
                        f"stacked ({e.problem.nx}x{e.problem.ny}), tiles {e.solver.tile_m}x{e.solver.tile_h}",
            "setup_seconds": setup_s}
-    arms = [("mixed", 1, False), ("fp64", 0, False)]
+    from musoc_solver_b200 import native as N
+
+    # (name, precision, Schwarz, one-launch Chebyshev iteration)
+    arms = [("mixed", 1, False, False), ("fp64", 0, False, False), ("mixed_cheb", 1, False, True)]
     if schwarz:
-        arms += [("mixed_schwarz", 1, True), ("fp64_schwarz", 0, True)]
-    for name, prec, sw in arms:
+        arms += [("mixed_schwarz", 1, True, False), ("fp64_schwarz", 0, True, False)]
+    for name, prec, sw, cheb in arms:
         if sw != bool(e.solver.schwarz_shift):
             e.solver.set_schwarz(-1 if sw else 0)
+        if cheb:
+            # spectrum bounds of the stacked operator (set-up, untimed)
+            e.solver.chebyshev_setup(b)
+        e.solver.set_method(N.METHOD_CHEB if cheb else N.METHOD_PCG)
         x = torch.zeros_like(b)
         for _ in range(W):
             e.solve(b, x=x.zero_(), precision=prec, inner_tol=inner_tol)
@@ -652,6 +659,9 @@ def run_ensemble(K, W, members=64, nx=720, ny=360, schwarz=False, inner_tol=1e-5
         rel = e.member_residuals(b, x)
         out[name] = {"value": members * K / t, "unit": "member solves/s", "ms_per_ensemble": 1e3 * t / K,
                      "iterations": res.iterations, "max_member_rel_residual": float(rel.max())}
+        if cheb:
+            out[name]["launches_per_iteration"] = 1
+            e.solver.set_method(N.METHOD_PCG)
         if name == "mixed":
             xm = x.clone()
         if name == "fp64":
@@ -805,10 +815,10 @@ def run_native(args, world, rank, local, dist):
     solver.set_method(method)
     torch.cuda.synchronize()
 
-    # per-group FP32 influence data of the inner iterations (PCG tile passes):
+    # per-group FP32 influence data of the inner iterations (tile passes):
     # growth limit measured (untimed) on the same warm-start step, unless given
     mix_limit, mix_table = 0.0, None
-    if args.influence_fp32 == "auto" and not args.precond_fp32 and method == N.METHOD_PCG:
+    if args.influence_fp32 == "auto" and not args.precond_fp32:
         mix_table, xw = {}, torch.zeros_like(eta[0])
         for lim in (0.0, 1e3, 1e4, 1e5, 1e6):
             solver.set_influence_fp32(lim)

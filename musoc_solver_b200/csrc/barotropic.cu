@@ -89,26 +89,42 @@ __device__ __forceinline__ float face_corr(double xr, double xl, float metric) {
   return __double2float_rn(-__dmul_rn(__dsub_rn(xr, xl), (double)metric));
 }
 
-// f[o + l * stride] += c * m[o + l * stride] for the n layers below the top
-// (the land mask of each layer), kFsLayerBatch layers loaded at a time.
-__device__ __forceinline__ void correct_layers(float *f, const int16_t *m, size_t o,
-                                               size_t stride, int n, float c) {
+// The layers below the top of one U face and one V face:
+// f[o + l so] += cf * m[o + l so] (when af) and g[p + l sp] += cg *
+// mg[p + l sp] (when ag) for l < nl, with each layer's land mask;
+// kFsLayerBatch layers of both faces are loaded before the first is used.
+__device__ __forceinline__ void correct_layers(float *f, const int16_t *m, size_t o, size_t so,
+                                               bool af, float cf, float *g, const int16_t *mg,
+                                               size_t p, size_t sp, bool ag, float cg, int nl) {
   int l = 0;
-  for (; l + kFsLayerBatch <= n; l += kFsLayerBatch) {
-    float fv[kFsLayerBatch];
-    int16_t mv[kFsLayerBatch];
+  for (; l + kFsLayerBatch <= nl; l += kFsLayerBatch) {
+    float fv[kFsLayerBatch], gv[kFsLayerBatch];
+    int16_t fm[kFsLayerBatch], gm[kFsLayerBatch];
 #pragma unroll
     for (int q = 0; q < kFsLayerBatch; ++q) {
-      fv[q] = f[o + (size_t)(l + q) * stride];
-      mv[q] = m[o + (size_t)(l + q) * stride];
+      if (af) {
+        fv[q] = f[o + (size_t)(l + q) * so];
+        fm[q] = m[o + (size_t)(l + q) * so];
+      }
+      if (ag) {
+        gv[q] = g[p + (size_t)(l + q) * sp];
+        gm[q] = mg[p + (size_t)(l + q) * sp];
+      }
     }
 #pragma unroll
-    for (int q = 0; q < kFsLayerBatch; ++q)
-      f[o + (size_t)(l + q) * stride] = __fadd_rn(fv[q], __fmul_rn(c, (float)mv[q]));
+    for (int q = 0; q < kFsLayerBatch; ++q) {
+      if (af) f[o + (size_t)(l + q) * so] = __fadd_rn(fv[q], __fmul_rn(cf, (float)fm[q]));
+      if (ag) g[p + (size_t)(l + q) * sp] = __fadd_rn(gv[q], __fmul_rn(cg, (float)gm[q]));
+    }
   }
-  for (; l < n; ++l)
-    f[o + (size_t)l * stride] = __fadd_rn(f[o + (size_t)l * stride],
-                                          __fmul_rn(c, (float)m[o + (size_t)l * stride]));
+  for (; l < nl; ++l) {
+    if (af)
+      f[o + (size_t)l * so] =
+          __fadd_rn(f[o + (size_t)l * so], __fmul_rn(cf, (float)m[o + (size_t)l * so]));
+    if (ag)
+      g[p + (size_t)l * sp] =
+          __fadd_rn(g[p + (size_t)l * sp], __fmul_rn(cg, (float)mg[p + (size_t)l * sp]));
+  }
 }
 
 // one thread per (I, J): P0 at the cell, the U face east of it, the V face
@@ -128,31 +144,33 @@ __global__ void k_fs_correct(int i0, int j0, int k0, const double *x, float odt,
     const size_t c = IDX2(i, j);
     p0[c] = __double2float_rn(__dadd_rn((double)p0[c], __dmul_rn((double)odt, X(i, j))));
   }
-  if (j >= 2 && j <= j1 && i <= i1) {  // U face (I, J), I = 1 .. I1
-    float c = 0.f;
+  const bool fu = j >= 2 && j <= j1 && i <= i1;  // U face (I, J), I = 1 .. I1
+  const bool fv = i >= 2 && i <= i1 && j <= j1;  // V face (I, J), J = 1 .. J1
+  float cu = 0.f, cv = 0.f;
+  if (fu) {
     if (i >= 2 && i <= i2)
-      c = face_corr(X(i + 1, j), X(i, j), odx[j - 1]);
+      cu = face_corr(X(i + 1, j), X(i, j), odx[j - 1]);
     else if (periodic)
-      c = face_corr(X(2, j), X(i1, j), odx[j - 1]);
+      cu = face_corr(X(2, j), X(i1, j), odx[j - 1]);
     const size_t o = IDX2(i, j);
-    s1[o] = c;
-    s3[o] = __fadd_rn(s3[o], c);
-    const float top = __fadd_rn(u[IDX3(j0, i, j, 1)], c);
+    s1[o] = cu;
+    s3[o] = __fadd_rn(s3[o], cu);
+    const float top = __fadd_rn(u[IDX3(j0, i, j, 1)], cu);
     u[IDX3(j0, i, j, 1)] = top;
-    correct_layers(u, iu, IDX3(j0, i, j, 2), plane, k1 - 1, c);
     if (i >= 2 && i <= i2) land = __fmul_rn((float)(1 - iu0[o]), fabsf(top));
   }
-  if (i >= 2 && i <= i1 && j <= j1) {  // V face (I, J), J = 1 .. J1
-    float c = 0.f;
-    if (j >= 2 && j <= j2) c = face_corr(X(i, j + 1), X(i, j), odyv[j - 1]);
+  if (fv) {
+    if (j >= 2 && j <= j2) cv = face_corr(X(i, j + 1), X(i, j), odyv[j - 1]);
     const size_t o = IDX2(i, j);
-    s2[o] = c;
-    s4[o] = __fadd_rn(s4[o], c);
-    const float top = __fadd_rn(v[IDX3(j0 - 1, i, j, 1)], c);
+    s2[o] = cv;
+    s4[o] = __fadd_rn(s4[o], cv);
+    const float top = __fadd_rn(v[IDX3(j0 - 1, i, j, 1)], cv);
     v[IDX3(j0 - 1, i, j, 1)] = top;
-    correct_layers(v, iv, IDX3(j0 - 1, i, j, 2), (size_t)i0 * (j0 - 1), k1 - 1, c);
     if (j >= 2 && j <= j2) land = fmaxf(land, __fmul_rn((float)(1 - iv0[o]), fabsf(top)));
   }
+  // the layers below the top, both faces at once
+  correct_layers(u, iu, fu ? IDX3(j0, i, j, 2) : 0, plane, fu, cu, v, iv,
+                 fv ? IDX3(j0 - 1, i, j, 2) : 0, (size_t)i0 * (j0 - 1), fv, cv, k1 - 1);
   // non-negative floats order like their bit patterns
   for (int o = 16; o > 0; o >>= 1) land = fmaxf(land, __shfl_xor_sync(0xffffffffu, land, o));
   if ((threadIdx.x & 31) == 0 && land > 0.f) atomicMax((int *)vmax, __float_as_int(land));

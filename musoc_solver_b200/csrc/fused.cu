@@ -94,7 +94,7 @@ __global__ void __launch_bounds__(kTileWarps * 32, 2)
     const bool active = n < mw;
     const int j0 = b * tg.th, hh = tile_height(tg, b), nb = tg.grp_nb[(size_t)b * tg.txg + grp];
     const int i = tile_col(tg, a, n);
-    const MT *mt = mats + (mw > 0 ? tg.moff[(size_t)b * tg.tx + a] : 0);
+    const MT *mt = tile_mats(mats, tg, b, grp, a, mw);
     const size_t idx0 = (size_t)j0 * nx + i;
 
     // west / east neighbours: a shuffle from the lane holding that column,
@@ -209,6 +209,8 @@ int launch_h(const ChebLaunch<V> &L) {
 template <typename V>
 int cheb_launch(const ChebLaunch<V> &L) {
   if (L.tg.hmax > kChebMaxRows) return SEVP_BAD_ARG;
+  if (L.mats_fp32 == 2)  // precision per warp group (MixMat)
+    return L.sym ? launch_h<V, MixMat, true>(L) : launch_h<V, MixMat, false>(L);
   if (L.mats_fp32)
     return L.sym ? launch_h<V, float, true>(L) : launch_h<V, float, false>(L);
   return L.sym ? launch_h<V, double, true>(L) : launch_h<V, double, false>(L);

@@ -491,11 +491,8 @@ __global__ void __launch_bounds__(kTileWarps * 32, 2)
   if ((DOTS || UPDATE) && st->done) return;
   constexpr bool kChain = sizeof(V) == 4;
   __shared__ double dv_all[kTileWarps * 32];
-  // per warp: the influence matrices of its group (tiles up to 16 wide)
-  __shared__ __align__(16) double mslot_all[kTileWarps * kGroupMatSlots];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   double *dv = dv_all + wib * 32;
-  double *mslot = mslot_all + wib * kGroupMatSlots;
   double acc_rz = 0.0, acc_rr = 0.0;
   double alpha = 0.0;
   if (UPDATE) alpha = st->alpha;
@@ -512,48 +509,35 @@ __global__ void __launch_bounds__(kTileWarps * 32, 2)
     const int i = tile_col(tg, a, n);
     const MT *mt = tile_mats(mats, tg, b, grp, a, mw);
     const size_t idx0 = (size_t)j0 * nx + i;
-    // a full-height single-sub-block group (the common case) copies its
-    // matrices to shared memory first: the copy overlaps the row loads and
-    // the forward sweep instead of following them
-    const bool pre = nb == 1 && hh == HM && tg.wseg * tg.wseg * tg.tpw <= kGroupMatSlots;
-    const MT *mts = pre ? prefetch_group_mats(mats, tg, b, grp, seg, lane, mslot) : mt;
 
-    // ---- all loads of the task, and the fused update x += alpha p,
-    //      r -= alpha q (its stores leave before the march)
-    V rr[HM];
+    // ---- all loads of the task
+    V rr[HM], xx[UPDATE ? HM : 1], pp[UPDATE ? HM : 1], qq[UPDATE ? HM : 1];
     float cc_[HM], ce_[HM], cn_[HM], cw_[SYM ? 1 : HM], cs_[SYM ? 1 : HM];
-    {
-      V xx[UPDATE ? HM : 1], pp[UPDATE ? HM : 1], qq[UPDATE ? HM : 1];
 #pragma unroll
-      for (int k = 0; k < HM; ++k) {
-        const bool ok = active && k < hh;
-        const size_t id = ok ? idx0 + (size_t)k * nx : 0;
-        rr[k] = ok ? r[id] : V(0);
-        if (UPDATE) {
-          xx[k] = ok ? x[id] : V(0);
-          pp[k] = ok ? p[id] : V(0);
-          qq[k] = ok ? q[id] : V(0);
-        }
-      }
-      load_task_coeffs<SYM, HM>(c, idx0, nx, hh, active, cc_, ce_, cn_, cw_, cs_);
+    for (int k = 0; k < HM; ++k) {
+      const bool ok = active && k < hh;
+      const size_t id = ok ? idx0 + (size_t)k * nx : 0;
+      rr[k] = ok ? r[id] : V(0);
       if (UPDATE) {
-#pragma unroll
-        for (int k = 0; k < HM; ++k) {
-          if (active && k < hh) {
-            const size_t idx = idx0 + (size_t)k * nx;
-            const V xn = xx[k] + (V)alpha * pp[k];
-            const V rn = rr[k] - (V)alpha * qq[k];
-            x[idx] = xn;
-            r[idx] = rn;
-            rr[k] = rn;
-          }
-        }
+        xx[k] = ok ? x[id] : V(0);
+        pp[k] = ok ? p[id] : V(0);
+        qq[k] = ok ? q[id] : V(0);
       }
     }
+    load_task_coeffs<SYM, HM>(c, idx0, nx, hh, active, cc_, ce_, cn_, cw_, cs_);
 
-    // row k's right-hand side: the (updated) residual
+    // row k's right-hand side: the residual, after the fused update
+    // x += alpha p, r -= alpha q
     auto rhs = [&](int k) -> double {
       if (!active) return 0.0;
+      if (UPDATE) {
+        const size_t idx = idx0 + (size_t)k * nx;
+        const V xn = xx[k] + (V)alpha * pp[k];
+        const V rn = rr[k] - (V)alpha * qq[k];
+        x[idx] = xn;
+        r[idx] = rn;
+        rr[k] = rn;
+      }
       const double rv = (double)rr[k];
       acc_rr += rv * rv;
       return rv;
@@ -563,13 +547,8 @@ __global__ void __launch_bounds__(kTileWarps * 32, 2)
       z[idx0 + (size_t)k * nx] = zv;
       if (DOTS) acc_rz += (double)rr[k] * (double)zv;
     };
-    if (pre)
-      march_task_full<MT, SYM, kChain, HM, UPDATE && !DOTS, true>(
-          cc_, ce_, cn_, cw_, cs_, n, mw, active, lane, segbase, dv, mts, rhs, emit);
-    else
-      march_task_regs<MT, SYM, kChain, HM, UPDATE && !DOTS>(cc_, ce_, cn_, cw_, cs_, hh, nb, n,
-                                                            mw, active, lane, segbase, dv, mt, rhs,
-                                                            emit);
+    march_task_regs<MT, SYM, kChain, HM, UPDATE && !DOTS>(cc_, ce_, cn_, cw_, cs_, hh, nb, n, mw,
+                                                          active, lane, segbase, dv, mt, rhs, emit);
   }
   if (DOTS) {
     double v2[2] = {acc_rz, acc_rr};
@@ -2040,8 +2019,11 @@ static int pcg_loop(sevp_ctx *ctx, V *x, V *r, V *z, V *p0, V *p1, V *q, int che
 static int launch_cheb_k(sevp_ctx *ctx, const float *din, float *dout, float *x, float *r) {
   const Tiling &T = ctx->ta;
   const bool m32 = ctx->infl32_active && T.d_mats32;
-  ChebLaunch<float> L{ctx->sym, m32 ? 1 : 0, T.tg, T.c, ctx->periodic,
-                      m32 ? (const void *)T.d_mats32 : (const void *)T.d_mats, din, dout, x, r,
+  const bool mix = !m32 && T.d_matsmix;
+  ChebLaunch<float> L{ctx->sym, m32 ? 1 : (mix ? 2 : 0), T.tg, T.c, ctx->periodic,
+                      m32 ? (const void *)T.d_mats32
+                          : (mix ? (const void *)T.d_matsmix : (const void *)T.d_mats),
+                      din, dout, x, r,
                       ctx->st, ctx->partials, ctx->tickets + 7, ctx->stream};
   ProfScope ps(ctx, 0);
   int s = cheb_launch<float>(L);
@@ -2074,7 +2056,8 @@ static int cheb_inner(sevp_ctx *ctx, int check_every, int *iters_out) {
     return SEVP_OK;
   };
   const void *const key[5] = {(const void *)ctx->d32, (const void *)ctx->p32[0],
-                              (const void *)(ctx->infl32_active ? ctx->ta.d_mats32 : nullptr),
+                              ctx->infl32_active ? (const void *)ctx->ta.d_mats32
+                                                 : (const void *)ctx->ta.d_matsmix,
                               nullptr, (const void *)(uintptr_t)SEVP_METHOD_CHEB};
   int s = graph_loop(ctx, true, key, check_every, check_every, interval);
   if (s) return s;

@@ -106,9 +106,6 @@ constexpr int kTileWarps = 8;
 // FP32-vector tiles up to this height use k_tile_short (measured faster
 // there; the FP64 kernel and taller tiles keep k_tile_apply)
 constexpr int kShortTileRows = 6;
-// 8-byte shared-memory slots per warp for its group's influence matrices
-// (k_tile_short): two 16 x 16 tiles, or four 8 x 8
-constexpr int kGroupMatSlots = 512;
 
 
 // Shared memory per warp: the tile's rows of z (FP64 marching state, 32
@@ -131,20 +128,13 @@ constexpr uintptr_t kMixF32Tag = 4;
 
 // out(n) = sum_k dv[seg + k] * M[k * mw + n].  All loads of the column are
 // issued before the first multiply-add, so a mat-vec costs one memory round
-// trip instead of one per group of rows.  MT is the stored matrix type; SM:
-// M points to a shared-memory copy (plain loads instead of the read-only
-// global path).
-template <int WMAX, typename MT, bool SM>
+// trip instead of one per group of rows.  MT is the stored matrix type.
+template <int WMAX, typename MT>
 __device__ __forceinline__ double seg_matvec_w(const double *dv, int segbase, const MT *M, int mw,
                                                int n) {
   MT m[WMAX];
 #pragma unroll
-  for (int k = 0; k < WMAX; ++k) {
-    if constexpr (SM)
-      m[k] = (k < mw) ? M[(size_t)k * mw + n] : MT(0);
-    else
-      m[k] = (k < mw) ? __ldg(M + (size_t)k * mw + n) : MT(0);
-  }
+  for (int k = 0; k < WMAX; ++k) m[k] = (k < mw) ? __ldg(M + (size_t)k * mw + n) : MT(0);
   if (sizeof(MT) == 4) {
     // FP32 influence data: multiply-add in FP32 (the mixed-precision mode)
     float s = 0.f;
@@ -159,24 +149,24 @@ __device__ __forceinline__ double seg_matvec_w(const double *dv, int segbase, co
     if (k < mw) s += dv[segbase + k] * (double)m[k];
   return s;
 }
-template <typename MT, bool SM>
+template <typename MT>
 __device__ __forceinline__ double seg_matvec_t(const double *dv, int segbase, const MT *M, int mw,
                                                int n) {
-  if (mw <= 8) return seg_matvec_w<8, MT, SM>(dv, segbase, M, mw, n);
-  if (mw <= 16) return seg_matvec_w<16, MT, SM>(dv, segbase, M, mw, n);
-  return seg_matvec_w<32, MT, SM>(dv, segbase, M, mw, n);
+  if (mw <= 8) return seg_matvec_w<8, MT>(dv, segbase, M, mw, n);
+  if (mw <= 16) return seg_matvec_w<16, MT>(dv, segbase, M, mw, n);
+  return seg_matvec_w<32, MT>(dv, segbase, M, mw, n);
 }
-template <typename MT, bool SM = false>
+template <typename MT>
 __device__ __forceinline__ double seg_matvec(const double *dv, int segbase, const MT *M, int mw,
                                              int n) {
   if constexpr (std::is_same<MT, MixMat>::value) {
     const uintptr_t u = reinterpret_cast<uintptr_t>(M);
     if (u & kMixF32Tag)
-      return seg_matvec_t<float, SM>(dv, segbase, reinterpret_cast<const float *>(u - kMixF32Tag),
-                                     mw, n);
-    return seg_matvec_t<double, SM>(dv, segbase, reinterpret_cast<const double *>(u), mw, n);
+      return seg_matvec_t<float>(dv, segbase, reinterpret_cast<const float *>(u - kMixF32Tag), mw,
+                                 n);
+    return seg_matvec_t<double>(dv, segbase, reinterpret_cast<const double *>(u), mw, n);
   } else {
-    return seg_matvec_t<MT, SM>(dv, segbase, M, mw, n);
+    return seg_matvec_t<MT>(dv, segbase, M, mw, n);
   }
 }
 
@@ -192,40 +182,6 @@ __device__ __forceinline__ void cp_async_elem(void *smem, const void *gmem, bool
   else
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dst), "l"(gmem), "r"(n)
                  : "memory");
-}
-
-// Influence matrices of a warp group of single-sub-block tiles copied to
-// shared memory: tile slot sg of the group (sg < tpw) gets its mw * mw
-// elements at slots + sg * wseg * wseg (8-byte slots; FP32 data fills the
-// first half), every lane issuing cp.async for elements lane, lane + 32, ...
-// of each tile.  Returns this lane's tile's copy (tagged like tile_mats for
-// MixMat).  The caller waits (cp.async.wait_all) and syncs the warp before
-// reading it; march_task_full<..., SM = true> does.
-template <typename MT>
-__device__ __forceinline__ const MT *prefetch_group_mats(const MT *mats, const TileGeom &tg, int b,
-                                                         int grp, int seg, int lane,
-                                                         double *slots) {
-  bool f32 = sizeof(MT) == 4;
-  if constexpr (std::is_same<MT, MixMat>::value)
-    f32 = tg.grp_f32 && tg.grp_f32[(size_t)b * tg.txg + grp];
-  const int ss = tg.wseg * tg.wseg;
-  for (int sg = 0; sg < tg.tpw; ++sg) {
-    const int a = grp * tg.tpw + sg;
-    if (a >= tg.tx) break;
-    const int cnt = tile_width(tg, a) * tile_width(tg, a);
-    const char *src = reinterpret_cast<const char *>(mats + tg.moff[(size_t)b * tg.tx + a]);
-    char *dst = reinterpret_cast<char *>(slots + (size_t)sg * ss);
-    if (f32) {
-      for (int e = lane; e < cnt; e += 32) cp_async_elem<4>(dst + 4 * e, src + 4 * e, true);
-    } else {
-      for (int e = lane; e < cnt; e += 32) cp_async_elem<8>(dst + 8 * e, src + 8 * e, true);
-    }
-  }
-  const double *mine = slots + (size_t)seg * ss;
-  if constexpr (std::is_same<MT, MixMat>::value)
-    return reinterpret_cast<const MT *>(reinterpret_cast<uintptr_t>(mine) + (f32 ? kMixF32Tag : 0));
-  else
-    return reinterpret_cast<const MT *>(mine);
 }
 
 // Influence data of tile (a, b) of warp group grp (mw: the tile's width;
@@ -298,11 +254,8 @@ struct TileFin {
 // code, without the sub-block bookkeeping.  RCP: the FP32-vector march
 // keeps the reciprocals of AT from the forward sweep for the backward sweep
 // (the same rows) instead of forming them again; chosen per kernel, since
-// the registers it takes pay off in some and not in others.  SM: mt is the
-// shared-memory copy that prefetch_group_mats started; the copy is waited
-// for just before the mat-vec, so it overlaps the forward sweep.
-template <typename MT, bool SYM, bool kChain, int HM, bool RCP, bool SM = false, class Rhs,
-          class Emit>
+// the registers it takes pay off in some and not in others.
+template <typename MT, bool SYM, bool kChain, int HM, bool RCP, class Rhs, class Emit>
 __device__ __forceinline__ void march_task_full(const float (&cc_)[HM], const float (&ce_)[HM],
                                                 const float (&cn_)[HM],
                                                 const float (&cw_)[SYM ? 1 : HM],
@@ -354,9 +307,8 @@ __device__ __forceinline__ void march_task_full(const float (&cc_)[HM], const fl
     }
   }
   dv[lane] = rho;
-  if constexpr (SM) asm volatile("cp.async.wait_all;\n" ::: "memory");
   __syncwarp();
-  const double v = active ? seg_matvec<MT, SM>(dv, segbase, mt, mw, n) : 0.0;
+  const double v = active ? seg_matvec<MT>(dv, segbase, mt, mw, n) : 0.0;
   __syncwarp();
   zs[0] += v;
   double hb = 0.0, hc = v;
@@ -577,7 +529,7 @@ constexpr int kChebMaxRows = 8;  // tile rows held in registers
 template <typename V>
 struct ChebLaunch {
   int sym;            // the operator is symmetric: 3-plane reads
-  int mats_fp32;      // mats holds FP32 influence data
+  int mats_fp32;      // mats holds FP32 influence data (1), or MixMat data (2)
   TileGeom tg;
   Coeffs c;
   int periodic;

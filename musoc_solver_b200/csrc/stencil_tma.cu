@@ -5,7 +5,7 @@
 // arithmetic, predicated loads and shuffles (about 90 instructions per grid
 // point for 28 bytes moved).  Here the tensor memory accelerator moves every
 // array of a 64 x 32 tile, with its halo, into shared memory: one thread
-// issues a handful of 2-D bulk copies per tile, three tiles are in flight
+// issues a handful of 2-D bulk copies per tile, up to four tiles are in flight
 // per CTA (an mbarrier per stage counts their bytes), and the 256 threads
 // then read the five-point neighbourhoods from shared memory.
 //
@@ -334,7 +334,11 @@ const Maps *tensor_maps(const PassALaunch<V> &L) {
 template <typename V, bool SYM>
 int launch(const PassALaunch<V> &L) {
   using S = Stage<V, SYM>;
-  constexpr int kStages = 3 * S::kBytes + 128 <= 220 * 1024 ? 3 : 2;
+  // as many stages as fit (four for FP32 vectors, three for FP64): with one
+  // CTA per SM the copies in flight have to cover the memory latency
+  constexpr int kStages = 4 * S::kBytes + 128 <= 220 * 1024
+                              ? 4
+                              : (3 * S::kBytes + 128 <= 220 * 1024 ? 3 : 2);
   const Maps *mp = tensor_maps<V, SYM>(L);
   if (!mp) {
     sevp_internal_set_message("pass A: tensor map encoding failed");

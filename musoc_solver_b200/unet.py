@@ -325,6 +325,9 @@ class UNet:
         for name, ci, co in CONVS:
             self._ck(lib().sevp_nn_weight_transpose(_p(self.w16[name]), _p(self.wt16[name]), ci, co,
                                                     self.sp), "transpose")
+            # the data gradient's tap-mirrored copy follows the new weights
+            self._ck(lib().sevp_nn_weight_mirror(_p(self.w16[name]), _p(self.wm16[name]), ci, co,
+                                                 self.sp), "mirror")
 
     # ---------------------------------------------------------- weights io
     def state(self) -> dict:

@@ -97,3 +97,29 @@ def test_partial_fp32_groups_solve_matches_oracle(torch_cuda, oracle):
     pc = oracle.TilePC(p, 16, 6, tile_nb=s.tile_nb)
     xo, _, _ = pc.pcg(p.b, tol=1e-12)
     assert np.abs(x - xo).max() <= 1e-8 * np.abs(xo).max()
+
+
+def test_chebyshev_reads_the_chosen_precision(torch_cuda):
+    """The one-launch Chebyshev iteration with every group FP32 equals its
+    all-FP32 (precond_fp32) solve bit for bit, and with a splitting limit
+    still reaches the tolerance."""
+    torch = torch_cuda
+    from musoc_solver_b200 import native as N
+    from musoc_solver_b200.solver import SevpSolver
+
+    p = P.global_grid(240, 120, seed=16)
+    b = torch.from_numpy(p.b).cuda()
+    out = {}
+    for key, kw, lim in (("all32", dict(precond_fp32=True), None), ("mix_all", {}, 1e300),
+                         ("mix_part", {}, 1e4)):
+        s = SevpSolver(p, tile_m=16, tile_h=6, **kw)
+        s.chebyshev_setup(b)
+        s.set_method(N.METHOD_CHEB)
+        if lim is not None:
+            s.set_influence_fp32(lim)
+        out[key] = _solve(s, b)
+    assert out["mix_all"][1].iterations == out["all32"][1].iterations
+    assert np.array_equal(out["mix_all"][0], out["all32"][0])
+    x = out["mix_part"][0]
+    res = np.linalg.norm(p.b - P.apply_operator(p, x)) / np.linalg.norm(p.b)
+    assert res <= 2e-12

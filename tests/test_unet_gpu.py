@@ -392,6 +392,12 @@ def test_unet_layers_through_the_network(torch_cuda):
     x[:, :3] = rng.standard_normal((H * W, 3))
     net.A["x"].copy_(torch.from_numpy(x).to(torch.bfloat16))
     t = torch.from_numpy(rng.standard_normal(H * W).astype(np.float32)).cuda()
+    # one training step first: the checked pass runs on updated weights (and
+    # their derived copies, which the data gradient reads)
+    net.forward()
+    net.backward(t)
+    net.adam_step(lr=1e-2)
+    torch.cuda.synchronize()
     dims = {n: (ci, co) for n, ci, co in CONVS}
     errs = {}
 
