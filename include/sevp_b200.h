@@ -60,9 +60,12 @@ int sevp_get_periodic_we(void);
  * (enable != 0), keyed by host address and size: a model that reads the EVP
  * file once and calls REP1 every step (M/fs_GLOBAL.f90:1852) then copies
  * only F, X, H and the DUM workspaces per call.  The caller promises that
- * those arrays keep their values while caching is on; sevp_dropin_cache(0)
- * frees the copies and turns caching off (the default).  Not part of the
- * reference interface. */
+ * those arrays keep their values while caching is on.  While it is on, the
+ * device blocks of every drop-in's per-call copies (workspaces, X, F, the
+ * Krylov drop-ins' vectors) are also kept and reused, so repeated calls make
+ * no cudaMalloc / cudaFree.  sevp_dropin_cache(0) frees the copies and the
+ * blocks and turns caching off (the default).  Not part of the reference
+ * interface. */
 int sevp_dropin_cache(int enable);
 
 /* ------------------------------------------- Fortran-compatible drop-ins */

@@ -18,22 +18,77 @@ using namespace sevp;
 namespace {
 thread_local int g_status = SEVP_OK;
 int g_periodic_we = 1;
+bool g_cache_on = false;
 
-// Device copy of a host span, freed on scope exit.
+// Device blocks of finished calls, kept for the next calls while caching is
+// on (sevp_dropin_cache), so that a call's workspaces cost no cudaMalloc /
+// cudaFree: (bytes, device, block).  A block goes back to the pool when its
+// call ends; before blocks are handed out again the device is synchronised
+// once (a call that failed half-way may have left a kernel running).
+struct PoolBlock {
+  size_t bytes;
+  int device;
+  void *p;
+};
+std::vector<PoolBlock> g_pool;
+bool g_pool_released = false;
+
+void *pool_get(size_t bytes, size_t *cap) {
+  int device = 0;
+  if (cudaGetDevice(&device) != cudaSuccess) return nullptr;
+  if (g_pool_released) {
+    if (cudaDeviceSynchronize() != cudaSuccess) return nullptr;
+    g_pool_released = false;
+  }
+  int best = -1;
+  for (size_t k = 0; k < g_pool.size(); ++k)
+    if (g_pool[k].device == device && g_pool[k].bytes >= bytes &&
+        (best < 0 || g_pool[k].bytes < g_pool[(size_t)best].bytes))
+      best = (int)k;
+  if (best >= 0) {
+    void *p = g_pool[(size_t)best].p;
+    *cap = g_pool[(size_t)best].bytes;
+    g_pool.erase(g_pool.begin() + best);
+    return p;
+  }
+  void *p = nullptr;
+  if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+  *cap = bytes;
+  return p;
+}
+void pool_put(void *p, size_t cap) {
+  int device = 0;
+  if (cudaGetDevice(&device) != cudaSuccess) return;
+  g_pool.push_back(PoolBlock{cap, device, p});
+  g_pool_released = true;
+}
+
+// Device copy of a host span, released on scope exit (to the pool while
+// caching is on, else freed).
 template <typename T>
 struct DBuf {
   T *d = nullptr;
   size_t n = 0;
+  size_t cap = 0;  // bytes of a pooled block (0: owned, freed on exit)
   int err = 0;
   explicit DBuf(size_t count) : n(count) {
-    if (cudaMalloc((void **)&d, std::max<size_t>(count, 1) * sizeof(T)) != cudaSuccess) err = 1, d = nullptr;
+    const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+    if (g_cache_on) {
+      d = static_cast<T *>(pool_get(bytes, &cap));
+      if (!d) err = 1, cap = 0;
+    } else if (cudaMalloc((void **)&d, bytes) != cudaSuccess) {
+      err = 1, d = nullptr;
+    }
   }
   DBuf(const T *h, size_t count) : DBuf(count) {
     if (!err && h && count && cudaMemcpy(d, h, count * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess)
       err = 1;
   }
   ~DBuf() {
-    if (d) cudaFree(d);
+    if (d && cap)
+      pool_put(d, cap);
+    else if (d)
+      cudaFree(d);
   }
   int zero() { return (!err && cudaMemset(d, 0, std::max<size_t>(n, 1) * sizeof(T)) == cudaSuccess) ? 0 : 1; }
   int to_host(T *h) const {
@@ -55,7 +110,6 @@ struct CacheEntry {
   void *dev;
 };
 std::vector<CacheEntry> g_cache;
-bool g_cache_on = false;
 
 const void *cached_upload(const void *host, size_t bytes, int *err) {
   int device = 0;
@@ -205,6 +259,8 @@ void pre_dropin(const float *ax, const float *ay, const float *bb, const float *
 
 }  // namespace
 
+bool sevp::dropin_cache_on() { return g_cache_on; }
+
 void sevp_internal_set_status(int s) { g_status = s; }
 
 extern "C" {
@@ -214,6 +270,10 @@ int sevp_last_status(void) { return g_status; }
 int sevp_dropin_cache(int enable) {
   for (const CacheEntry &e : g_cache) cudaFree(e.dev);
   g_cache.clear();
+  release_kept_work();
+  for (const PoolBlock &b : g_pool) cudaFree(b.p);
+  g_pool.clear();
+  g_pool_released = false;
   g_cache_on = enable != 0;
   return SEVP_OK;
 }

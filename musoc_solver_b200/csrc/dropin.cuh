@@ -5,6 +5,11 @@
 
 namespace sevp {
 
+// The drop-in cache (sevp_dropin_cache, capi.cu): whether it is on, and the
+// release of the Krylov work buffers kept while it is (krylov.cu).
+bool dropin_cache_on();
+void release_kept_work();
+
 // Arguments of the marching solve; every pointer is a device pointer and
 // every array keeps the reference's column-major layout and leading
 // dimension (see M/sevp.f90:11-438).

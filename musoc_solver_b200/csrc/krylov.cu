@@ -12,6 +12,7 @@
 // Fortran); dot products are a fixed-order parallel tree (deterministic, but
 // rounded differently from the serial Fortran sum).
 #include <cmath>
+#include <memory>
 #include <vector>
 
 #include "common.cuh"
@@ -172,6 +173,158 @@ __global__ void k_bicg_xr(double *x, double *r, const double *ph, const double *
   }
 }
 
+// ---------------------------------------------- one-CTA BiCGSTAB (small grids)
+// The whole restarted BiCGSTAB of dev_bicgstab below in ONE thread block:
+// on the reference's own grid (182 x 92) the multi-launch loop spends its
+// time in some 16 launches and a host round trip per iteration, while each
+// pass touches only 130 KB.  Here 1024 threads run every pass between block
+// barriers and keep the scalars in shared memory; the arithmetic of every
+// element-wise step is that of the kernels above (k_sqprod, k_rhs_minus,
+// k_bicg_*), the control flow that of the host loop (restart quirk and
+// stopping tests included).  Dot products are a fixed-order block tree
+// (deterministic; rounded differently from the multi-CTA tree).
+constexpr int kCtaThreads = 1024;
+// padded grids up to this many points run dev_bicgstab in one thread block
+// (the vectors stay in L2); larger ones run the multi-launch loop
+constexpr size_t kCtaMaxPoints = (size_t)1 << 17;
+
+struct BicgVecs {
+  double *r, *rh, *p, *v, *s, *t, *ph, *sh;
+};
+
+__device__ double cta_dot(const double *a, const double *b, int i2, int j2, double *red,
+                          double *out) {
+  const int i0 = i2 + 2;
+  const size_t n = (size_t)i2 * j2;
+  double v[1] = {0.0};
+  for (size_t e = threadIdx.x; e < n; e += blockDim.x) {
+    const int i = 2 + (int)(e % i2), j = 2 + (int)(e / i2);
+    v[0] += a[IXK(i0, i, j)] * b[IXK(i0, i, j)];
+  }
+  block_sum<1>(v, red);
+  if (threadIdx.x == 0) *out = v[0];
+  __syncthreads();
+  return *out;
+}
+__device__ void cta_apply(const float *al, const float *ab, const float *ac, const float *ar,
+                          const float *at, const double *x, double *r, int i2, int j2) {
+  const int i0 = i2 + 2;
+  const size_t n = (size_t)i2 * j2;
+  for (size_t e = threadIdx.x; e < n; e += blockDim.x) {
+    const int i = 1 + (int)(e % i2), j = 1 + (int)(e / i2);
+    const size_t c = IXK(i2, i, j);
+    double t = mul((double)ab[c], x[IXK(i0, i + 1, j)]);
+    t = add(t, mul((double)al[c], x[IXK(i0, i, j + 1)]));
+    t = add(t, mul((double)ac[c], x[IXK(i0, i + 1, j + 1)]));
+    t = add(t, mul((double)ar[c], x[IXK(i0, i + 2, j + 1)]));
+    t = add(t, mul((double)at[c], x[IXK(i0, i + 1, j + 2)]));
+    r[IXK(i0, i + 1, j + 1)] = t;
+  }
+  __syncthreads();
+}
+__device__ void cta_boundary(double *x, int i2, int j2, int periodic) {
+  if (!periodic) return;
+  const int i0 = i2 + 2;
+  for (int j = 2 + threadIdx.x; j <= j2 + 1; j += blockDim.x) {
+    x[IXK(i0, 1, j)] = x[IXK(i0, i2 + 1, j)];
+    x[IXK(i0, i2 + 2, j)] = x[IXK(i0, 2, j)];
+  }
+  __syncthreads();
+}
+
+// out[0] = iterations, out[1] = final r.r, out[2] = 1 when r.r became
+// non-finite (the host loop's early return, without the last ghost refresh)
+__global__ void __launch_bounds__(kCtaThreads, 1)
+    k_bicgstab_cta(const float *al, const float *ab, const float *ac, const float *ar,
+                   const float *at, const float *b, double *x, BicgVecs V, int i2, int j2,
+                   int periodic, double tol, double *out) {
+  __shared__ double red[32];
+  __shared__ double sc[S_NSC];
+  const int tid = threadIdx.x;
+  const int i0 = i2 + 2;
+  const size_t n = (size_t)(i2 + 2) * (j2 + 2), ni = (size_t)i2 * j2;
+  int iter = 0;
+  bool nonfinite = false;
+  double tp = 1.0, res = 0.0;
+  cta_boundary(x, i2, j2, periodic);
+  while (sqrt(tp) > tol && iter < 1000) {
+    if (tid == 0) sc[S_RHO] = 1.0, sc[S_ALPHA] = 1.0, sc[S_W] = 1.0;
+    cta_apply(al, ab, ac, ar, at, x, V.r, i2, j2);
+    for (size_t e = tid; e < ni; e += blockDim.x) {
+      const int i = 1 + (int)(e % i2), j = 1 + (int)(e / i2);
+      V.r[IXK(i0, i + 1, j + 1)] = sub((double)b[IXK(i2, i, j)], V.r[IXK(i0, i + 1, j + 1)]);
+    }
+    __syncthreads();
+    cta_boundary(V.r, i2, j2, periodic);
+    for (size_t k = tid; k < n; k += blockDim.x) V.rh[k] = V.r[k];
+    __syncthreads();
+    tp = cta_dot(V.r, V.r, i2, j2, red, &sc[S_TP]);
+    res = sqrt(tp);
+    if (res < tol) break;
+    while (sqrt(tp) / res > tol) {
+      iter = iter + 1;
+      const double rhn = cta_dot(V.r, V.rh, i2, j2, red, &sc[S_RHN]);
+      if (tid == 0)
+        sc[S_BETA] = __dmul_rn(__ddiv_rn(rhn, sc[S_RHO]), __ddiv_rn(sc[S_ALPHA], sc[S_W]));
+      __syncthreads();
+      {
+        const double beta = sc[S_BETA], w = sc[S_W];
+        for (size_t k = tid; k < n; k += blockDim.x) {
+          const double pv = add(V.r[k], mul(beta, sub(V.p[k], mul(w, V.v[k]))));
+          V.p[k] = pv;
+          V.ph[k] = pv;
+        }
+      }
+      __syncthreads();
+      cta_boundary(V.ph, i2, j2, periodic);
+      cta_apply(al, ab, ac, ar, at, V.ph, V.v, i2, j2);
+      cta_boundary(V.v, i2, j2, periodic);
+      const double tmp = cta_dot(V.rh, V.v, i2, j2, red, &sc[S_TMP]);
+      if (tid == 0) sc[S_ALPHA] = __ddiv_rn(rhn, tmp);
+      __syncthreads();
+      {
+        const double alpha = sc[S_ALPHA];
+        for (size_t k = tid; k < n; k += blockDim.x) {
+          const double sv = sub(V.r[k], mul(alpha, V.v[k]));
+          V.s[k] = sv;
+          V.sh[k] = sv;
+        }
+      }
+      __syncthreads();
+      cta_boundary(V.sh, i2, j2, periodic);
+      cta_apply(al, ab, ac, ar, at, V.sh, V.t, i2, j2);
+      cta_boundary(V.t, i2, j2, periodic);
+      const double tt = cta_dot(V.t, V.t, i2, j2, red, &sc[S_TT]);
+      const double ts = cta_dot(V.t, V.s, i2, j2, red, &sc[S_TS]);
+      if (tid == 0) sc[S_W] = __ddiv_rn(ts, tt);
+      __syncthreads();
+      {
+        const double alpha = sc[S_ALPHA], w = sc[S_W];
+        for (size_t k = tid; k < n; k += blockDim.x) {
+          x[k] = add(add(x[k], mul(alpha, V.ph[k])), mul(w, V.sh[k]));
+          V.r[k] = sub(V.s[k], mul(w, V.t[k]));
+        }
+      }
+      __syncthreads();
+      tp = cta_dot(V.r, V.r, i2, j2, red, &sc[S_TP]);
+      if (tid == 0) sc[S_RHO] = rhn;
+      __syncthreads();
+      if (!isfinite(tp)) {
+        nonfinite = true;
+        break;
+      }
+      if (iter % 100 == 0) break;
+    }
+    if (nonfinite) break;
+  }
+  if (!nonfinite) cta_boundary(x, i2, j2, periodic);
+  if (tid == 0) {
+    out[0] = (double)iter;
+    out[1] = tp;
+    out[2] = nonfinite ? 1.0 : 0.0;
+  }
+}
+
 // CSI: q = omega*work1 + (csy*omega - 1)*q; x = x + q
 __global__ void k_csi_qx(const double *work1, double *q, double *x, double omega, double csy,
                          size_t n, int first) {
@@ -219,6 +372,13 @@ struct Work {
     if (sc) cudaFree(sc);
     if (hsc) cudaFreeHost(hsc);
   }
+  // the state init leaves: every buffer, the ticket and the scalars zero
+  int zero(size_t n, cudaStream_t st) {
+    for (double *b : bufs) SEVP_CUDA_TRY(cudaMemsetAsync(b, 0, n * 8, st));
+    SEVP_CUDA_TRY(cudaMemsetAsync(ticket, 0, 8, st));
+    SEVP_CUDA_TRY(cudaMemsetAsync(sc, 0, S_NSC * 8, st));
+    return SEVP_OK;
+  }
   int init(int nvec, size_t n, cudaStream_t st) {
     bufs.assign(nvec, nullptr);
     for (auto &b : bufs) {
@@ -233,6 +393,47 @@ struct Work {
     SEVP_CUDA_TRY(cudaMallocHost((void **)&hsc, S_NSC * 8));
     return SEVP_OK;
   }
+};
+
+// Work buffers kept between calls while the drop-in cache is on
+// (sevp_dropin_cache): one set per (device, vectors, length), zeroed again
+// for every call, so repeated calls allocate nothing (the pinned scalar
+// mirror costs the most).
+struct KeptWork {
+  int device, nvec;
+  size_t n;
+  Work *w;
+};
+std::vector<KeptWork> g_kept_work;
+
+// The buffers of one Krylov call: the kept set while caching is on, else a
+// set owned by the call.
+class CallWork {
+  std::unique_ptr<Work> own_;
+  Work *w_ = nullptr;
+
+ public:
+  int acquire(int nvec, size_t n, cudaStream_t st) {
+    if (dropin_cache_on()) {
+      int dev = 0;
+      SEVP_CUDA_TRY(cudaGetDevice(&dev));
+      for (const KeptWork &k : g_kept_work)
+        if (k.device == dev && k.nvec == nvec && k.n == n) {
+          w_ = k.w;
+          return w_->zero(n, st);
+        }
+      std::unique_ptr<Work> w(new Work);
+      int s = w->init(nvec, n, st);
+      if (s) return s;
+      w_ = w.get();
+      g_kept_work.push_back(KeptWork{dev, nvec, n, w.release()});
+      return SEVP_OK;
+    }
+    own_.reset(new Work);
+    w_ = own_.get();
+    return w_->init(nvec, n, st);
+  }
+  Work &get() { return *w_; }
 };
 
 unsigned dot_blocks(int i2, int j2) {
@@ -263,9 +464,10 @@ static int dot_into(const double *a, const double *b, int i2, int j2, double *ou
 
 int dev_inprod(const double *r, const double *p, int i2, int j2, double *result_host,
                cudaStream_t st) {
-  Work w;
-  int s = w.init(0, 1, st);
+  CallWork cw;
+  int s = cw.acquire(0, 1, st);
   if (s) return s;
+  Work &w = cw.get();
   s = dot_into(r, p, i2, j2, w.sc, w, st);
   if (s) return s;
   SEVP_CUDA_TRY(cudaMemcpyAsync(result_host, w.sc, 8, cudaMemcpyDeviceToHost, st));
@@ -290,11 +492,29 @@ int dev_bicgstab(const float *al, const float *ab, const float *ac, const float 
                  const float *at, const float *b, double *x, int i2, int j2, int periodic,
                  int *iters, double *final_res, cudaStream_t st) {
   const size_t n = (size_t)(i2 + 2) * (j2 + 2);
-  Work w;
-  TRY(w.init(8, n, st));
+  CallWork cw;
+  TRY(cw.acquire(8, n, st));
+  Work &w = cw.get();
   double *r = w.bufs[0], *rh = w.bufs[1], *p = w.bufs[2], *v = w.bufs[3], *s = w.bufs[4],
          *t = w.bufs[5], *ph = w.bufs[6], *sh = w.bufs[7];
   const double tol = (double)1e-8f;
+  if (n <= kCtaMaxPoints) {
+    // small grid: the whole solve in one thread block, one launch
+    k_bicgstab_cta<<<1, kCtaThreads, 0, st>>>(al, ab, ac, ar, at, b, x,
+                                              BicgVecs{r, rh, p, v, s, t, ph, sh}, i2, j2,
+                                              periodic, tol, w.partials);
+    SEVP_CUDA_TRY(cudaGetLastError());
+    double out[3];
+    SEVP_CUDA_TRY(cudaMemcpyAsync(out, w.partials, sizeof out, cudaMemcpyDeviceToHost, st));
+    SEVP_CUDA_TRY(cudaStreamSynchronize(st));
+    *iters = (int)out[0];
+    if (out[2] != 0.0) {
+      *final_res = out[1];
+      return SEVP_NONFINITE;
+    }
+    *final_res = std::sqrt(out[1]);
+    return (std::sqrt(out[1]) > tol) ? SEVP_MAXITER : SEVP_OK;
+  }
   auto bdry = [&](double *a) { return periodic ? dev_boundary(a, i2, j2, st) : SEVP_OK; };
   auto fetch = [&]() -> int {
     SEVP_CUDA_TRY(cudaMemcpyAsync(w.hsc, w.sc, S_NSC * 8, cudaMemcpyDeviceToHost, st));
@@ -357,8 +577,9 @@ int dev_csi(const float *al, const float *ab, const float *ac, const float *ar, 
             double mineig, double maxeig, const float *b, double *x, int i2, int j2, int periodic,
             int *iters, double *final_res, cudaStream_t st) {
   const size_t n = (size_t)(i2 + 2) * (j2 + 2);
-  Work w;
-  TRY(w.init(4, n, st));  // r, s, q, work1 all start at zero, as in the reference
+  CallWork cw;
+  TRY(cw.acquire(4, n, st));  // r, s, q, work1 all start at zero, as in the reference
+  Work &w = cw.get();
   double *r = w.bufs[0], *s = w.bufs[1], *q = w.bufs[2], *work1 = w.bufs[3];
   auto bdry = [&](double *a) { return periodic ? dev_boundary(a, i2, j2, st) : SEVP_OK; };
   const double tol = (double)1e-7f;
@@ -412,8 +633,9 @@ int dev_lanczos(const float *al, const float *ab, const float *ac, const float *
                 const float *at, int i2, int j2, double *mineig, double *maxeig, cudaStream_t st) {
   enum { M = 10 };
   const size_t n = (size_t)(i2 + 2) * (j2 + 2);
-  Work w;
-  TRY(w.init(7, n, st));
+  CallWork cw;
+  TRY(cw.acquire(7, n, st));
+  Work &w = cw.get();
   double *v = w.bufs[0], *ww = w.bufs[1], *vp = w.bufs[2], *wp = w.bufs[3], *s = w.bufs[4],
          *q = w.bufs[5], *work = w.bufs[6];
   const unsigned eb = ew_blocks(n);
@@ -538,4 +760,11 @@ int host_ratqr(int n, double eps1, const double *d, const double *e, double *min
   return 0;
 }
 
+// Frees the Work sets kept for the drop-in cache (sevp_dropin_cache).
+void release_kept_work() {
+  for (const KeptWork &k : g_kept_work) delete k.w;
+  g_kept_work.clear();
+}
+
 }  // namespace sevp
+
