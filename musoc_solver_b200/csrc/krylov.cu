@@ -192,11 +192,16 @@ struct BicgVecs {
   double *r, *rh, *p, *v, *s, *t, *ph, *sh;
 };
 
-__device__ double cta_dot(const double *a, const double *b, int i2, int j2, double *red,
-                          double *out) {
+// The passes below take restrict-qualified pointers (the vectors are
+// distinct buffers) and unroll by four, so a thread issues the loads of
+// several elements before the first store: each pass costs a few memory
+// round trips instead of one per element.
+__device__ double cta_dot(const double *__restrict__ a, const double *__restrict__ b, int i2,
+                          int j2, double *red, double *out) {
   const int i0 = i2 + 2;
   const size_t n = (size_t)i2 * j2;
   double v[1] = {0.0};
+#pragma unroll 4
   for (size_t e = threadIdx.x; e < n; e += blockDim.x) {
     const int i = 2 + (int)(e % i2), j = 2 + (int)(e / i2);
     v[0] += a[IXK(i0, i, j)] * b[IXK(i0, i, j)];
@@ -206,10 +211,13 @@ __device__ double cta_dot(const double *a, const double *b, int i2, int j2, doub
   __syncthreads();
   return *out;
 }
-__device__ void cta_apply(const float *al, const float *ab, const float *ac, const float *ar,
-                          const float *at, const double *x, double *r, int i2, int j2) {
+__device__ void cta_apply(const float *__restrict__ al, const float *__restrict__ ab,
+                          const float *__restrict__ ac, const float *__restrict__ ar,
+                          const float *__restrict__ at, const double *__restrict__ x,
+                          double *__restrict__ r, int i2, int j2) {
   const int i0 = i2 + 2;
   const size_t n = (size_t)i2 * j2;
+#pragma unroll 4
   for (size_t e = threadIdx.x; e < n; e += blockDim.x) {
     const int i = 1 + (int)(e % i2), j = 1 + (int)(e / i2);
     const size_t c = IXK(i2, i, j);
@@ -219,6 +227,58 @@ __device__ void cta_apply(const float *al, const float *ab, const float *ac, con
     t = add(t, mul((double)ar[c], x[IXK(i0, i + 2, j + 1)]));
     t = add(t, mul((double)at[c], x[IXK(i0, i + 1, j + 2)]));
     r[IXK(i0, i + 1, j + 1)] = t;
+  }
+  __syncthreads();
+}
+// b - r on the interior
+__device__ void cta_rhs_minus(const float *__restrict__ b, double *__restrict__ r, int i2,
+                              int j2) {
+  const int i0 = i2 + 2;
+  const size_t ni = (size_t)i2 * j2;
+#pragma unroll 4
+  for (size_t e = threadIdx.x; e < ni; e += blockDim.x) {
+    const int i = 1 + (int)(e % i2), j = 1 + (int)(e / i2);
+    r[IXK(i0, i + 1, j + 1)] = sub((double)b[IXK(i2, i, j)], r[IXK(i0, i + 1, j + 1)]);
+  }
+  __syncthreads();
+}
+__device__ void cta_copy(const double *__restrict__ a, double *__restrict__ c, size_t n) {
+#pragma unroll 4
+  for (size_t k = threadIdx.x; k < n; k += blockDim.x) c[k] = a[k];
+  __syncthreads();
+}
+// p = r + beta*(p - w*v); ph = p
+__device__ void cta_p(const double *__restrict__ r, double *__restrict__ p,
+                      const double *__restrict__ v, double *__restrict__ ph, double beta, double w,
+                      size_t n) {
+#pragma unroll 4
+  for (size_t k = threadIdx.x; k < n; k += blockDim.x) {
+    const double pv = add(r[k], mul(beta, sub(p[k], mul(w, v[k]))));
+    p[k] = pv;
+    ph[k] = pv;
+  }
+  __syncthreads();
+}
+// s = r - alpha*v; sh = s
+__device__ void cta_s(const double *__restrict__ r, const double *__restrict__ v,
+                      double *__restrict__ s, double *__restrict__ sh, double alpha, size_t n) {
+#pragma unroll 4
+  for (size_t k = threadIdx.x; k < n; k += blockDim.x) {
+    const double sv = sub(r[k], mul(alpha, v[k]));
+    s[k] = sv;
+    sh[k] = sv;
+  }
+  __syncthreads();
+}
+// x = x + alpha*ph + w*sh; r = s - w*t
+__device__ void cta_xr(double *__restrict__ x, double *__restrict__ r,
+                       const double *__restrict__ ph, const double *__restrict__ sh,
+                       const double *__restrict__ s, const double *__restrict__ t, double alpha,
+                       double w, size_t n) {
+#pragma unroll 4
+  for (size_t k = threadIdx.x; k < n; k += blockDim.x) {
+    x[k] = add(add(x[k], mul(alpha, ph[k])), mul(w, sh[k]));
+    r[k] = sub(s[k], mul(w, t[k]));
   }
   __syncthreads();
 }
@@ -241,8 +301,7 @@ __global__ void __launch_bounds__(kCtaThreads, 1)
   __shared__ double red[32];
   __shared__ double sc[S_NSC];
   const int tid = threadIdx.x;
-  const int i0 = i2 + 2;
-  const size_t n = (size_t)(i2 + 2) * (j2 + 2), ni = (size_t)i2 * j2;
+  const size_t n = (size_t)(i2 + 2) * (j2 + 2);
   int iter = 0;
   bool nonfinite = false;
   double tp = 1.0, res = 0.0;
@@ -250,14 +309,9 @@ __global__ void __launch_bounds__(kCtaThreads, 1)
   while (sqrt(tp) > tol && iter < 1000) {
     if (tid == 0) sc[S_RHO] = 1.0, sc[S_ALPHA] = 1.0, sc[S_W] = 1.0;
     cta_apply(al, ab, ac, ar, at, x, V.r, i2, j2);
-    for (size_t e = tid; e < ni; e += blockDim.x) {
-      const int i = 1 + (int)(e % i2), j = 1 + (int)(e / i2);
-      V.r[IXK(i0, i + 1, j + 1)] = sub((double)b[IXK(i2, i, j)], V.r[IXK(i0, i + 1, j + 1)]);
-    }
-    __syncthreads();
+    cta_rhs_minus(b, V.r, i2, j2);
     cta_boundary(V.r, i2, j2, periodic);
-    for (size_t k = tid; k < n; k += blockDim.x) V.rh[k] = V.r[k];
-    __syncthreads();
+    cta_copy(V.r, V.rh, n);
     tp = cta_dot(V.r, V.r, i2, j2, red, &sc[S_TP]);
     res = sqrt(tp);
     if (res < tol) break;
@@ -267,30 +321,14 @@ __global__ void __launch_bounds__(kCtaThreads, 1)
       if (tid == 0)
         sc[S_BETA] = __dmul_rn(__ddiv_rn(rhn, sc[S_RHO]), __ddiv_rn(sc[S_ALPHA], sc[S_W]));
       __syncthreads();
-      {
-        const double beta = sc[S_BETA], w = sc[S_W];
-        for (size_t k = tid; k < n; k += blockDim.x) {
-          const double pv = add(V.r[k], mul(beta, sub(V.p[k], mul(w, V.v[k]))));
-          V.p[k] = pv;
-          V.ph[k] = pv;
-        }
-      }
-      __syncthreads();
+      cta_p(V.r, V.p, V.v, V.ph, sc[S_BETA], sc[S_W], n);
       cta_boundary(V.ph, i2, j2, periodic);
       cta_apply(al, ab, ac, ar, at, V.ph, V.v, i2, j2);
       cta_boundary(V.v, i2, j2, periodic);
       const double tmp = cta_dot(V.rh, V.v, i2, j2, red, &sc[S_TMP]);
       if (tid == 0) sc[S_ALPHA] = __ddiv_rn(rhn, tmp);
       __syncthreads();
-      {
-        const double alpha = sc[S_ALPHA];
-        for (size_t k = tid; k < n; k += blockDim.x) {
-          const double sv = sub(V.r[k], mul(alpha, V.v[k]));
-          V.s[k] = sv;
-          V.sh[k] = sv;
-        }
-      }
-      __syncthreads();
+      cta_s(V.r, V.v, V.s, V.sh, sc[S_ALPHA], n);
       cta_boundary(V.sh, i2, j2, periodic);
       cta_apply(al, ab, ac, ar, at, V.sh, V.t, i2, j2);
       cta_boundary(V.t, i2, j2, periodic);
@@ -298,14 +336,7 @@ __global__ void __launch_bounds__(kCtaThreads, 1)
       const double ts = cta_dot(V.t, V.s, i2, j2, red, &sc[S_TS]);
       if (tid == 0) sc[S_W] = __ddiv_rn(ts, tt);
       __syncthreads();
-      {
-        const double alpha = sc[S_ALPHA], w = sc[S_W];
-        for (size_t k = tid; k < n; k += blockDim.x) {
-          x[k] = add(add(x[k], mul(alpha, V.ph[k])), mul(w, V.sh[k]));
-          V.r[k] = sub(V.s[k], mul(w, V.t[k]));
-        }
-      }
-      __syncthreads();
+      cta_xr(x, V.r, V.ph, V.sh, V.s, V.t, sc[S_ALPHA], sc[S_W], n);
       tp = cta_dot(V.r, V.r, i2, j2, red, &sc[S_TP]);
       if (tid == 0) sc[S_RHO] = rhn;
       __syncthreads();

@@ -5,9 +5,9 @@
 // arithmetic, predicated loads and shuffles (about 90 instructions per grid
 // point for 28 bytes moved).  Here the tensor memory accelerator moves every
 // array of a 64 x 32 tile, with its halo, into shared memory: one thread
-// issues a handful of 2-D bulk copies per tile, up to four tiles are in flight
-// per CTA (an mbarrier per stage counts their bytes), and the 256 threads
-// then read the five-point neighbourhoods from shared memory.
+// issues a handful of 2-D bulk copies per tile, two or three tiles are in
+// flight per CTA (an mbarrier per stage counts their bytes), and the 256
+// threads then read the five-point neighbourhoods from shared memory.
 //
 // Boxes of a tile with origin (x0, j0) (x0 a multiple of 64, so every box's
 // first column is 16-byte aligned, as a tensor copy requires):
@@ -115,7 +115,7 @@ struct TmaFin {
 };
 
 template <typename V, bool SYM, int STAGES>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(kThreads, 2)
     k_pass_a_tma(const __grid_constant__ Maps maps, GridDims g, const V *__restrict__ z,
                  const V *__restrict__ pold, const float *__restrict__ ar_g, V *pnew, V *q,
                  SolveState *st, double *partials, unsigned *ticket) {
@@ -334,10 +334,10 @@ const Maps *tensor_maps(const PassALaunch<V> &L) {
 template <typename V, bool SYM>
 int launch(const PassALaunch<V> &L) {
   using S = Stage<V, SYM>;
-  // as many stages as fit (four for FP32 vectors, three for FP64): with one
-  // CTA per SM the copies in flight have to cover the memory latency
-  constexpr int kStages = 4 * S::kBytes + 128 <= 220 * 1024
-                              ? 4
+  // FP32 vectors: two CTAs per SM with two stages each (one CTA computes
+  // while the other waits at a barrier); FP64: one CTA with three stages
+  constexpr int kStages = 2 * (2 * S::kBytes + 128) <= 220 * 1024
+                              ? 2
                               : (3 * S::kBytes + 128 <= 220 * 1024 ? 3 : 2);
   const Maps *mp = tensor_maps<V, SYM>(L);
   if (!mp) {

@@ -273,3 +273,27 @@ def test_step_submit_overlapped_copies_match_step_host(torch_cuda):
     s2.step_wait()
     s1.step_host(rhs[0], xb, guess=N.GUESS_LINEAR, precision=1)
     assert np.array_equal(xa, xb)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_solve_at_the_1440x720_grid_matches_oracle(torch_cuda, oracle, precision):
+    """Parity at a configuration's own size: the 1440x720 global grid (c2,
+    16x6 tiles, growth bound 1e10), FP64 and mixed, against the oracle's
+    FP64 tile PCG on all host cores; the residual recomputed on the host."""
+    torch = torch_cuda
+    from musoc_solver_b200.solver import SevpSolver
+
+    p = P.global_grid(1440, 720, seed=11)
+    s = SevpSolver(p, tile_m=16, tile_h=6, growth_limit=1e10)
+    b = torch.from_numpy(p.b).cuda()
+    x, rep = s.solve(b, precision=precision, tol=1e-12)
+    assert rep.status == 0 and rep.rel_residual <= 1e-12
+    xg = x.cpu().numpy()
+    res = np.linalg.norm(p.b - P.apply_operator(p, xg)) / np.linalg.norm(p.b)
+    assert res <= 2e-12
+    pc = oracle.TilePC(p, 16, 6, tile_nb=s.tile_nb)
+    xo, it, rel = pc.pcg(p.b, tol=1e-12)
+    assert rel <= 1e-12
+    assert np.abs(xg - xo).max() <= 1e-9 * np.abs(xo).max()
+    if precision == 0:
+        assert abs(rep.iterations - it) <= 2
