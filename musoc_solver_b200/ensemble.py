@@ -56,14 +56,23 @@ class EnsembleSolver:
     def member_norms(self, v):
         return v.reshape(self.m, -1).norm(dim=1)
 
-    def solve(self, b, x=None, precision=1, tol=1e-12, max_iter=5000, inner_tol=1e-5):
-        """Solves all members; returns (x, result, per-member relative
-        residuals as a host array)."""
+    def stacked_tol(self, b, tol=1e-12):
+        """The stacked system's tolerance that guarantees ``tol`` for every
+        member (see the module note)."""
         bn = self.member_norms(b)
-        tol_stack = tol * float(bn.min() / b.norm()) if float(b.norm()) > 0 else tol
+        return tol * float(bn.min() / b.norm()) if float(b.norm()) > 0 else tol
+
+    def solve(self, b, x=None, precision=1, tol=1e-12, max_iter=5000, inner_tol=1e-5,
+              residuals=True, tol_stack=None, x_is_guess=True):
+        """Solves all members; returns (x, result, per-member relative
+        residuals as a host array, or None with ``residuals=False``).
+        ``tol_stack`` (from ``stacked_tol``) skips recomputing the stacked
+        tolerance; ``x_is_guess=False`` solves from zero into ``x``."""
+        if tol_stack is None:
+            tol_stack = self.stacked_tol(b, tol)
         x, res = self.solver.solve(b, x=x, precision=precision, tol=tol_stack, max_iter=max_iter,
-                                   inner_tol=inner_tol)
-        return x, res, self.member_residuals(b, x)
+                                   inner_tol=inner_tol, x_is_guess=x_is_guess)
+        return x, res, (self.member_residuals(b, x) if residuals else None)
 
     def member_residuals(self, b, x):
         r = b - self.solver.apply(x)

@@ -292,11 +292,13 @@ class SevpSolver:
         return bool(N.lib().sevp_operator_symmetric(self.h))
 
     def solve(self, b, x=None, precision=0, tol=1e-12, max_iter=5000, inner_tol=1e-5,
-              check_every=4):
+              check_every=4, x_is_guess=True):
         """Solves on device tensors (float64, shape (ny, nx)).  ``x`` holds the
-        initial guess when given and receives the solution."""
+        initial guess when given and receives the solution; with
+        ``x_is_guess=False`` it only receives the solution of a solve from
+        zero (the library zeroes it)."""
         torch = self.torch
-        use_guess = x is not None
+        use_guess = x is not None and x_is_guess
         if x is None:
             x = torch.zeros((self.ny, self.nx), dtype=torch.float64, device=self.device)
         o = self.opts(precision, tol, max_iter, inner_tol, use_guess, check_every)

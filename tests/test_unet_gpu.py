@@ -514,3 +514,39 @@ def test_conv_wgrad_tcgen05(torch_cuda, cin, cout, B, H, W, x_ld, x_off):
     dxr = torch.nn.grad.conv2d_input((B, cin, H, W), wr, gm, padding=1).permute(0, 2, 3, 1)
     dxr = dxr.reshape(P, cin)
     assert (torch.norm(dx2.double().cpu() - dxr) / torch.norm(dxr)).item() < 4e-3
+
+
+def test_conv_wgrad_tcgen05_bounded_wait(torch_cuda):
+    """The weight-gradient kernel's bounded waits: with the poll limit at 0
+    every CTA gives up at its first wait for a stage (each has five steps of
+    64 pixels here), drains the MMAs it issued, adds nothing to dw and
+    records SEVP_TIMEOUT; with the limit restored the same call is exact."""
+    torch = torch_cuda
+    import ctypes as C
+
+    from musoc_solver_b200.unet import lib
+
+    L = lib()
+    cin, cout, H, W = 32, 32, 64, 160
+    rng = np.random.default_rng(9)
+    x = _bf(torch, rng.standard_normal((H * W, cin))).cuda()
+    g = _bf(torch, rng.standard_normal((H * W, cout))).cuda()
+    dw = torch.zeros((9, cin, cout), dtype=torch.float32, device="cuda")
+    p = lambda t: C.c_void_p(t.data_ptr())
+    code = C.c_int(-1)
+    assert L.sevp_nn_tc_status(C.byref(code)) == 0
+    try:
+        assert L.sevp_nn_tc_set_wait_limit(0) == 0
+        assert L.sevp_nn_conv3x3_wgrad_tc(p(x), cin, 0, cin, p(g), cout, p(dw), 1, H, W, None) == 0
+        assert L.sevp_nn_tc_status(C.byref(code)) == 0
+        assert code.value == 4  # SEVP_TIMEOUT
+        assert bool((dw == 0).all())
+    finally:
+        assert L.sevp_nn_tc_set_wait_limit(0xFFFFFFFF) == 0
+    assert L.sevp_nn_conv3x3_wgrad_tc(p(x), cin, 0, cin, p(g), cout, p(dw), 1, H, W, None) == 0
+    assert L.sevp_nn_tc_status(C.byref(code)) == 0 and code.value == 0
+    xr = x.double().cpu().reshape(1, H, W, cin).permute(0, 3, 1, 2)
+    gr = g.double().cpu().reshape(1, H, W, cout).permute(0, 3, 1, 2)
+    dwr = torch.nn.grad.conv2d_weight(xr, (cout, cin, 3, 3), gr, padding=1)
+    dwr = dwr.permute(2, 3, 1, 0).reshape(9, cin, cout)
+    assert (torch.norm(dw.double().cpu() - dwr) / torch.norm(dwr)).item() < 1e-5
