@@ -624,6 +624,7 @@ def run_ensemble(K, W, members=64, nx=720, ny=360, schwarz=False, inner_tol=1e-5
     t0 = time.perf_counter()
     ms = P.ensemble(members=members, nx=nx, ny=ny, seed=5)
     e = EnsembleSolver(ms)
+    e_th = e.solver.tile_h  # the oracle check uses the same tiles
     setup_s = time.perf_counter() - t0
     b = e.rhs()
     stream = e.solver.stream
@@ -685,7 +686,8 @@ def run_ensemble(K, W, members=64, nx=720, ny=360, schwarz=False, inner_tol=1e-5
         x64_h = x64.reshape(members, ny, nx).cpu().numpy()
         errs_m, errs_64, t0 = [], [], time.perf_counter()
         for k, m in enumerate(ms):
-            pc = O.TilePC(m, 16, 8, tile_nb=tile_sub_blocks(m, 16, 8, GROWTH))
+            th = e_th
+            pc = O.TilePC(m, 16, th, tile_nb=tile_sub_blocks(m, 16, th, GROWTH))
             xo, _, relo = pc.pcg(m.b, tol=1e-12)
             sc = np.abs(xo).max()
             errs_m.append(float(np.abs(xm_h[k] - xo).max() / sc))

@@ -32,5 +32,5 @@ def test_member_tile_height_divides_rows():
     for ny in (24, 48, 360, 180, 90):
         h = member_tile_height(ny)
         assert ny % h == 0 and 6 <= h <= 24
-    assert member_tile_height(360) == 8
+    assert member_tile_height(360) == 6
     assert member_tile_height(45) == 15
