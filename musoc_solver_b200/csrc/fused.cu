@@ -64,8 +64,9 @@ struct FinCheb {
 // task's rows and its halo), dout = d_{k+1}; x and r updated in place.
 template <typename V, typename MT, bool SYM, int HM>
 __global__ void __launch_bounds__(kTileWarps * 32, 2)
-    k_cheb(TileGeom tg, Coeffs c, int periodic, const MT *__restrict__ mats, const V *din,
-           V *dout, V *x, V *r, SolveState *st, double *partials, unsigned *ticket) {
+    k_cheb(TileGeom tg, Coeffs c, int periodic, const MT *__restrict__ mats,
+           const V *__restrict__ din, V *__restrict__ dout, V *__restrict__ x,
+           V *__restrict__ r, SolveState *st, double *partials, unsigned *ticket) {
   if (st->done) return;
   constexpr bool kChain = sizeof(V) == 4;
   __shared__ double dv_all[kTileWarps * 32];
@@ -129,7 +130,8 @@ __global__ void __launch_bounds__(kTileWarps * 32, 2)
     if constexpr (SYM) ab0 = has_s ? __ldg(c.at + idx0 - nx) : 0.f;
 
     // ---- r -= A d on the task's rows (the full operator, across tile
-    //      edges; in FP64 from the FP32 values, rounded once) and x += d
+    //      edges; in the vector type, the same explicitly rounded
+    //      multiply-adds as the PCG's stencil pass) and x += d
 #pragma unroll
     for (int k = 0; k < HM; ++k) {
       V dw = __shfl_sync(0xffffffffu, dk[k], src_w);
@@ -149,14 +151,10 @@ __global__ void __launch_bounds__(kTileWarps * 32, 2)
       const float cb = SYM ? (k == 0 ? ab0 : cn_[k > 0 ? k - 1 : 0]) : cs_[SYM ? 0 : k];
       const V vb = k == 0 ? ds : dk[k > 0 ? k - 1 : 0];
       const V va = (k + 1 < hh) ? dk[k + 1 < HM ? k + 1 : k] : dn;
-      double av = (double)cb * (double)vb;
-      av += (double)cw * (double)dw;
-      av += (double)cc_[k] * (double)dk[k];
-      av += (double)ce_[k] * (double)de;
-      av += (double)cn_[k] * (double)va;
+      const V av = stencil5<V>(cb, vb, cw, dw, cc_[k], dk[k], ce_[k], de, cn_[k], va);
       if (ok) {
         const size_t g = idx0 + (size_t)k * nx;
-        const V rn = (V)((double)rv[k] - av);
+        const V rn = rv[k] - av;
         rv[k] = rn;
         r[g] = rn;
         x[g] = xr[k] + dk[k];
