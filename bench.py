@@ -172,13 +172,15 @@ def measured_peak_hbm():
 
 def ncu_traffic(nx, ny, tiles, kernel="passb"):
     """Per-launch DRAM bytes from the committed ncu summaries (profiles/):
-    the FP32 pass-B kernel ("passb") or the Schwarz stage kernel averaged
-    over stages 2 and 3 ("couple"); None when the summary covers another
-    grid or tile shape (they are 3600x2400 captures with 16x6 tiles)."""
+    the FP32 pass-B kernel ("passb"), the Schwarz stage kernel averaged over
+    stages 2 and 3 ("couple") or the one-launch Chebyshev kernel ("cheb");
+    None when the summary covers another grid or tile shape (they are
+    3600x2400 captures with 16x6 tiles)."""
     if (nx, ny, tuple(tiles)) != (3600, 2400, (16, 6)):
         return None
     name, key = {"passb": ("tile_pass_b_3600x2400.md", "traffic_bytes_per_launch_mixed:"),
-                 "couple": ("schwarz_stages_3600x2400.md", "traffic_bytes_per_launch_avg:")}[kernel]
+                 "couple": ("schwarz_stages_3600x2400.md", "traffic_bytes_per_launch_avg:"),
+                 "cheb": ("cheb_3600x2400.md", "traffic_bytes_per_launch:")}[kernel]
     try:
         for line in open(os.path.join(ROOT, "profiles", name)):
             if line.startswith(key):
@@ -1040,7 +1042,7 @@ def run_native(args, world, rank, local, dist):
     if method == N.METHOD_CHEB:
         dom_name = "k_cheb<float> (one-launch Chebyshev iteration)"
         bytes_per_launch, avg_s, dom_n = b_cheb, tile_ms / 1e3 / max(tile_n, 1), tile_n
-        traffic = None
+        traffic = ncu_traffic(p.nx, p.ny, tiles, "cheb")
     elif use_sw and cpl_n:
         dom_name = "k_tile_couple<float> (Schwarz stages 2 and 3, averaged per launch)"
         bytes_per_launch, avg_s, dom_n = b_couple, cpl_ms / 1e3 / cpl_n, cpl_n
