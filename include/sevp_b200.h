@@ -225,9 +225,10 @@ typedef struct {
   int tol_abs;       /* 1: stop on ||b - A x||_2 <= tol (absolute, the reference's rule,
                         M/sevp.f90:482); 0: the relative test above */
   int method;        /* SEVP_METHOD_*: the outer iteration */
-  int restart_inner; /* precision 1 with PCG: 1 restarts CG at every FP64 residual; 0
-                        (default) replaces the FP32 residual by the FP64 one and keeps the
-                        search direction (reliable updates) */
+  int restart_inner; /* precision 1: 1 restarts the inner iteration at every FP64
+                        residual; 0 (default) replaces the FP32 residual by the FP64 one
+                        and continues: CG keeps its search direction (reliable
+                        updates), Chebyshev its recurrence and last direction */
 } sevp_solve_opts;
 /* Outer iterations of sevp_solve. */
 #define SEVP_METHOD_PCG 0     /* preconditioned CG, two grid passes per iteration */

@@ -1878,6 +1878,23 @@ __global__ void k_state_keep(SolveState *st, double tol2, int max_iter) {
   *st = s;
 }
 
+// State for a residual replacement that continues the Chebyshev
+// recurrence: as k_state_init, with the Chebyshev scalars kept and the
+// launch count at one, so the next launch takes the recurrence's next step
+// on the replaced residual instead of starting over.
+__global__ void k_state_keep_cheb(SolveState *st, double tol2, int max_iter) {
+  SolveState s{};
+  s.tol2 = tol2;
+  s.max_iter = max_iter;
+  s.status = SEVP_OK;
+  s.cheb_theta = st->cheb_theta;
+  s.cheb_delta = st->cheb_delta;
+  s.cheb_sigma = st->cheb_sigma;
+  s.cheb_rho = st->cheb_rho;
+  s.iter = 1;
+  *st = s;
+}
+
 // Starts an FP64 PCG run from the residual pass's norms: the recursive
 // (row-scaled) residual must fall by the factor the outer test still needs,
 // target / ||b - A x||^2 with target = tol^2 ||b||^2 (relative test) or
@@ -2040,12 +2057,16 @@ __global__ void k_state_cheb(SolveState *st, double theta, double delta) {
 
 // Inner FP32 solve A d = r32 from d = 0 (d32 zeroed by the caller) with the
 // one-launch Chebyshev iteration: directions in p32[0], p32[1], x = d32, r =
-// r32 in place.
-static int cheb_inner(sevp_ctx *ctx, int check_every, int *iters_out) {
+// r32 in place.  cont: continue the recurrence of the previous inner solve
+// (its scalars kept by k_state_keep_cheb, its last direction in p32[0])
+// instead of starting it.
+static int cheb_inner(sevp_ctx *ctx, int check_every, int *iters_out, bool cont) {
   const double lmin = ctx->cheb_lmin, lmax = ctx->cheb_lmax;
-  k_state_cheb<<<1, 1, 0, ctx->stream>>>(ctx->st, 0.5 * (lmax + lmin), 0.5 * (lmax - lmin));
-  ctx->launches++;
-  SEVP_CUDA_TRY(cudaGetLastError());
+  if (!cont) {
+    k_state_cheb<<<1, 1, 0, ctx->stream>>>(ctx->st, 0.5 * (lmax + lmin), 0.5 * (lmax - lmin));
+    ctx->launches++;
+    SEVP_CUDA_TRY(cudaGetLastError());
+  }
   float *db[2] = {ctx->p32[0], ctx->p32[1]};
   auto interval = [&](int &cur) -> int {
     for (int k = 0; k < check_every; ++k) {
@@ -2061,7 +2082,7 @@ static int cheb_inner(sevp_ctx *ctx, int check_every, int *iters_out) {
                               nullptr, (const void *)(uintptr_t)SEVP_METHOD_CHEB};
   int s = graph_loop(ctx, true, key, check_every, check_every, interval);
   if (s) return s;
-  *iters_out = ctx->h_st->iter;
+  *iters_out = ctx->h_st->iter - (cont ? 1 : 0);
   return SEVP_OK;
 }
 
@@ -2150,10 +2171,16 @@ static int solve_mixed(sevp_ctx *ctx, const double *b, double *x, const sevp_sol
   // into x, and CG goes on along its previous search direction (unless the
   // caller asks for restarts)
   const bool keep = method == SEVP_METHOD_PCG && !o->restart_inner;
+  // the Chebyshev counterpart: the recurrence continues on the replaced
+  // residual with its last direction
+  const bool keep_cheb = method == SEVP_METHOD_CHEB && !o->restart_inner;
   bool have_dir = false;
   for (int refine = 0; refine < 64; ++refine) {
     if (keep && have_dir)
       k_state_keep<<<1, 1, 0, ctx->stream>>>(ctx->st, inner2, std::max(o->max_iter - total, 0));
+    else if (keep_cheb && have_dir)
+      k_state_keep_cheb<<<1, 1, 0, ctx->stream>>>(ctx->st, inner2,
+                                                   std::max(o->max_iter - total, 0) + 1);
     else
       k_state_init<<<1, 1, 0, ctx->stream>>>(ctx->st, inner2, std::max(o->max_iter - total, 0));
     ctx->launches++;
@@ -2199,7 +2226,13 @@ static int solve_mixed(sevp_ctx *ctx, const double *b, double *x, const sevp_sol
                                       cudaMemcpyDeviceToDevice, ctx->stream));
       have_dir = have_dir || it > 0;
     } else {
-      s = cheb_inner(ctx, std::max(1, o->check_every), &it);
+      s = cheb_inner(ctx, std::max(1, o->check_every), &it, keep_cheb && have_dir);
+      // launch j writes its direction into p32[(j + 1) & 1]; the next inner
+      // solve continues from p32[0]
+      if (!s && keep_cheb && (it & 1))
+        SEVP_CUDA_TRY(cudaMemcpyAsync(ctx->p32[0], ctx->p32[1], ctx->n * sizeof(float),
+                                      cudaMemcpyDeviceToDevice, ctx->stream));
+      have_dir = have_dir || it > 0;
     }
     if (s) return s;
     total += it;

@@ -198,3 +198,31 @@ def test_chebyshev_refuses_unsupported_settings(torch_cuda):
         s.solve(b, precision=1)
     s.close()
 
+
+
+def test_chebyshev_continues_across_residual_replacements(torch_cuda):
+    """Mixed Chebyshev solves that continue the recurrence on each replaced
+    FP64 residual (the default) and ones that restart it: both reach the
+    tolerance, the continued one in at most one more iteration (odd and
+    even check intervals, so the direction's buffer parity is exercised)."""
+    from musoc_solver_b200 import native as N
+    from musoc_solver_b200.solver import SevpSolver
+
+    torch = torch_cuda
+    p = P.global_grid(360, 180, seed=21)
+    s = SevpSolver(p, tile_m=16, tile_h=6, growth_limit=1e6)
+    b = torch.from_numpy(p.b).cuda()
+    s.chebyshev_setup(b)
+    s.set_method(N.METHOD_CHEB)
+    for ce in (3, 4):
+        out = {}
+        for restart in (False, True):
+            s.restart_inner = restart
+            x, rep = s.solve(b, precision=1, tol=1e-12, inner_tol=1e-4, check_every=ce)
+            assert rep.status == 0 and rep.rel_residual <= 1e-12, (ce, restart, rep)
+            assert _residual(p, x.cpu().numpy()) <= 2e-12
+            out[restart] = rep
+        s.restart_inner = False
+        assert out[False].refinements >= 2
+        assert out[False].iterations <= out[True].iterations + 1, (ce, out)
+    s.close()
