@@ -138,8 +138,8 @@ int sevp_nn_to_bf16(const float *a, void *b, long long n, void *stream);
 
 /* Warm-start features of a solver context (on its stream):
  *   e = 2 eta1 - eta2, m = M^-1 (b - A e) (one tile-SEVP solve), d = eta1 - eta2,
- * the three fields averaged over coarse x coarse cells (coarse 1, 2, 4 or 8
- * dividing nx and ny), scales = the RMS of those averages over the cells,
+ * the three fields averaged over coarse x coarse cells (coarse 1, 2, 4, 8 or
+ * 16 dividing nx and ny), scales = the RMS of those averages over the cells,
  * and feat = the averages divided by their scales, as BF16 channels 0..2 of
  * 16 on a wn x hn grid (multiples of 8, at least nx/coarse x ny/coarse;
  * zero padding). */

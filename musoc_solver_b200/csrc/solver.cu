@@ -2518,7 +2518,7 @@ extern "C" int sevp_step_wait(sevp_ctx *ctx) {
 // m/s1, d/s2, then zeros.
 
 // The network grid is the solver grid averaged over coarse x coarse cells
-// (coarse = 1, 2, 4 or 8), padded with zeros to wn x hn (multiples of 8).
+// (coarse = 1, 2, 4, 8 or 16), padded with zeros to wn x hn (multiples of 8).
 // feat holds 16 BF16 channels per network pixel.
 __device__ __forceinline__ bool net_cell(size_t k, int wn, int cx, int cy, int coarse, int &i,
                                          int &j) {
@@ -2641,7 +2641,7 @@ __global__ void k_nn_combine(const double *e, const double *m, const float *y, c
 static unsigned grid_for(size_t n) { return (unsigned)std::min<size_t>((n + 255) / 256, 148 * 16); }
 
 static bool net_grid_ok(const sevp_ctx *ctx, int coarse, int wn, int hn) {
-  if (coarse != 1 && coarse != 2 && coarse != 4 && coarse != 8) return false;
+  if (coarse != 1 && coarse != 2 && coarse != 4 && coarse != 8 && coarse != 16) return false;
   if (ctx->nx % coarse || ctx->ny % coarse) return false;
   return wn % 8 == 0 && hn % 8 == 0 && wn >= ctx->nx / coarse && hn >= ctx->ny / coarse;
 }

@@ -26,14 +26,14 @@ import numpy as np
 from . import native as N
 from .unet import UNet, lib as nnlib
 
-COARSE = (1, 2, 4, 8)
+COARSE = (1, 2, 4, 8, 16)
 
 
 def net_grid(nx: int, ny: int, coarse: int):
     """(H, W) of the network for a solver grid averaged over coarse x coarse
     cells, rounded up to multiples of 8."""
     if coarse not in COARSE or nx % coarse or ny % coarse:
-        raise ValueError("coarse must be 1, 2, 4 or 8 and divide the grid")
+        raise ValueError("coarse must be 1, 2, 4, 8 or 16 and divide the grid")
     r8 = lambda v: (v + 7) // 8 * 8
     return r8(ny // coarse), r8(nx // coarse)
 
