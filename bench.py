@@ -73,7 +73,7 @@ def parse():
                     help="leading steps of the sequence solved in FP64 and used to train the "
                          "warm-start network (untimed)")
     ap.add_argument("--epochs", type=int, default=3)
-    ap.add_argument("--coarse", type=int, default=8, choices=[1, 2, 4, 8, 16],
+    ap.add_argument("--coarse", type=int, default=16, choices=[1, 2, 4, 8, 16],
                     help="the network runs on the grid averaged over coarse x coarse cells")
     ap.add_argument("--tiles", default="auto",
                     help="tile shape MxH of the GPU solver, or 'auto' (measured at start-up)")

@@ -212,7 +212,9 @@ struct OpResidual {
   // (safety * outer tolerance)^2: the inner solve need not go below it; a
   // relative tolerance (of ||b||) unless abs_mode
   double outer2;
-  int set_inner;  // 1: also initialise the inner FP32 solve state
+  // 1: also initialise the inner FP32 solve state; 2: the same for a PCG run
+  // that resumes on this residual (beta from the stopped run's last two r.z)
+  int set_inner;
   const double *roww;  // row weights (ny) or null
   int abs_mode;        // the outer test is absolute: ||b - A x|| <= tol
   __device__ void prepare(SolveState *) {}
@@ -253,6 +255,12 @@ struct OpResidual {
       st->done = 0;
       st->beta = 0.0;
       st->status = SEVP_OK;
+      if (set_inner == 2 && st->rz != 0.0) {
+        // the step the stopped run would have taken next, now on the
+        // replaced residual: z of its last pass stays (one step behind r)
+        st->beta = st->rz_next / st->rz;
+        st->rz = st->rz_next;
+      }
     }
     if (!isfinite(s[0]) || !isfinite(s[2]) || !isfinite(s[3])) st->status = SEVP_NONFINITE;
   }
@@ -1867,13 +1875,15 @@ __global__ void k_state_init(SolveState *st, double tol2, int max_iter, double *
 }
 
 // State for a residual replacement that keeps the search direction: as
-// k_state_init, but r.z of the last iteration stays for the next beta.
+// k_state_init, but the last two r.z of the stopped run stay for the next
+// beta.
 __global__ void k_state_keep(SolveState *st, double tol2, int max_iter) {
   SolveState s{};
   s.tol2 = tol2;
   s.max_iter = max_iter;
   s.status = SEVP_OK;
   s.rz = st->rz;
+  s.rz_next = st->rz_next;
   s.keep_dir = 1;
   *st = s;
 }
@@ -2185,8 +2195,15 @@ static int solve_mixed(sevp_ctx *ctx, const double *b, double *x, const sevp_sol
       k_state_init<<<1, 1, 0, ctx->stream>>>(ctx->st, inner2, std::max(o->max_iter - total, 0));
     ctx->launches++;
     int s;
+    // PCG with reliable updates resumes its run on the FP64 residual: the
+    // replaced r enters the next pass B (r - alpha q) and the preconditioned
+    // residual of the stopped run's last pass stands in for one step.  With
+    // the Schwarz preconditioner the continuation applies the preconditioner
+    // to the replaced residual first (k_state_keep and a start pass)
+    const bool resume = keep && have_dir && !schwarz_on(ctx);
     if (have_d)
-      s = launch_residual<float>(ctx, xa, ctx->d32, xb, b, ctx->r32, 1, inner2, outer2, o->tol_abs);
+      s = launch_residual<float>(ctx, xa, ctx->d32, xb, b, ctx->r32, resume ? 2 : 1, inner2, outer2,
+                                 o->tol_abs);
     else
       s = launch_residual<float>(ctx, xa, nullptr, nullptr, b, ctx->r32, 1, inner2, outer2,
                                  o->tol_abs);
@@ -2215,8 +2232,11 @@ static int solve_mixed(sevp_ctx *ctx, const double *b, double *x, const sevp_sol
     SEVP_CUDA_TRY(cudaMemsetAsync(ctx->d32, 0, ctx->n * 4, ctx->stream));
     int it = 0;
     if (method == SEVP_METHOD_PCG) {
-      s = precondition_pass<float, false, true>(ctx, nullptr, nullptr, ctx->r32, nullptr, ctx->z32);
-      if (s) return s;
+      if (!resume) {
+        s = precondition_pass<float, false, true>(ctx, nullptr, nullptr, ctx->r32, nullptr,
+                                                  ctx->z32);
+        if (s) return s;
+      }
       s = pcg_loop<float>(ctx, ctx->d32, ctx->r32, ctx->z32, ctx->p32[0], ctx->p32[1], ctx->q32,
                           std::max(1, o->check_every), &it);
       // iteration k writes its search direction into p32[(k + 1) & 1]; the

@@ -28,6 +28,10 @@ struct SolveState {
   // 1: the next tile pass continues the previous search direction after a
   // residual replacement (beta = new r.z / old r.z instead of a restart)
   int keep_dir;
+  // r.z of the last tile pass, also when that pass ended the run (rz keeps
+  // the one before): a run resumed on a replaced residual takes its next
+  // beta from the two
+  double rz_next;
   unsigned ticket[4];
   // optional record of the PCG coefficients: alpha_j at hist[2 (j-1)],
   // beta_j at hist[2 (j-1) + 1] for iterations j = 1..hist_cap
@@ -219,6 +223,7 @@ struct TileFin {
     int first = (st->beta == 0.0 && st->iter == 0 && !st->keep_dir);
     st->keep_dir = 0;
     st->rr = rr;
+    st->rz_next = rz;
     if (!isfinite(rz) || !isfinite(rr)) {
       st->status = SEVP_NONFINITE;
       st->done = 1;
