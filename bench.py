@@ -789,7 +789,7 @@ def run_native(args, world, rank, local, dist):
     cands = CANDIDATES if args.tiles == "auto" else (
         tuple(int(v) for v in args.tiles.lower().split("x")),)
     sw_opts = {"auto": (False, True), "bj": (False,), "schwarz": (True,)}[args.precond]
-    itols = (1e-4, 1e-5, 1e-6) if args.inner_tol == "auto" else (float(args.inner_tol),)
+    itols = (1e-3, 1e-4, 1e-5) if args.inner_tol == "auto" else (float(args.inner_tol),)
     methods = {"auto": (N.METHOD_PCG, N.METHOD_CHEB), "pcg": (N.METHOD_PCG,),
                "cheb": (N.METHOD_CHEB,)}[args.method]
     if len(cands) * len(sw_opts) * len(itols) * len(methods) > 1:
