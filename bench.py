@@ -87,6 +87,9 @@ def parse():
     ap.add_argument("--influence-fp32", default="auto",
                     help="growth limit of the per-group FP32 influence data of the inner "
                          "iterations: a number, 'off', or 'auto' (measured)")
+    ap.add_argument("--pass-b", default="registers", choices=["staged", "registers"],
+                    help="kernel of the FP32 PCG tile pass: shared-memory task stages filled "
+                         "by tensor copies, or per-task register loads")
     ap.add_argument("--no-fs", action="store_true",
                     help="skip the barotropic correction loop arm (3600x2400, 20 layers)")
     ap.add_argument("--no-ensemble", action="store_true",
@@ -172,13 +175,15 @@ def measured_peak_hbm():
 
 def ncu_traffic(nx, ny, tiles, kernel="passb"):
     """Per-launch DRAM bytes from the committed ncu summaries (profiles/):
-    the FP32 pass-B kernel ("passb"), the Schwarz stage kernel averaged over
+    the FP32 pass-B kernel ("passb", or "passb_staged" for the kernel with
+    tensor-copied task stages), the Schwarz stage kernel averaged over
     stages 2 and 3 ("couple") or the one-launch Chebyshev kernel ("cheb");
     None when the summary covers another grid or tile shape (they are
     3600x2400 captures with 16x6 tiles)."""
     if (nx, ny, tuple(tiles)) != (3600, 2400, (16, 6)):
         return None
     name, key = {"passb": ("tile_pass_b_3600x2400.md", "traffic_bytes_per_launch_mixed:"),
+                 "passb_staged": ("pass_b_staged_3600x2400.md", "traffic_bytes_per_launch:"),
                  "couple": ("schwarz_stages_3600x2400.md", "traffic_bytes_per_launch_avg:"),
                  "cheb": ("cheb_3600x2400.md", "traffic_bytes_per_launch:")}[kernel]
     try:
@@ -814,6 +819,7 @@ def run_native(args, world, rank, local, dist):
         base.close()
         solver = SevpSolver(p, tile_m=tiles[0], tile_h=tiles[1], growth_limit=GROWTH,
                             precond_fp32=args.precond_fp32, schwarz=use_sw)
+    solver.set_pass_b_kernel(N.PASS_B_STAGED if args.pass_b == "staged" else N.PASS_B_REGISTERS)
     stream = solver.stream
     cheb_bounds = None
     if method == N.METHOD_CHEB:
@@ -1037,8 +1043,12 @@ def run_native(args, world, rank, local, dist):
     # coefficient planes; influence data
     b_cheb = n * (4 * 3 + 4 * 3 + 4 * ncoef) + infl_a
     short_tiles = tiles[1] <= 6  # FP32 vectors with tiles up to 6 rows run the short-tile kernel
-    passb_name = ("k_tile_short<float, update, dots>" if short_tiles
-                  else "k_tile_apply<float, update, dots>") + " (PCG pass B)"
+    staged = solver.pass_b_kernel_used() == N.PASS_B_STAGED
+    if staged:
+        passb_name = "k_pass_b_tma (PCG pass B, tensor-copied task stages)"
+    else:
+        passb_name = ("k_tile_short<float, update, dots>" if short_tiles
+                      else "k_tile_apply<float, update, dots>") + " (PCG pass B)"
     if method == N.METHOD_CHEB:
         dom_name = "k_cheb<float> (one-launch Chebyshev iteration)"
         bytes_per_launch, avg_s, dom_n = b_cheb, tile_ms / 1e3 / max(tile_n, 1), tile_n
@@ -1050,7 +1060,7 @@ def run_native(args, world, rank, local, dist):
     else:
         dom_name = passb_name
         bytes_per_launch, avg_s, dom_n = b_passb, tile_ms / 1e3 / max(tile_n, 1), tile_n
-        traffic = ncu_traffic(p.nx, p.ny, tiles, "passb")
+        traffic = ncu_traffic(p.nx, p.ny, tiles, "passb_staged" if staged else "passb")
     achieved = bytes_per_launch / avg_s / 1e9 if dom_n else None
 
     # ---- 64-member ensemble (720x360 each), every launch over all members
@@ -1126,6 +1136,9 @@ def run_native(args, world, rank, local, dist):
             "marching_growth_limit": GROWTH,
             "coefficient_planes": 3 if solver.symmetric else 5,
             "influence_fp32_in_inner_solve": bool(args.precond_fp32),
+            "pass_b_kernel": {N.PASS_B_STAGED: "staged (tensor-copied task stages)",
+                              N.PASS_B_REGISTERS: "registers"}.get(solver.pass_b_kernel_used(),
+                                                                    "none"),
             "influence_fp32_growth_limit": mix_limit or None,
             "influence_fp32_groups": [mix_groups[0], mix_groups[1]],
             "influence_bytes_per_tile_pass": mix_groups[2],
@@ -1219,6 +1232,7 @@ def run_profile(args):
         tiles = (16, 6) if args.tiles == "auto" else tuple(int(v) for v in args.tiles.split("x"))
         s = SevpSolver(p, tile_m=tiles[0], tile_h=tiles[1], growth_limit=GROWTH,
                        schwarz=args.precond == "schwarz")
+        s.set_pass_b_kernel(N.PASS_B_STAGED if args.pass_b == "staged" else N.PASS_B_REGISTERS)
         b = torch.from_numpy(p.b).cuda()
         if args.method == "cheb":
             s.chebyshev_setup(b)

@@ -292,6 +292,23 @@ int sevp_set_graphs(sevp_ctx *ctx, int enable);
 #define SEVP_PASS_A_TILES 0
 #define SEVP_PASS_A_COLUMNS 1
 int sevp_set_pass_a_kernel(sevp_ctx *ctx, int kind);
+/* Kernel of the FP32 PCG's tile pass (x += alpha p, r -= alpha q, z = M^-1 r,
+ * r.z, r.r) on block-Jacobi tiles of at most 6 rows:
+ * SEVP_PASS_B_REGISTERS (default) loads each task's rows and influence
+ * matrices into registers when it starts; SEVP_PASS_B_STAGED has every warp keep
+ * a shared-memory stage that tensor copies fill with the next task's rows
+ * and matrices while it marches the current one, where the tiling and the
+ * buffers allow it (tiles 8, 16 or 32 columns wide, nx a multiple of 4,
+ * symmetric operator, FP64 influence data; otherwise the register kernel
+ * runs).  Both give the same x, r and z bit for bit.  Not part of the
+ * reference interface. */
+#define SEVP_PASS_B_REGISTERS 0
+#define SEVP_PASS_B_STAGED 1
+int sevp_set_pass_b_kernel(sevp_ctx *ctx, int kind);
+/* The kernel the context's last FP32 PCG tile pass ran: SEVP_PASS_B_REGISTERS
+ * or SEVP_PASS_B_STAGED, -1 before the first.  Test hook; not part of the
+ * reference interface. */
+int sevp_pass_b_kernel_used(const sevp_ctx *ctx);
 /* One stencil pass on caller device buffers with the context's operator and
  * pass A kernel: p = z + beta p_old (z alone when beta == 0), q = A p, and
  * p.q through pq_out.  Test hook; not part of the reference interface. */

@@ -1021,6 +1021,8 @@ struct sevp_ctx {
   int use_graphs = 1;
   int stencil_rpw = 0;  // rows per CTA of the stencil kernels (0: not chosen yet)
   int pass_a_kernel = SEVP_PASS_A_TILES;
+  int pass_b_kernel = SEVP_PASS_B_REGISTERS;
+  int pass_b_used = -1;  // kernel of the last FP32 pass B launch
   cudaStream_t cap_stream = nullptr;
   cudaGraphExec_t inner_graph = nullptr;
   int inner_graph_ce = 0;
@@ -1166,6 +1168,21 @@ static int launch_tile_k(sevp_ctx *ctx, const Tiling &T, const MT *mats, V *x, c
   if (s) return s;
   const unsigned blocks = (unsigned)std::min<size_t>((warps + kTileWarps - 1) / kTileWarps,
                                                      (size_t)slots[short_tiles]);
+  if constexpr (sizeof(V) == 4 && std::is_same<MT, double>::value && UPDATE && DOTS && SYM) {
+    // PCG pass B with tensor-copied task stages, on the same grid
+    if (short_tiles && ctx->pass_b_kernel == SEVP_PASS_B_STAGED) {
+      const PassBLaunch L{T.tg, T.c, mats, x, p, r, q, z, ctx->st, ctx->partials,
+                          ctx->partials_n, ctx->tickets + ticket_slot, blocks, ctx->stream};
+      if (pass_b_tma_eligible(L)) {
+        ProfScope ps(ctx, 0);
+        const int s2 = pass_b_tma_launch(L);
+        ctx->launches++;
+        ctx->pass_b_used = SEVP_PASS_B_STAGED;
+        return s2;
+      }
+    }
+    ctx->pass_b_used = SEVP_PASS_B_REGISTERS;
+  }
   ProfScope ps(ctx, UPDATE ? 0 : 2);
   kern<<<blocks, kTileWarps * 32, smem, ctx->stream>>>(T.tg, T.c, mats, x, p, r, q, z, ctx->st,
                                                       ctx->partials, ctx->tickets + ticket_slot);
@@ -1414,6 +1431,15 @@ extern "C" int sevp_set_pass_a_kernel(sevp_ctx *ctx, int kind) {
   drop_inner_graph(ctx);
   return SEVP_OK;
 }
+
+extern "C" int sevp_set_pass_b_kernel(sevp_ctx *ctx, int kind) {
+  if (!ctx || (kind != SEVP_PASS_B_REGISTERS && kind != SEVP_PASS_B_STAGED)) return SEVP_BAD_ARG;
+  ctx->pass_b_kernel = kind;
+  drop_inner_graph(ctx);
+  return SEVP_OK;
+}
+
+extern "C" int sevp_pass_b_kernel_used(const sevp_ctx *ctx) { return ctx ? ctx->pass_b_used : -1; }
 
 extern "C" int sevp_set_full_coefficients(sevp_ctx *ctx, int force) {
   if (!ctx) return SEVP_BAD_ARG;

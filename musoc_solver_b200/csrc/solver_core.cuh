@@ -259,14 +259,16 @@ struct TileFin {
 // code, without the sub-block bookkeeping.  RCP: the FP32-vector march
 // keeps the reciprocals of AT from the forward sweep for the backward sweep
 // (the same rows) instead of forming them again; chosen per kernel, since
-// the registers it takes pay off in some and not in others.
-template <typename MT, bool SYM, bool kChain, int HM, bool RCP, class Rhs, class Emit>
-__device__ __forceinline__ void march_task_full(const float (&cc_)[HM], const float (&ce_)[HM],
-                                                const float (&cn_)[HM],
-                                                const float (&cw_)[SYM ? 1 : HM],
-                                                const float (&cs_)[SYM ? 1 : HM], int n, int mw,
-                                                bool active, int lane, int segbase, double *dv,
-                                                const MT *mt, Rhs &&rhs, Emit &&emit) {
+// the registers it takes pay off in some and not in others.  mv() gives an
+// active lane its entry of the influence mat-vec of dv (filled by the
+// forward sweep); post() runs on every lane once all lanes have it.
+template <bool SYM, bool kChain, int HM, bool RCP, class Rhs, class Emit, class Mv, class Post>
+__device__ __forceinline__ void march_task_full_mv(const float (&cc_)[HM], const float (&ce_)[HM],
+                                                   const float (&cn_)[HM],
+                                                   const float (&cw_)[SYM ? 1 : HM],
+                                                   const float (&cs_)[SYM ? 1 : HM], int n, int mw,
+                                                   bool active, int lane, double *dv, Rhs &&rhs,
+                                                   Emit &&emit, Mv &&mv, Post &&post) {
   double zs[HM], rcp[RCP ? HM : 1];
   double zb = 0.0, zc = 0.0, rho = 0.0;
   float cn_prev = 0.f;
@@ -313,8 +315,9 @@ __device__ __forceinline__ void march_task_full(const float (&cc_)[HM], const fl
   }
   dv[lane] = rho;
   __syncwarp();
-  const double v = active ? seg_matvec<MT>(dv, segbase, mt, mw, n) : 0.0;
+  const double v = active ? mv() : 0.0;
   __syncwarp();
+  post();
   zs[0] += v;
   double hb = 0.0, hc = v;
   float cn_prev_b = 0.f;
@@ -351,6 +354,18 @@ __device__ __forceinline__ void march_task_full(const float (&cc_)[HM], const fl
 #pragma unroll
     for (int k = 0; k < HM; ++k) emit(k, zs[k]);
   }
+}
+
+template <typename MT, bool SYM, bool kChain, int HM, bool RCP, class Rhs, class Emit>
+__device__ __forceinline__ void march_task_full(const float (&cc_)[HM], const float (&ce_)[HM],
+                                                const float (&cn_)[HM],
+                                                const float (&cw_)[SYM ? 1 : HM],
+                                                const float (&cs_)[SYM ? 1 : HM], int n, int mw,
+                                                bool active, int lane, int segbase, double *dv,
+                                                const MT *mt, Rhs &&rhs, Emit &&emit) {
+  march_task_full_mv<SYM, kChain, HM, RCP>(
+      cc_, ce_, cn_, cw_, cs_, n, mw, active, lane, dv, rhs, emit,
+      [&]() { return seg_matvec<MT>(dv, segbase, mt, mw, n); }, []() {});
 }
 
 // SEVP march of one task with every row in registers: the forward sweep
@@ -590,5 +605,32 @@ template <typename V>
 bool pass_a_tma_eligible(const PassALaunch<V> &L);
 template <typename V>
 int pass_a_tma_launch(const PassALaunch<V> &L);
+
+// PCG pass B on FP32 vectors with the task rows and influence matrices
+// brought in by the tensor memory accelerator (tile_tma.cu): x += alpha p,
+// r -= alpha q, z = M^-1 r on the block-Jacobi tiles (symmetric operator,
+// FP64 influence data), r.z and r.r, and the finish of the iteration.
+struct PassBLaunch {
+  TileGeom tg;
+  Coeffs c;
+  const double *mats;
+  float *x;
+  const float *p;
+  float *r;
+  const float *q;
+  float *z;
+  SolveState *st;
+  double *partials;
+  size_t partials_n;  // doubles in partials (three per CTA are used)
+  unsigned *ticket;
+  unsigned blocks;  // grid size (the register kernel's, so the sums run in its order)
+  cudaStream_t stream;
+};
+// Whether the tiling and the buffers suit the kernel (tile columns of 8, 16
+// or 32 lanes, unshifted, at most kShortTileRows rows; rows of a multiple
+// of 16 bytes; 16-byte aligned buffers; tensor maps the driver accepts).
+bool pass_b_tma_eligible(const PassBLaunch &L);
+// SEVP_BAD_ARG (nothing launched) when not eligible.
+int pass_b_tma_launch(const PassBLaunch &L);
 
 }  // namespace sevp

@@ -23,13 +23,10 @@
 // Waits on the stage barriers are bounded: a wait that gives up marks the
 // pass failed (the finisher then reports SEVP_TIMEOUT) and the CTA still
 // waits, with the same bound, for the copies it issued before it exits.
-#include <cuda.h>
-#include <cudaTypedefs.h>
-
 #include <algorithm>
-#include <mutex>
 
 #include "solver_core.cuh"
+#include "tma_util.cuh"
 
 namespace sevp {
 
@@ -38,41 +35,10 @@ namespace {
 constexpr int kTW = 64, kTH = 32;   // output tile
 constexpr int kThreads = 256;       // 4 row groups of 8 rows x 64 columns
 constexpr int kRowsPerThread = kTH / (kThreads / kTW);
-constexpr unsigned kWaitLimit = 1u << 20;
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(uint32_t bar, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, unsigned parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-      " selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(ok)
-      : "r"(bar), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, unsigned parity) {
-  for (unsigned k = 0; k < kWaitLimit; ++k)
-    if (mbar_try_wait(bar, parity)) return true;
-  return false;
-}
-__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int c0, int c1,
-                                            uint32_t bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3}], [%4];\n" ::"r"(dst),
-      "l"((uint64_t)map), "r"(c0), "r"(c1), "r"(bar)
-      : "memory");
-}
+using tma::mbar_expect_tx;
+using tma::mbar_init;
+using tma::mbar_wait;
+using tma::smem_u32;
 
 __host__ __device__ constexpr uint32_t round128(uint32_t b) { return (b + 127u) & ~127u; }
 
@@ -132,7 +98,7 @@ __global__ void __launch_bounds__(kThreads, 2)
   const int TX = (nx + kTW - 1) / kTW, TY = (ny + kTH - 1) / kTH, ntile = TX * TY;
   if (tid == 0) {
     for (int s = 0; s < STAGES; ++s) mbar_init(smem_u32(&full[s]), 1);
-    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    tma::fence_mbar_init();
   }
   __syncthreads();
   auto issue = [&](int k) {  // the copies of this CTA's k-th tile
@@ -143,16 +109,16 @@ __global__ void __launch_bounds__(kThreads, 2)
     const uint32_t bar = smem_u32(&full[k % STAGES]);
     // the stage's previous tile was read and written through the generic
     // proxy (ordered before this thread by the CTA barrier)
-    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    tma::fence_proxy_async();
     mbar_expect_tx(bar, S::kTx);
-    tma_load_2d(st0 + S::kOff_z, &maps.z, x0 - S::kH, j0 - 1, bar);
-    tma_load_2d(st0 + S::kOff_p, &maps.p, x0 - S::kH, j0 - 1, bar);
-    tma_load_2d(st0 + S::kOff_ac, &maps.ac, x0, j0, bar);
-    tma_load_2d(st0 + S::kOff_ar, &maps.ar, x0 - 4, j0, bar);
-    tma_load_2d(st0 + S::kOff_at, &maps.at, x0, j0 - 1, bar);
+    tma::load_2d(st0 + S::kOff_z, &maps.z, x0 - S::kH, j0 - 1, bar);
+    tma::load_2d(st0 + S::kOff_p, &maps.p, x0 - S::kH, j0 - 1, bar);
+    tma::load_2d(st0 + S::kOff_ac, &maps.ac, x0, j0, bar);
+    tma::load_2d(st0 + S::kOff_ar, &maps.ar, x0 - 4, j0, bar);
+    tma::load_2d(st0 + S::kOff_at, &maps.at, x0, j0 - 1, bar);
     if (!SYM) {
-      tma_load_2d(st0 + S::kOff_al, &maps.al, x0, j0, bar);
-      tma_load_2d(st0 + S::kOff_ab, &maps.ab, x0, j0, bar);
+      tma::load_2d(st0 + S::kOff_al, &maps.al, x0, j0, bar);
+      tma::load_2d(st0 + S::kOff_ab, &maps.ab, x0, j0, bar);
     }
   };
   const int nmine = blockIdx.x < ntile ? (ntile - 1 - blockIdx.x) / gridDim.x + 1 : 0;
@@ -252,34 +218,9 @@ __global__ void __launch_bounds__(kThreads, 2)
   reduce_and_finish<2>(acc, partials, ticket, fin);
 }
 
-PFN_cuTensorMapEncodeTiled_v12000 encoder() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    void *f = nullptr;
-    cudaDriverEntryPointQueryResult qr{};
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &qr) ==
-            cudaSuccess &&
-        qr == cudaDriverEntryPointSuccess)
-      fn = (PFN_cuTensorMapEncodeTiled_v12000)f;
-  });
-  return fn;
-}
-
-// A 2-D tensor map of an (nx, ny) row-major plane with the given box.
-bool encode(PFN_cuTensorMapEncodeTiled_v12000 enc, CUtensorMap *m, const void *base, bool fp64,
-            int nx, int ny, int bw, int bh) {
-  const cuuint64_t dims[2] = {(cuuint64_t)nx, (cuuint64_t)ny};
-  const cuuint64_t strides[1] = {(cuuint64_t)nx * (fp64 ? 8 : 4)};
-  const cuuint32_t box[2] = {(cuuint32_t)bw, (cuuint32_t)bh};
-  const cuuint32_t es[2] = {1, 1};
-  return enc(m, fp64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
-             const_cast<void *>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
-}
-
-bool aligned16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
+using tma::aligned16;
+using tma::encode;
+using tma::encoder;
 
 // Tensor maps of recent launches (a solve alternates between two p buffers;
 // a few contexts may share the thread).

@@ -29,6 +29,8 @@ METHOD_CHEB = 1  # one-launch Chebyshev iteration (mixed precision, needs bounds
 
 PASS_A_TILES = 0    # stencil pass on tensor-copied shared-memory tiles
 PASS_A_COLUMNS = 1  # stencil pass walking columns with warp shuffles
+PASS_B_REGISTERS = 0  # tile pass loading each task into registers
+PASS_B_STAGED = 1     # tile pass with tensor-copied shared-memory task stages
 
 GUESS_ZERO, GUESS_PREVIOUS, GUESS_LINEAR, GUESS_LEARNED = 0, 1, 2, 3
 
@@ -121,6 +123,8 @@ _SIGS = {
     "sevp_set_full_coefficients": ([P, C.c_int], C.c_int),
     "sevp_set_graphs": ([P, C.c_int], C.c_int),
     "sevp_set_pass_a_kernel": ([P, C.c_int], C.c_int),
+    "sevp_set_pass_b_kernel": ([P, C.c_int], C.c_int),
+    "sevp_pass_b_kernel_used": ([P], C.c_int),
     "sevp_pass_a_f32": ([P, P, P, C.c_double, P, P, P], C.c_int),
     "sevp_pass_a_f64": ([P, P, P, C.c_double, P, P, P], C.c_int),
     "sevp_set_schwarz": ([P, C.c_int], C.c_int),

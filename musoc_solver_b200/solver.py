@@ -395,6 +395,17 @@ class SevpSolver:
         tiles, the default where the grid allows) or N.PASS_A_COLUMNS."""
         N.check(N.lib().sevp_set_pass_a_kernel(self.h, int(kind)), "sevp_set_pass_a_kernel")
 
+    def set_pass_b_kernel(self, kind: int):
+        """Kernel of the FP32 PCG's tile pass: N.PASS_B_REGISTERS (the
+        default) or N.PASS_B_STAGED (tensor-copied task stages, where the
+        tiling allows)."""
+        N.check(N.lib().sevp_set_pass_b_kernel(self.h, int(kind)), "sevp_set_pass_b_kernel")
+
+    def pass_b_kernel_used(self) -> int:
+        """The kernel the last FP32 tile pass ran (N.PASS_B_*), -1 before
+        the first."""
+        return int(N.lib().sevp_pass_b_kernel_used(self.h))
+
     def pass_a(self, z, pold, beta: float):
         """One stencil pass: (p, q, p.q) with p = z + beta p_old, q = A p."""
         pnew = self.torch.empty_like(z)
