@@ -90,6 +90,9 @@ def parse():
     ap.add_argument("--pass-b", default="registers", choices=["staged", "registers"],
                     help="kernel of the FP32 PCG tile pass: shared-memory task stages filled "
                          "by tensor copies, or per-task register loads")
+    ap.add_argument("--resume-dev", type=float, default=0.3,
+                    help="largest relative distance between the recursive and the replaced "
+                         "residual at which a mixed PCG run resumes (<= 0: never)")
     ap.add_argument("--no-fs", action="store_true",
                     help="skip the barotropic correction loop arm (3600x2400, 20 layers)")
     ap.add_argument("--no-ensemble", action="store_true",
@@ -820,6 +823,7 @@ def run_native(args, world, rank, local, dist):
         solver = SevpSolver(p, tile_m=tiles[0], tile_h=tiles[1], growth_limit=GROWTH,
                             precond_fp32=args.precond_fp32, schwarz=use_sw)
     solver.set_pass_b_kernel(N.PASS_B_STAGED if args.pass_b == "staged" else N.PASS_B_REGISTERS)
+    solver.set_resume_check(args.resume_dev)
     stream = solver.stream
     cheb_bounds = None
     if method == N.METHOD_CHEB:
@@ -1136,6 +1140,7 @@ def run_native(args, world, rank, local, dist):
             "marching_growth_limit": GROWTH,
             "coefficient_planes": 3 if solver.symmetric else 5,
             "influence_fp32_in_inner_solve": bool(args.precond_fp32),
+            "resume_check_max_rel_dev": args.resume_dev,
             "pass_b_kernel": {N.PASS_B_STAGED: "staged (tensor-copied task stages)",
                               N.PASS_B_REGISTERS: "registers"}.get(solver.pass_b_kernel_used(),
                                                                     "none"),

@@ -305,6 +305,15 @@ int sevp_set_pass_a_kernel(sevp_ctx *ctx, int kind);
 #define SEVP_PASS_B_REGISTERS 0
 #define SEVP_PASS_B_STAGED 1
 int sevp_set_pass_b_kernel(sevp_ctx *ctx, int kind);
+/* Mixed-precision PCG with block-Jacobi tiles (restart_inner 0): after each
+ * FP64 residual the stopped run resumes with the preconditioned residual of
+ * its last pass, one step behind, when the distance between its recursive
+ * FP32 residual and the replaced one is at most max_rel_dev times the
+ * replaced residual's norm (default 0.3); otherwise, and always with the
+ * Schwarz preconditioner, the replaced residual is preconditioned afresh
+ * before CG goes on along its last direction.  max_rel_dev <= 0 never
+ * resumes.  Not part of the reference interface. */
+int sevp_set_resume_check(sevp_ctx *ctx, double max_rel_dev);
 /* The kernel the context's last FP32 PCG tile pass ran: SEVP_PASS_B_REGISTERS
  * or SEVP_PASS_B_STAGED, -1 before the first.  Test hook; not part of the
  * reference interface. */

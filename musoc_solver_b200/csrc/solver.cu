@@ -200,7 +200,8 @@ struct OpPassA {
 template <typename R>
 struct OpResidual {
   using T = double;
-  static constexpr int NV = 4;
+  // ||r||^2, ||w b||^2, ||ru||^2, ||b||^2, and for a resumed run ||r - r_old||^2
+  static constexpr int NV = 5;
   static constexpr bool kUsesState = false;
   const double *x;
   const float *d;
@@ -214,7 +215,10 @@ struct OpResidual {
   double outer2;
   // 1: also initialise the inner FP32 solve state; 2: the same for a PCG run
   // that resumes on this residual (beta from the stopped run's last two r.z)
+  // when the stopped run's recursive residual, still in r, is within
+  // resume_dev of the replaced one (relative)
   int set_inner;
+  double resume_dev;
   const double *roww;  // row weights (ny) or null
   int abs_mode;        // the outer test is absolute: ||b - A x|| <= tol
   __device__ void prepare(SolveState *) {}
@@ -232,6 +236,10 @@ struct OpResidual {
       const double w = roww[j];
       rv = w * ru;
       bw = w * bv;
+    }
+    if (set_inner == 2 && r) {
+      const double dr = rv - (double)r[idx];
+      acc[4] += dr * dr;
     }
     if (r) r[idx] = (R)rv;
     acc[0] += rv * rv;
@@ -255,11 +263,17 @@ struct OpResidual {
       st->done = 0;
       st->beta = 0.0;
       st->status = SEVP_OK;
-      if (set_inner == 2 && st->rz != 0.0) {
-        // the step the stopped run would have taken next, now on the
-        // replaced residual: z of its last pass stays (one step behind r)
+      // the step the stopped run would have taken next, now on the replaced
+      // residual: z of its last pass stays (one step behind r).  Sound only
+      // while the recursive residual still tracks the true one; a run that
+      // reduced its residual down to FP32 rounding (a nearly exact
+      // preconditioner) leaves a z unrelated to the replaced residual, and
+      // the caller then preconditions the replaced residual afresh
+      st->resumed = 0;
+      if (set_inner == 2 && st->rz != 0.0 && s[4] <= resume_dev * resume_dev * s[0]) {
         st->beta = st->rz_next / st->rz;
         st->rz = st->rz_next;
+        st->resumed = 1;
       }
     }
     if (!isfinite(s[0]) || !isfinite(s[2]) || !isfinite(s[3])) st->status = SEVP_NONFINITE;
@@ -964,6 +978,9 @@ struct sevp_ctx {
   // growth limit of the per-group FP32 influence data of the FP32-vector
   // tile passes (sevp_set_influence_fp32; <= 1: off)
   double mix_limit = 0.0;
+  // largest ||r_true - r_recursive|| / ||r_true|| at which a mixed PCG run
+  // resumes on a replaced residual (sevp_set_resume_check)
+  double resume_dev = 0.3;
   // the tiling request of the last sevp_set_operator (the second tiling is
   // built from it)
   sevp_tiling treq{};
@@ -1439,6 +1456,12 @@ extern "C" int sevp_set_pass_b_kernel(sevp_ctx *ctx, int kind) {
   return SEVP_OK;
 }
 
+extern "C" int sevp_set_resume_check(sevp_ctx *ctx, double max_rel_dev) {
+  if (!ctx || !(max_rel_dev == max_rel_dev)) return SEVP_BAD_ARG;
+  ctx->resume_dev = max_rel_dev;
+  return SEVP_OK;
+}
+
 extern "C" int sevp_pass_b_kernel_used(const sevp_ctx *ctx) { return ctx ? ctx->pass_b_used : -1; }
 
 extern "C" int sevp_set_full_coefficients(sevp_ctx *ctx, int force) {
@@ -1883,7 +1906,7 @@ template <typename R>
 static int launch_residual(sevp_ctx *ctx, const double *x, const float *d, double *xout,
                            const double *b, R *r, int set_inner, double tol2,
                            double outer2 = 0.0, int abs_mode = 0) {
-  OpResidual<R> op{x, d, xout, b, r, ctx->st, tol2, outer2, set_inner,
+  OpResidual<R> op{x, d, xout, b, r, ctx->st, tol2, outer2, set_inner, ctx->resume_dev,
                    ctx->have_res ? ctx->roww : nullptr, abs_mode};
   if (ctx->have_res) return launch_stencil_c(ctx, op, 2, ctx->cres, ctx->res_sym);
   return launch_stencil(ctx, op, 2);
@@ -2223,10 +2246,13 @@ static int solve_mixed(sevp_ctx *ctx, const double *b, double *x, const sevp_sol
     int s;
     // PCG with reliable updates resumes its run on the FP64 residual: the
     // replaced r enters the next pass B (r - alpha q) and the preconditioned
-    // residual of the stopped run's last pass stands in for one step.  With
-    // the Schwarz preconditioner the continuation applies the preconditioner
-    // to the replaced residual first (k_state_keep and a start pass)
-    const bool resume = keep && have_dir && !schwarz_on(ctx);
+    // residual of the stopped run's last pass stands in for one step, when
+    // the residual pass finds the stopped run's recursive residual close to
+    // the replaced one (SolveState::resumed); otherwise the continuation
+    // applies the preconditioner to the replaced residual first.  The
+    // Schwarz sweep does not resume: on the 64-member ensemble its runs are
+    // a few iterations long and resumed solves took 9 iterations against 5
+    const bool resume = keep && have_dir && !schwarz_on(ctx) && ctx->resume_dev > 0.0;
     if (have_d)
       s = launch_residual<float>(ctx, xa, ctx->d32, xb, b, ctx->r32, resume ? 2 : 1, inner2, outer2,
                                  o->tol_abs);
@@ -2258,7 +2284,7 @@ static int solve_mixed(sevp_ctx *ctx, const double *b, double *x, const sevp_sol
     SEVP_CUDA_TRY(cudaMemsetAsync(ctx->d32, 0, ctx->n * 4, ctx->stream));
     int it = 0;
     if (method == SEVP_METHOD_PCG) {
-      if (!resume) {
+      if (!(resume && ctx->h_st->resumed)) {
         s = precondition_pass<float, false, true>(ctx, nullptr, nullptr, ctx->r32, nullptr,
                                                   ctx->z32);
         if (s) return s;

@@ -32,6 +32,10 @@ struct SolveState {
   // the one before): a run resumed on a replaced residual takes its next
   // beta from the two
   double rz_next;
+  // 1 when the last residual pass resumed the stopped run (its recursive
+  // residual was close to the replaced one); 0 when the run restarts its
+  // preconditioned residual from the replaced residual
+  int resumed;
   unsigned ticket[4];
   // optional record of the PCG coefficients: alpha_j at hist[2 (j-1)],
   // beta_j at hist[2 (j-1) + 1] for iterations j = 1..hist_cap

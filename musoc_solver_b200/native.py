@@ -125,6 +125,7 @@ _SIGS = {
     "sevp_set_pass_a_kernel": ([P, C.c_int], C.c_int),
     "sevp_set_pass_b_kernel": ([P, C.c_int], C.c_int),
     "sevp_pass_b_kernel_used": ([P], C.c_int),
+    "sevp_set_resume_check": ([P, C.c_double], C.c_int),
     "sevp_pass_a_f32": ([P, P, P, C.c_double, P, P, P], C.c_int),
     "sevp_pass_a_f64": ([P, P, P, C.c_double, P, P, P], C.c_int),
     "sevp_set_schwarz": ([P, C.c_int], C.c_int),

@@ -401,6 +401,12 @@ class SevpSolver:
         tiling allows)."""
         N.check(N.lib().sevp_set_pass_b_kernel(self.h, int(kind)), "sevp_set_pass_b_kernel")
 
+    def set_resume_check(self, max_rel_dev: float):
+        """Largest ||r_true - r_recursive|| / ||r_true|| at which a mixed PCG
+        run resumes on a replaced residual (default 0.3; <= 0: never)."""
+        N.check(N.lib().sevp_set_resume_check(self.h, float(max_rel_dev)),
+                "sevp_set_resume_check")
+
     def pass_b_kernel_used(self) -> int:
         """The kernel the last FP32 tile pass ran (N.PASS_B_*), -1 before
         the first."""
