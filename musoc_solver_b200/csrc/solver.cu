@@ -1310,10 +1310,17 @@ static int precondition_pass(sevp_ctx *ctx, V *x, const V *p, V *r, const V *q, 
 }
 
 // Folds recorded event pairs into per-class totals (synchronises the stream).
-static void prof_collect(sevp_ctx *ctx) {
+// iters >= 0: the recorded launches are one check interval of PCG
+// iterations, of which iters ran; the launches after the run finished
+// return at once and are not counted (the first iters pass-A and pass-B
+// launches, and the first 2 iters Schwarz stages, are the ones that ran).
+static void prof_collect(sevp_ctx *ctx, int iters = -1) {
   if (!ctx->ev_used) return;
   cudaStreamSynchronize(ctx->stream);
+  int seen[4] = {0, 0, 0, 0};
   for (size_t k = 0; k < ctx->ev_used; ++k) {
+    const int cls = ctx->ev_class[k];
+    if (iters >= 0 && cls != 2 && seen[cls]++ >= (cls == 3 ? 2 * iters : iters)) continue;
     float ms = 0.f;
     if (cudaEventElapsedTime(&ms, ctx->ev_pool[k].first, ctx->ev_pool[k].second) == cudaSuccess) {
       ctx->prof_ms[ctx->ev_class[k]] += ms;
@@ -1982,7 +1989,7 @@ static bool outer_converged(const SolveState *h, const sevp_solve_opts *o) {
 // the same roles.  launches: kernel launches per interval.
 template <class Interval>
 static int graph_loop(sevp_ctx *ctx, bool graph, const void *const (&key)[5], int check_every,
-                      int launches, Interval &&interval) {
+                      int launches, Interval &&interval, bool pcg_iters = false) {
   int cur = 0;
   graph = graph && ctx->use_graphs && !ctx->prof && check_every % 2 == 0;
   if (graph && !(ctx->inner_graph && ctx->inner_graph_ce == check_every &&
@@ -2017,6 +2024,7 @@ static int graph_loop(sevp_ctx *ctx, bool graph, const void *const (&key)[5], in
     ctx->inner_graph_ce = check_every;
     std::copy(key, key + 5, ctx->inner_graph_key);
   }
+  int it0 = 0;  // the run's iterations before this interval (a run starts at 0)
   for (;;) {
     if (graph) {
       SEVP_CUDA_TRY(cudaGraphLaunch(ctx->inner_graph, ctx->stream));
@@ -2027,7 +2035,8 @@ static int graph_loop(sevp_ctx *ctx, bool graph, const void *const (&key)[5], in
     }
     int s = read_state(ctx);
     if (s) return s;
-    prof_collect(ctx);
+    prof_collect(ctx, pcg_iters ? std::max(ctx->h_st->iter - it0, 0) : -1);
+    it0 = ctx->h_st->iter;
     if (ctx->h_st->done) break;
   }
   return SEVP_OK;
@@ -2085,7 +2094,7 @@ static int pcg_loop(sevp_ctx *ctx, V *x, V *r, V *z, V *p0, V *p1, V *q, int che
                               (const void *)(schwarz_on(ctx) ? ctx->tb.d_mats : nullptr),
                               (const void *)(uintptr_t)SEVP_METHOD_PCG};
   int s = graph_loop(ctx, sizeof(V) == 4, key, check_every,
-                     (schwarz_on(ctx) ? 4 : 2) * check_every, interval);
+                     (schwarz_on(ctx) ? 4 : 2) * check_every, interval, true);
   if (s) return s;
   *iters_out = ctx->h_st->iter;
   return SEVP_OK;

@@ -62,3 +62,24 @@ def test_resumed_and_restarted_continuations_agree(torch_cuda, tiles):
     assert abs(i0 - i1) <= max(3, i0 // 10), (i0, i1)
     assert np.abs(x0 - x1).max() <= 1e-9 * np.abs(x0).max()
     s.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_profiled_tile_passes_are_the_iterations(torch_cuda, precision):
+    """Per-kernel profiling counts the pass-B launches that ran an iteration:
+    the launches of a check interval after the run finished return at once
+    and are left out, so the count equals the solve's iterations."""
+    from musoc_solver_b200.solver import SevpSolver
+
+    torch = torch_cuda
+    p = P.global_grid(320, 160, seed=12)
+    s = SevpSolver(p, tile_m=16, tile_h=6)
+    b = torch.from_numpy(p.b).cuda()
+    s.profile(True)
+    x, rep = s.solve(b, precision=precision, tol=1e-12, check_every=4)
+    prof = s.profile_read()
+    s.profile(False)
+    assert rep.status == 0 and rep.rel_residual <= 1e-12
+    assert prof["tile"][1] == rep.iterations, (prof, rep.iterations)
+    assert prof["tile"][0] > 0.0
+    s.close()
