@@ -2609,36 +2609,43 @@ __device__ __forceinline__ bool net_cell(size_t k, int wn, int cx, int cy, int c
   return ci < cx && cj < cy;
 }
 
-// Coarse-cell averages of r, m and d into avg (3 planes of wn x hn, zero
-// on the padding), and their RMS over the network grid's cells as the
-// normalisation scales[0..2] (the last CTA finishes the sums).
-__global__ void k_pack_avg(const double *r, const double *m, const double *d, float *avg, int nx,
-                           int ny, int coarse, int wn, int hn, double *partials, unsigned *ticket,
-                           float *scales) {
+// Coarse-cell averages of r, m and d into avg (3 planes of wn x hn; the
+// caller zeroes the padding), and their RMS over the network grid's cells
+// as the normalisation scales[0..2] (the last CTA finishes the sums).
+// Grid: blockIdx.y is the coarse row, each thread one fine column of it
+// (coalesced reads down the coarse rows), and the coarse lanes of a cell
+// add their column sums by shuffles (coarse divides 32).
+constexpr int kPackThreads = 256;
+__global__ void __launch_bounds__(kPackThreads)
+    k_pack_avg(const double *r, const double *m, const double *d, float *avg, int nx, int ny,
+               int coarse, int wn, int hn, double *partials, unsigned *ticket, float *scales) {
   const int cx = nx / coarse, cy = ny / coarse;
   const size_t n = (size_t)wn * hn;
   const double inv = 1.0 / (coarse * coarse);
-  double s[3] = {0.0, 0.0, 0.0};
-  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
-       k += (size_t)gridDim.x * blockDim.x) {
-    int i, j;
-    double a = 0.0, bm = 0.0, c = 0.0;
-    if (net_cell(k, wn, cx, cy, coarse, i, j)) {
-      for (int dj = 0; dj < coarse; ++dj)
-        for (int di = 0; di < coarse; ++di) {
-          const size_t q = (size_t)(j + dj) * nx + i + di;
-          a += r[q];
-          bm += m[q];
-          c += d[q];
-        }
+  const int cj = blockIdx.y;
+  const int i = blockIdx.x * kPackThreads + threadIdx.x;
+  double a = 0.0, bm = 0.0, c = 0.0;
+  if (i < cx * coarse) {
+    for (int dj = 0; dj < coarse; ++dj) {
+      const size_t q = (size_t)(cj * coarse + dj) * nx + i;
+      a += r[q];
+      bm += m[q];
+      c += d[q];
     }
+  }
+  for (int off = coarse >> 1; off > 0; off >>= 1) {
+    a += __shfl_down_sync(0xffffffffu, a, off);
+    bm += __shfl_down_sync(0xffffffffu, bm, off);
+    c += __shfl_down_sync(0xffffffffu, c, off);
+  }
+  double s[3] = {0.0, 0.0, 0.0};
+  if (i % coarse == 0 && i / coarse < cx) {
+    const size_t k = (size_t)cj * wn + i / coarse;
     a *= inv, bm *= inv, c *= inv;
     avg[k] = (float)a;
     avg[n + k] = (float)bm;
     avg[2 * n + k] = (float)c;
-    s[0] += a * a;
-    s[1] += bm * bm;
-    s[2] += c * c;
+    s[0] = a * a, s[1] = bm * bm, s[2] = c * c;
   }
   struct Fin {
     float *scales;
@@ -2767,9 +2774,12 @@ extern "C" int sevp_nn_features(sevp_ctx *ctx, const double *eta1, const double 
   // network was trained on), whichever preconditioner the solves use
   s = launch_tile<double, false, false>(ctx, ctx->ta, nullptr, nullptr, ctx->r64, nullptr, m, 1);
   if (s) return s;
-  k_pack_avg<<<grid_for(nn), 256, 0, ctx->stream>>>(ctx->r64, m, d, ctx->nn_avg, ctx->nx, ctx->ny,
-                                                     coarse, wn, hn, ctx->partials,
-                                                     ctx->tickets + 5, scales);
+  SEVP_CUDA_TRY(cudaMemsetAsync(ctx->nn_avg, 0, 3 * nn * sizeof(float), ctx->stream));
+  const dim3 pgrid((unsigned)ceil_div(ctx->nx / coarse * coarse, kPackThreads),
+                   (unsigned)(ctx->ny / coarse));
+  k_pack_avg<<<pgrid, kPackThreads, 0, ctx->stream>>>(ctx->r64, m, d, ctx->nn_avg, ctx->nx,
+                                                      ctx->ny, coarse, wn, hn, ctx->partials,
+                                                      ctx->tickets + 5, scales);
   k_pack_features<<<grid_for(nn), 256, 0, ctx->stream>>>(ctx->nn_avg, scales,
                                                          (__nv_bfloat16 *)feat, nn);
   ctx->launches += 2;
